@@ -1,0 +1,116 @@
+"""Allen raw-bank layout (non-MEP) for VP super-pixel banks, on the host.
+
+A slice of N events is four arrays (main/src/Transpose.cpp:333-425; readers in
+device/event_model/velo/include/ClusteringDefinitions.cuh:97-144 and
+main/include/MEPTools.h:26-53):
+
+* ``raw``      bytes; per event ``n_banks`` (u32), ``bank_offsets[n_banks + 1]``
+               (u32, bytes from the payload start), then per bank its sourceID
+               (u32) followed by the bank data padded to 4 bytes;
+* ``offsets``  u32[N + 1], byte offset of each event blob in ``raw``;
+* ``sizes``    u32[N + 1] offsets in u16 units from the array start, followed by
+               the u16 payload size of every bank;
+* ``types``    u32[N + 1] offsets in u8 units from the array start, followed by
+               the u8 bank type of every bank (VP = 63, Velo = 8).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+BANK_TYPE_VELO = 8
+BANK_TYPE_VP = 63
+
+
+@dataclass
+class RawSlice:
+    raw: np.ndarray      # uint8
+    offsets: np.ndarray  # uint32[N + 1]
+    sizes: np.ndarray    # uint32
+    types: np.ndarray    # uint32
+    bank_version: int
+
+    @property
+    def n_events(self) -> int:
+        return int(self.offsets.shape[0] - 1)
+
+    def n_super_pixels(self) -> int:
+        """Total super pixels of the slice, from the bank sizes alone (no payload read)."""
+        return int(super_pixels_per_event(self).sum())
+
+
+def build_slice(events, bank_version: int) -> RawSlice:
+    """events: list (per event) of lists of (bank_type, source_id, payload bytes)."""
+    n = len(events)
+    blobs, sizes16, types8 = [], [], []
+    for banks in events:
+        words = [np.array([len(banks)], dtype=np.uint32)]
+        offs = [0]
+        datas = []
+        for (btype, src, payload) in banks:
+            pad = (-len(payload)) % 4
+            d = np.frombuffer(bytes(payload) + b"\0" * pad, dtype=np.uint32)
+            datas.append(np.concatenate([np.array([src], dtype=np.uint32), d]))
+            offs.append(offs[-1] + 4 * (1 + d.size))
+            sizes16.append(len(payload))
+            types8.append(btype)
+        words.append(np.array(offs, dtype=np.uint32))
+        words.extend(datas)
+        blobs.append(np.concatenate(words).view(np.uint8))
+    offsets = np.zeros(n + 1, dtype=np.uint32)
+    offsets[1:] = np.cumsum([b.size for b in blobs])
+    raw = np.concatenate(blobs) if blobs else np.zeros(0, np.uint8)
+    nb = np.array([len(b) for b in events], dtype=np.int64)
+    first16, first8 = 2 * (n + 1), 4 * (n + 1)
+    size_offs = first16 + np.concatenate([[0], np.cumsum(nb)])
+    type_offs = first8 + np.concatenate([[0], np.cumsum(nb)])
+    s16 = np.zeros(first16 + int(nb.sum()) + 1, dtype=np.uint16)
+    s16.view(np.uint8)[: 4 * (n + 1)] = size_offs.astype(np.uint32).view(np.uint8)
+    s16[first16:first16 + len(sizes16)] = np.array(sizes16, dtype=np.uint16)
+    t8 = np.zeros(first8 + int(nb.sum()) + 3, dtype=np.uint8)
+    t8[: 4 * (n + 1)] = type_offs.astype(np.uint32).view(np.uint8)
+    t8[first8:first8 + len(types8)] = np.array(types8, dtype=np.uint8)
+    sizes = np.frombuffer(s16.tobytes() + b"\0" * ((-s16.nbytes) % 4), dtype=np.uint32).copy()
+    types = np.frombuffer(t8.tobytes() + b"\0" * ((-t8.nbytes) % 4), dtype=np.uint32).copy()
+    return RawSlice(raw, offsets, sizes, types, bank_version)
+
+
+def banks_of_event(s: RawSlice, event: int):
+    """Decodes one event back into (bank_type, source_id, payload bytes) tuples."""
+    base = int(s.offsets[event])
+    blob = s.raw[base:int(s.offsets[event + 1])]
+    w = blob.view(np.uint32)
+    n_banks = int(w[0])
+    offs = w[1:n_banks + 2]
+    payload_start = 4 * (n_banks + 2)
+    s16 = s.sizes.view(np.uint16)
+    t8 = s.types.view(np.uint8)
+    so, to = int(s.sizes[event]), int(s.types[event])
+    out = []
+    for b in range(n_banks):
+        p = payload_start + int(offs[b])
+        src = int(blob[p:p + 4].view(np.uint32)[0])
+        size = int(s16[so + b])
+        out.append((int(t8[to + b]), src, bytes(blob[p + 4:p + 4 + size])))
+    return out
+
+
+def super_pixels_per_event(s: RawSlice) -> np.ndarray:
+    """Super pixels per event from the bank sizes: (size - 4) / 4 for v2/v3 (count word
+    first), size / 4 for v4.  Upper bound used to size device buffers before launch."""
+    n = s.n_events
+    s16 = s.sizes.view(np.uint16)
+    t8 = s.types.view(np.uint8)
+    out = np.zeros(n, dtype=np.int64)
+    starts = s.sizes[:n + 1].astype(np.int64)
+    tstarts = s.types[:n + 1].astype(np.int64)
+    for e in range(n):
+        sz = s16[starts[e]:starts[e + 1]].astype(np.int64)
+        ty = t8[tstarts[e]:tstarts[e] + sz.size]
+        sel = (ty == BANK_TYPE_VP) | (ty == BANK_TYPE_VELO)
+        words = sz[sel] // 4
+        if s.bank_version in (2, 3):
+            words = np.maximum(words - 1, 0)
+        out[e] = words.sum()
+    return out

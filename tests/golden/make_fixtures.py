@@ -1,0 +1,96 @@
+"""Builds the committed fixtures from the reference checkout (run here, not on the GPU box).
+
+Outputs:
+  allen_b200/data/velo_geometry.bin
+      the detector description the reference ships as
+      input/detector_configuration/velo_geometry.bin (written by
+      Dumpers/BinaryDumpers/src/DumpVPGeometry.cpp:82-90), copied byte for byte;
+  tests/golden/minbias_vp_10ev.npz
+      the VP super-pixel banks (type 63, version 2) of the 10 events of
+      input/minbias/mdf/MiniBrunel_2018_MinBias_FTv4_DIGI_retinacluster_v1.mdf, in
+      Allen's raw-bank layout, plus the reference's own outputs for them;
+  tests/golden/synthetic_seed7_20ev.npz
+      20 generated events (nu = 7.6, seed 7) plus the reference's outputs for them.
+
+The reference outputs come from oracle/_ref/libvelo_ref.so, the reference's VELO
+kernels compiled as CPU C++ (oracle/Makefile).  Usage:
+    python tests/golden/make_fixtures.py [/path/to/reference]
+"""
+from __future__ import annotations
+
+import os
+import struct
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "tests"))
+
+from allen_b200 import rawbanks  # noqa: E402
+
+# Buffers whose contents do not depend on the order atomics are served in.
+GOLDEN_BUFFERS = [
+    "dev_number_of_candidates", "dev_candidates_offsets", "dev_estimated_input_size",
+    "dev_offsets_estimated_input_size", "dev_module_candidate_num", "dev_module_cluster_num",
+    "dev_number_of_velo_tracks", "dev_offsets_velo_tracks", "dev_number_of_three_hit_tracks_output",
+    "dev_offsets_number_of_three_hit_tracks_filtered", "dev_offsets_all_velo_tracks",
+    "dev_velo_track_hit_number", "dev_offsets_velo_track_hit_number", "dev_velo_track_hits",
+    "dev_sorted_velo_cluster_container", "dev_cluster_candidates", "dev_three_hit_tracks_output",
+    "dev_hit_used", "dev_atomics_velo",
+]
+
+
+def read_mdf_vp_events(path):
+    data = open(path, "rb").read()
+    p, events = 0, []
+    while p + 20 <= len(data):
+        size0 = struct.unpack_from("<I", data, p)[0]
+        hdr = data[p + 17]
+        sub = (hdr & 0x0F) * 4
+        q, end = p + 20 + sub, p + size0
+        banks = []
+        while q < end:
+            magic, size, btype, version, src = struct.unpack_from("<HHBBH", data, q)
+            assert magic == 0xCBCB
+            if btype == rawbanks.BANK_TYPE_VP:
+                assert version == 2
+                banks.append((btype, src, data[q + 8:q + size]))
+            q += (size + 3) // 4 * 4
+        events.append(banks)
+        p = end
+    return events
+
+
+def main(ref_root):
+    geo_src = os.path.join(ref_root, "input/detector_configuration/velo_geometry.bin")
+    geometry = open(geo_src, "rb").read()
+    os.makedirs(os.path.join(REPO, "allen_b200/data"), exist_ok=True)
+    with open(os.path.join(REPO, "allen_b200/data/velo_geometry.bin"), "wb") as f:
+        f.write(geometry)
+
+    import cpu_checkers  # noqa: E402
+    ref = cpu_checkers.load("ref")
+
+    mdf = os.path.join(ref_root, "input/minbias/mdf/MiniBrunel_2018_MinBias_FTv4_DIGI_retinacluster_v1.mdf")
+    real = rawbanks.build_slice(read_mdf_vp_events(mdf), bank_version=2)
+
+    from allen_b200 import generator  # noqa: E402
+    synth = generator.generate(20, seed=7, geometry=geometry).raw
+
+    for name, s in (("minbias_vp_10ev", real), ("synthetic_seed7_20ev", synth)):
+        out = ref.run(s, geometry)
+        arrays = {"raw": s.raw, "offsets": s.offsets, "sizes": s.sizes, "types": s.types,
+                  "bank_version": np.array([s.bank_version])}
+        for b in GOLDEN_BUFFERS:
+            arrays["ref__" + b] = out[b]
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+        print(name, s.n_events, "events;",
+              int(out["dev_offsets_all_velo_tracks"][-1]), "tracks;",
+              int(out["dev_module_cluster_num"].sum()), "clusters")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
