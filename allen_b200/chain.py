@@ -1,0 +1,259 @@
+"""Python front end of the C ABI in include/velo_b200.h (ctypes).
+
+Device memory and streams come from torch (plumbing only); every computation runs in
+libvelo_b200.so.  There is no CPU fallback: without an sm_100 device the constructor
+raises.
+
+    chain = VeloChain()                       # geometry from allen_b200/data
+    chain.reserve(max_events, max_super_pixels)
+    dev = upload(raw_slice)                   # RawSlice -> device copy (torch tensors)
+    chain.run(dev)                            # whole chain, one stream, no host sync
+    totals = chain.synchronize()
+    out = chain.outputs_to_host(totals)       # numpy arrays keyed by Allen argument name
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from .rawbanks import RawSlice, super_pixels_per_event
+
+ELEMENT_SIZE = 18
+TRACK_HITS_BYTES = 54
+TRACKLET_BYTES = 6
+N_MODULE_PAIRS = 26
+
+STATUS = {0: "ok", 1: "argument", 2: "cuda", 3: "capacity", 4: "device flags", 5: "no device"}
+DEVICE_FLAGS = {
+    1: "cluster capacity", 2: "track capacity", 4: "tracks-to-follow overflow", 8: "bad sensor",
+    16: "bulk copy timeout", 32: "output capacity", 64: "input capacity", 128: "hits per event",
+}
+
+
+class VeloError(RuntimeError):
+    def __init__(self, status, message, flags=0):
+        super().__init__(f"velo_b200: {STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.flags = flags
+
+
+class Properties(C.Structure):
+    _fields_ = [("phi_tolerance", C.c_float), ("max_scatter", C.c_float),
+                ("max_skipped_modules", C.c_uint), ("max_chi2", C.c_float)]
+
+
+class DeviceSliceC(C.Structure):
+    _fields_ = [("raw", C.c_void_p), ("offsets", C.c_void_p), ("sizes", C.c_void_p), ("types", C.c_void_p),
+                ("event_start", C.c_uint), ("n_events", C.c_uint), ("bank_version", C.c_int)]
+
+
+class HostSliceC(C.Structure):
+    _fields_ = [("raw", C.c_void_p), ("raw_bytes", C.c_size_t), ("offsets", C.c_void_p),
+                ("sizes", C.c_void_p), ("sizes_bytes", C.c_size_t), ("types", C.c_void_p),
+                ("types_bytes", C.c_size_t), ("n_events", C.c_uint), ("bank_version", C.c_int)]
+
+
+OUTPUT_FIELDS = [
+    "dev_number_of_candidates", "dev_estimated_input_size", "dev_module_candidate_num",
+    "dev_offsets_estimated_input_size", "dev_module_cluster_num", "dev_sorted_velo_cluster_container",
+    "dev_tracks", "dev_three_hit_tracks", "dev_hit_used", "dev_atomics_velo", "dev_number_of_velo_tracks",
+    "dev_offsets_velo_tracks", "dev_three_hit_tracks_output", "dev_number_of_three_hit_tracks_output",
+    "dev_offsets_number_of_three_hit_tracks_filtered", "dev_offsets_all_velo_tracks",
+    "dev_velo_track_hit_number", "dev_offsets_velo_track_hit_number", "dev_velo_track_hits",
+    "dev_accepted_velo_tracks",
+]
+
+
+class OutputsC(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in OUTPUT_FIELDS]
+
+
+class TotalsC(C.Structure):
+    _fields_ = [(f, C.c_uint) for f in (
+        "n_events", "host_total_number_of_velo_clusters", "host_number_of_cluster_candidates",
+        "host_number_of_velo_tracks_at_least_four_hits", "host_number_of_three_hit_tracks_filtered",
+        "host_number_of_reconstructed_velo_tracks", "host_accumulated_number_of_hits_in_velo_tracks",
+        "track_container_size", "device_flags")]
+
+
+def _lib():
+    lib = _native.load_chain()
+    if getattr(lib, "_typed", False):
+        return lib
+    lib.velo_last_error_string.restype = C.c_char_p
+    lib.velo_device_check.restype = C.c_int
+    lib.velo_default_properties.argtypes = [C.POINTER(Properties)]
+    lib.velo_chain_create.restype = C.c_int
+    lib.velo_chain_create.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(Properties), C.POINTER(C.c_void_p)]
+    lib.velo_chain_reserve.restype = C.c_int
+    lib.velo_chain_reserve.argtypes = [C.c_void_p, C.c_uint, C.c_ulonglong, C.c_ulonglong]
+    lib.velo_chain_run.restype = C.c_int
+    lib.velo_chain_run.argtypes = [C.c_void_p, C.POINTER(DeviceSliceC), C.c_void_p, C.c_int]
+    lib.velo_chain_run_host.restype = C.c_int
+    lib.velo_chain_run_host.argtypes = [C.c_void_p, C.POINTER(HostSliceC), C.c_void_p,
+                                        C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                        C.POINTER(TotalsC), C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]
+    lib.velo_chain_synchronize.restype = C.c_int
+    lib.velo_chain_synchronize.argtypes = [C.c_void_p, C.POINTER(TotalsC)]
+    lib.velo_chain_outputs.restype = C.c_int
+    lib.velo_chain_outputs.argtypes = [C.c_void_p, C.POINTER(OutputsC)]
+    lib.velo_chain_destroy.argtypes = [C.c_void_p]
+    lib.velo_copy_to_host.restype = C.c_int
+    lib.velo_copy_to_host.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.velo_copy_to_device.restype = C.c_int
+    lib.velo_copy_to_device.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib._typed = True
+    return lib
+
+
+def _check(lib, status, flags=0):
+    if status != 0:
+        raise VeloError(status, lib.velo_last_error_string().decode(), flags)
+
+
+def _current_stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@dataclass
+class DeviceSlice:
+    """A RawSlice resident on the GPU (torch tensors keep the memory alive)."""
+    raw: object
+    offsets: object
+    sizes: object
+    types: object
+    n_events: int
+    bank_version: int
+    event_start: int = 0
+
+    def c_struct(self) -> DeviceSliceC:
+        return DeviceSliceC(self.raw.data_ptr(), self.offsets.data_ptr(), self.sizes.data_ptr(),
+                            self.types.data_ptr(), self.event_start, self.n_events, self.bank_version)
+
+    def sub(self, event_start: int, n_events: int) -> "DeviceSlice":
+        return DeviceSlice(self.raw, self.offsets, self.sizes, self.types, n_events, self.bank_version,
+                           event_start)
+
+
+def upload(s: RawSlice, device="cuda") -> DeviceSlice:
+    import torch
+    raw = np.ascontiguousarray(s.raw)
+    pad = (-raw.size) % 16
+    if pad:
+        raw = np.concatenate([raw, np.zeros(pad, np.uint8)])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+    return DeviceSlice(t(raw), t(s.offsets.view(np.int32)), t(s.sizes.view(np.int32)),
+                       t(s.types.view(np.int32)), s.n_events, s.bank_version)
+
+
+class VeloChain:
+    def __init__(self, geometry: bytes | None = None, phi_tolerance=0.045, max_scatter=0.08,
+                 max_skipped_modules=1, max_chi2=20.0):
+        self.lib = _lib()
+        self.geometry = geometry if geometry is not None else _native.default_geometry()
+        props = Properties(phi_tolerance, max_scatter, max_skipped_modules, max_chi2)
+        h = C.c_void_p()
+        _check(self.lib, self.lib.velo_chain_create(self.geometry, len(self.geometry), C.byref(props), C.byref(h)))
+        self.handle = h
+        self.max_events = 0
+        self.max_super_pixels = 0
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.velo_chain_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reserve(self, max_events: int, max_super_pixels: int, max_raw_bytes: int = 0):
+        _check(self.lib, self.lib.velo_chain_reserve(self.handle, max_events, max_super_pixels, max_raw_bytes))
+        self.max_events, self.max_super_pixels = max_events, max_super_pixels
+
+    def reserve_for(self, s: RawSlice, margin: float = 1.0):
+        n_sp = int(super_pixels_per_event(s).sum())
+        self.reserve(s.n_events, int(n_sp * margin) + 64, s.raw.nbytes + 64)
+
+    def run(self, d: DeviceSlice, stream=None, use_graph: bool = False):
+        st = d.c_struct()
+        _check(self.lib, self.lib.velo_chain_run(self.handle, C.byref(st),
+                                                 stream if stream is not None else _current_stream(),
+                                                 int(use_graph)))
+
+    def synchronize(self, check: bool = True) -> dict:
+        t = TotalsC()
+        status = self.lib.velo_chain_synchronize(self.handle, C.byref(t))
+        totals = {f: getattr(t, f) for f, _ in TotalsC._fields_}
+        if check:
+            _check(self.lib, status, totals["device_flags"])
+        return totals
+
+    def device_outputs(self) -> dict:
+        o = OutputsC()
+        _check(self.lib, self.lib.velo_chain_outputs(self.handle, C.byref(o)))
+        return {f: getattr(o, f) for f in OUTPUT_FIELDS}
+
+    def _fetch(self, ptr, nbytes, dtype):
+        out = np.empty(nbytes, dtype=np.uint8)
+        if nbytes:
+            _check(self.lib, self.lib.velo_copy_to_host(out.ctypes.data, ptr, nbytes))
+        return out.view(dtype) if nbytes % np.dtype(dtype).itemsize == 0 else out
+
+    def outputs_to_host(self, totals: dict) -> dict:
+        """Every output buffer, sized like the reference's set_arguments_size does."""
+        n = totals["n_events"]
+        T = totals["host_total_number_of_velo_clusters"]
+        tcs = totals["track_container_size"]
+        reco = totals["host_number_of_reconstructed_velo_tracks"]
+        three = totals["host_number_of_three_hit_tracks_filtered"]
+        TH = totals["host_accumulated_number_of_hits_in_velo_tracks"]
+        p = self.device_outputs()
+        u4 = np.uint32
+        sizes = {
+            "dev_number_of_candidates": (4 * n, u4), "dev_estimated_input_size": (4 * 26 * n, u4),
+            "dev_module_candidate_num": (4 * n, u4), "dev_offsets_estimated_input_size": (4 * (26 * n + 1), u4),
+            "dev_module_cluster_num": (4 * 26 * n, u4),
+            "dev_sorted_velo_cluster_container": (ELEMENT_SIZE * T, np.uint8),
+            "dev_tracks": (TRACK_HITS_BYTES * tcs, np.uint8), "dev_three_hit_tracks": (TRACKLET_BYTES * tcs, np.uint16),
+            "dev_hit_used": (T, np.uint8), "dev_atomics_velo": (4 * 3 * n, u4),
+            "dev_number_of_velo_tracks": (4 * n, u4), "dev_offsets_velo_tracks": (4 * (n + 1), u4),
+            "dev_three_hit_tracks_output": (TRACKLET_BYTES * tcs, np.uint16),
+            "dev_number_of_three_hit_tracks_output": (4 * n, u4),
+            "dev_offsets_number_of_three_hit_tracks_filtered": (4 * (n + 1), u4),
+            "dev_offsets_all_velo_tracks": (4 * (n + 1), u4), "dev_velo_track_hit_number": (4 * reco, u4),
+            "dev_offsets_velo_track_hit_number": (4 * (reco + 1), u4),
+            "dev_velo_track_hits": (ELEMENT_SIZE * TH, np.uint8),
+            "dev_accepted_velo_tracks": (reco + three, np.uint8),
+        }
+        return {k: self._fetch(p[k], nb, dt) for k, (nb, dt) in sizes.items()}
+
+    def run_host(self, s: RawSlice, stream=None) -> tuple[dict, dict, int, int]:
+        """End-to-end from host buffers; returns (totals, consolidated outputs, h2d bytes, d2h bytes)."""
+        raw = np.ascontiguousarray(s.raw)
+        hs = HostSliceC(raw.ctypes.data, raw.nbytes, s.offsets.ctypes.data, s.sizes.ctypes.data, s.sizes.nbytes,
+                        s.types.ctypes.data, s.types.nbytes, s.n_events, s.bank_version)
+        cap_tracks = 2 * self.max_super_pixels + 64
+        off_all = np.empty(s.n_events + 1, np.uint32)
+        off_hn = np.empty(cap_tracks + 1, np.uint32)
+        hits = np.empty(ELEMENT_SIZE * cap_tracks, np.uint8)
+        t = TotalsC()
+        up, down = C.c_ulonglong(), C.c_ulonglong()
+        status = self.lib.velo_chain_run_host(
+            self.handle, C.byref(hs), stream if stream is not None else _current_stream(),
+            off_all.ctypes.data, off_all.nbytes, off_hn.ctypes.data, off_hn.nbytes, hits.ctypes.data, hits.nbytes,
+            C.byref(t), C.byref(up), C.byref(down))
+        totals = {f: getattr(t, f) for f, _ in TotalsC._fields_}
+        _check(self.lib, status, totals["device_flags"])
+        reco = totals["host_number_of_reconstructed_velo_tracks"]
+        TH = totals["host_accumulated_number_of_hits_in_velo_tracks"]
+        out = {"dev_offsets_all_velo_tracks": off_all,
+               "dev_offsets_velo_track_hit_number": off_hn[:reco + 1],
+               "dev_velo_track_hits": hits[:ELEMENT_SIZE * TH]}
+        return totals, out, up.value, down.value

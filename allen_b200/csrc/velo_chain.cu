@@ -1,0 +1,755 @@
+// Host side of the C ABI (include/velo_b200.h): geometry and lookup tables, the device
+// workspace, the launch sequence of the chain, CUDA-graph capture and the host-buffer path.
+//
+// Launch sequence for one slice of N events, on the caller's stream, no host sync:
+//   memset(bank index, status)
+//   estimate_kernel        [N CTAs]  velo_calculate_number_of_candidates + velo_estimate_input_size
+//   exclusive_scan_kernel  [2 jobs]  prefix_sum_offsets_velo_candidates, event estimate bases
+//   cluster_sort_kernel    [N CTAs]  velo_masked_clustering + velo_sort_by_phi
+//                                    (+ prefix_sum_offsets_estimated_input_size, per event)
+//   search_by_triplet_kernel [N]     velo_search_by_triplet + velo_three_hit_tracks_filter
+//   exclusive_scan_kernel  [3 jobs]  prefix_sum_offsets_velo_tracks,
+//                                    prefix_sum_offsets_number_of_three_hit_tracks_filtered,
+//                                    per-event track-hit bases
+//   consolidate_kernel     [N CTAs]  velo_copy_track_hit_number + prefix_sum_offsets_velo_track_hit_number
+//                                    + velo_consolidate_tracks
+//   totals_kernel + one 40-byte device-to-host copy of the host scalars.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "velo_b200.h"
+#include "velo_kernels.cuh"
+
+namespace {
+  thread_local std::string last_error;
+
+  VeloStatus fail(VeloStatus s, const std::string& what)
+  {
+    last_error = what;
+    return s;
+  }
+
+#define VELO_CUDA(call)                                                                                 \
+  do {                                                                                                  \
+    const cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) return fail(VELO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+  // ClusteringCommon.cpp:6-104 restated: 8-connected groups of the 2 x 4 super pixel,
+  // seeded in ascending bit order (bit = col * 4 + row); per group the centroid
+  // (row | col << 2, shifted by 4 for the second group), bit 3 set for a second group,
+  // and the fractional centroid offsets.
+  void build_sp_tables(uint8_t* patterns, float* fx, float* fy)
+  {
+    std::memset(patterns, 0, 256);
+    std::memset(fx, 0, 512 * sizeof(float));
+    std::memset(fy, 0, 512 * sizeof(float));
+    for (unsigned sp = 0; sp < 256; ++sp) {
+      unsigned left = sp, clu = 0;
+      for (unsigned seed = 0; seed < 8; ++seed) {
+        if (!(left & (1u << seed))) continue;
+        unsigned group = 1u << seed, before;
+        do {
+          before = group;
+          for (unsigned b = 0; b < 8; ++b) {
+            if (!(left & (1u << b)) || (group & (1u << b))) continue;
+            for (unsigned o = 0; o < 8; ++o) {
+              if (!(group & (1u << o))) continue;
+              const int dc = int(b / 4) - int(o / 4), dr = int(b % 4) - int(o % 4);
+              if (dc >= -1 && dc <= 1 && dr >= -1 && dr <= 1) {
+                group |= 1u << b;
+                break;
+              }
+            }
+          }
+        } while (group != before);
+        left &= ~group;
+        unsigned x = 0, y = 0, n = 0;
+        for (unsigned b = 0; b < 8; ++b)
+          if (group & (1u << b)) {
+            x += b / 4;
+            y += b % 4;
+            ++n;
+          }
+        const unsigned cx = x / n, cy = y / n;
+        fx[2 * sp + clu] = float(x) / float(n) - float(cx);
+        fy[2 * sp + clu] = float(y) / float(n) - float(cy);
+        patterns[sp] |= uint8_t(((cx << 2) | cy) << (4 * clu));
+        patterns[sp] |= uint8_t(clu << 3);
+        ++clu;
+      }
+    }
+  }
+
+  bool parse_geometry(const char* p, size_t size, velo::Geometry& g)
+  {
+    const char* end = p + size;
+    auto read = [&](size_t n, float* dst) {
+      uint64_t count;
+      if (p + 8 > end) return false;
+      std::memcpy(&count, p, 8);
+      p += 8;
+      if (count != n || p + n * 4 > end) return false;
+      std::memcpy(dst, p, n * 4);
+      p += n * 4;
+      return true;
+    };
+    if (!read(velo::n_modules, g.module_zs) || !read(velo::n_cols, g.local_x) || !read(velo::n_cols, g.x_pitch))
+      return false;
+    uint64_t n_ltg, n_trans;
+    if (p + 16 > end) return false;
+    std::memcpy(&n_ltg, p, 8);
+    std::memcpy(&n_trans, p + 8, 8);
+    p += 16;
+    if (n_ltg != velo::n_sensors || n_trans != 12 || p + velo::n_sensors * 12 * 4 > end) return false;
+    std::memcpy(g.ltg, p, velo::n_sensors * 12 * 4);
+    return true;
+  }
+
+  template<typename T>
+  struct DeviceBuffer {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t reserve(size_t count)
+    {
+      if (count <= n && p) return cudaSuccess;
+      if (p) cudaFree(p);
+      p = nullptr;
+      n = 0;
+      const cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+      if (e == cudaSuccess) n = count;
+      return e;
+    }
+    void release()
+    {
+      if (p) cudaFree(p);
+      p = nullptr;
+      n = 0;
+    }
+  };
+
+  struct DeviceTotals {
+    unsigned n_events;
+    unsigned total_clusters;
+    unsigned candidates;
+    unsigned four_hit;
+    unsigned three_hit;
+    unsigned reconstructed;
+    unsigned track_hits;
+    unsigned track_container_size;
+    unsigned flags;
+  };
+
+  __global__ void totals_kernel(
+    unsigned n,
+    const unsigned* event_base,
+    const unsigned* candidates_offsets,
+    const unsigned* offsets_tracks,
+    const unsigned* offsets_three,
+    const unsigned* track_hit_base,
+    const unsigned* status,
+    DeviceTotals* out)
+  {
+    const unsigned T = event_base[n];
+    const float by_clusters = __uint2float_rn(T) * 0.34f;
+    out->n_events = n;
+    out->total_clusters = T;
+    out->candidates = candidates_offsets[n];
+    out->four_hit = offsets_tracks[n];
+    out->three_hit = offsets_three[n];
+    out->reconstructed = offsets_tracks[n] + offsets_three[n];
+    out->track_hits = track_hit_base[n];
+    out->track_container_size = by_clusters < __uint2float_rn(n * velo::minimum_container_size) ?
+                                  n * velo::minimum_container_size :
+                                  static_cast<unsigned>(by_clusters);
+    out->flags = *status;
+  }
+} // namespace
+
+static constexpr unsigned n_timed_kernels = 7;
+static const char* const kernel_names[n_timed_kernels] = {
+  "estimate_kernel", "exclusive_scan_kernel(candidates, estimates)", "cluster_sort_kernel",
+  "search_by_triplet_kernel", "exclusive_scan_kernel(tracks, three-hit, track hits)", "consolidate_kernel",
+  "totals_kernel"};
+
+struct VeloChain {
+  int device = 0;
+  velo::Constants k {};
+  DeviceBuffer<velo::Geometry> geo;
+
+  // capacities
+  unsigned cap_events = 0;
+  size_t cap_clusters = 0; // T
+  size_t cap_tracks = 0;   // track container entries
+  size_t cap_track_hits = 0;
+
+  // launch configuration (autotuned by the Python layer)
+  unsigned estimate_blob_bytes = 32 * 1024;
+  unsigned cluster_blob_bytes = 24 * 1024;
+  unsigned cluster_stage_capacity = 3072;
+  unsigned search_hit_capacity = 2560;
+
+  // workspace
+  DeviceBuffer<unsigned long long> bank_index_key;
+  DeviceBuffer<unsigned> status;
+  DeviceBuffer<unsigned> number_of_candidates, candidates_offsets, estimated, candidate_num, event_estimate,
+    event_base, offsets_est, cluster_num, atomics, n_tracks, offsets_tracks, n_three_out, offsets_three,
+    event_track_hits, event_track_hit_base, offsets_all, track_hit_number, offsets_hit_number;
+  DeviceBuffer<char> sorted, staging, track_hits;
+  DeviceBuffer<velo::TrackHits> tracks;
+  DeviceBuffer<velo::TrackletHits> three_hit, three_out;
+  DeviceBuffer<uint8_t> hit_used, accepted;
+  DeviceBuffer<DeviceTotals> totals_dev;
+  DeviceTotals* totals_host = nullptr;
+  cudaEvent_t done = nullptr;
+  cudaStream_t capture_stream = nullptr; // graphs are captured here (the legacy stream cannot be)
+
+  // host-buffer path
+  DeviceBuffer<char> in_raw;
+  DeviceBuffer<unsigned> in_offsets, in_sizes, in_types;
+
+  // CUDA graphs, one per slice (pointers, event range), with optional per-kernel timing
+  // events captured into them.
+  struct GraphEntry {
+    VeloDeviceSlice key;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev[n_timed_kernels + 1] = {};
+  };
+  std::vector<GraphEntry> graphs;
+  cudaEvent_t direct_ev[n_timed_kernels + 1] = {};
+  bool timing = false;
+  bool direct_timed = false;
+  unsigned last_n = 0;
+
+  void release_graph()
+  {
+    for (auto& g : graphs) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      for (auto& e : g.ev)
+        if (e) cudaEventDestroy(e);
+    }
+    graphs.clear();
+    direct_timed = false;
+  }
+};
+
+namespace {
+  VeloStatus enqueue_chain(VeloChain* c, const VeloDeviceSlice& s, cudaStream_t stream, cudaEvent_t* ev)
+  {
+    using namespace velo;
+    const unsigned n = s.n_events;
+    RawInput in {s.raw, s.offsets, s.sizes, s.types, s.event_start, s.n_events, s.bank_version};
+    unsigned stage = 0;
+    auto mark = [&]() -> cudaError_t { return ev ? cudaEventRecord(ev[stage++], stream) : cudaSuccess; };
+
+    VELO_CUDA(cudaMemsetAsync(c->bank_index_key.p, 0, n_sensors * sizeof(unsigned long long), stream));
+    VELO_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(unsigned), stream));
+    VELO_CUDA(mark());
+
+    EstimateParams ep {};
+    ep.in = in;
+    ep.estimated_input_size = c->estimated.p;
+    ep.number_of_candidates = c->number_of_candidates.p;
+    ep.module_candidate_num = c->candidate_num.p;
+    ep.event_estimate = c->event_estimate.p;
+    ep.bank_index_key = c->bank_index_key.p;
+    ep.designated_stride = (n + 255) / 256;
+    ep.status = c->status.p;
+    ep.smem_blob_bytes = c->estimate_blob_bytes;
+    estimate_kernel<<<n, decode_threads, c->estimate_blob_bytes, stream>>>(ep);
+    VELO_CUDA(cudaGetLastError());
+    VELO_CUDA(mark());
+
+    ScanParams sp1 {};
+    sp1.jobs[0] = {c->event_estimate.p, c->event_base.p, n};
+    sp1.jobs[1] = {c->number_of_candidates.p, c->candidates_offsets.p, n};
+    exclusive_scan_kernel<<<2, scan_threads, 0, stream>>>(sp1);
+    VELO_CUDA(cudaGetLastError());
+    VELO_CUDA(mark());
+
+    ClusterSortParams cp {};
+    cp.in = in;
+    cp.geo = c->geo.p;
+    cp.k = c->k;
+    cp.estimated_input_size = c->estimated.p;
+    cp.event_base = c->event_base.p;
+    cp.bank_index_key = c->bank_index_key.p;
+    cp.offsets_estimated_input_size = c->offsets_est.p;
+    cp.module_cluster_num = c->cluster_num.p;
+    cp.sorted_container = c->sorted.p;
+    cp.staging = c->staging.p;
+    cp.status = c->status.p;
+    cp.smem_blob_bytes = c->cluster_blob_bytes;
+    cp.smem_cluster_capacity = c->cluster_stage_capacity;
+    cp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
+    const unsigned cluster_smem = ((c->cluster_stage_capacity * element_size + 15u) & ~15u) + c->cluster_blob_bytes;
+    cluster_sort_kernel<<<n, decode_threads, cluster_smem, stream>>>(cp);
+    VELO_CUDA(cudaGetLastError());
+    VELO_CUDA(mark());
+
+    SearchParams sp {};
+    sp.geo = c->geo.p;
+    sp.k = c->k;
+    sp.n_events = n;
+    sp.offsets_estimated_input_size = c->offsets_est.p;
+    sp.module_cluster_num = c->cluster_num.p;
+    sp.sorted_container = c->sorted.p;
+    sp.track_capacity = static_cast<unsigned>(c->cap_tracks);
+    sp.tracks = c->tracks.p;
+    sp.three_hit_tracks = c->three_hit.p;
+    sp.hit_used = reinterpret_cast<bool*>(c->hit_used.p);
+    sp.atomics_velo = c->atomics.p;
+    sp.number_of_velo_tracks = c->n_tracks.p;
+    sp.three_hit_tracks_output = c->three_out.p;
+    sp.number_of_three_hit_tracks_output = c->n_three_out.p;
+    sp.event_track_hits = c->event_track_hits.p;
+    sp.status = c->status.p;
+    sp.smem_hit_capacity = c->search_hit_capacity;
+    sp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
+    const unsigned search_smem = ((c->search_hit_capacity * element_size + 15u) & ~15u) + c->search_hit_capacity;
+    search_by_triplet_kernel<<<n, search_threads, search_smem, stream>>>(sp);
+    VELO_CUDA(cudaGetLastError());
+    VELO_CUDA(mark());
+
+    ScanParams sp2 {};
+    sp2.jobs[0] = {c->n_tracks.p, c->offsets_tracks.p, n};
+    sp2.jobs[1] = {c->n_three_out.p, c->offsets_three.p, n};
+    sp2.jobs[2] = {c->event_track_hits.p, c->event_track_hit_base.p, n};
+    exclusive_scan_kernel<<<3, scan_threads, 0, stream>>>(sp2);
+    VELO_CUDA(cudaGetLastError());
+    VELO_CUDA(mark());
+
+    ConsolidateParams kp {};
+    kp.n_events = n;
+    kp.offsets_estimated_input_size = c->offsets_est.p;
+    kp.sorted_container = c->sorted.p;
+    kp.tracks = c->tracks.p;
+    kp.three_hit_tracks_output = c->three_out.p;
+    kp.offsets_velo_tracks = c->offsets_tracks.p;
+    kp.offsets_three_hit = c->offsets_three.p;
+    kp.event_track_hit_base = c->event_track_hit_base.p;
+    kp.offsets_all_velo_tracks = c->offsets_all.p;
+    kp.velo_track_hit_number = c->track_hit_number.p;
+    kp.offsets_velo_track_hit_number = c->offsets_hit_number.p;
+    kp.velo_track_hits = c->track_hits.p;
+    kp.accepted_velo_tracks = reinterpret_cast<bool*>(c->accepted.p);
+    kp.track_capacity = static_cast<unsigned>(c->cap_tracks);
+    kp.track_hit_capacity = static_cast<unsigned>(c->cap_track_hits);
+    kp.track_container_capacity = static_cast<unsigned>(c->cap_tracks);
+    kp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
+    kp.status = c->status.p;
+    consolidate_kernel<<<n, consolidate_threads, 0, stream>>>(kp);
+    VELO_CUDA(cudaGetLastError());
+    VELO_CUDA(mark());
+
+    totals_kernel<<<1, 1, 0, stream>>>(
+      n,
+      c->event_base.p,
+      c->candidates_offsets.p,
+      c->offsets_tracks.p,
+      c->offsets_three.p,
+      c->event_track_hit_base.p,
+      c->status.p,
+      c->totals_dev.p);
+    VELO_CUDA(cudaGetLastError());
+    VELO_CUDA(mark());
+    VELO_CUDA(cudaMemcpyAsync(c->totals_host, c->totals_dev.p, sizeof(DeviceTotals), cudaMemcpyDeviceToHost, stream));
+    return VELO_OK;
+  }
+
+  VeloStatus configure_kernels(VeloChain* c)
+  {
+    using namespace velo;
+    const int cluster_smem = int(((c->cluster_stage_capacity * element_size + 15u) & ~15u) + c->cluster_blob_bytes);
+    const int search_smem = int(((c->search_hit_capacity * element_size + 15u) & ~15u) + c->search_hit_capacity);
+    VELO_CUDA(cudaFuncSetAttribute(estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c->estimate_blob_bytes)));
+    VELO_CUDA(cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cluster_smem));
+    VELO_CUDA(cudaFuncSetAttribute(search_by_triplet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, search_smem));
+    return VELO_OK;
+  }
+} // namespace
+
+extern "C" {
+
+const char* velo_last_error_string(void) { return last_error.c_str(); }
+
+void velo_default_properties(VeloChainProperties* props)
+{
+  props->phi_tolerance = 0.045f;
+  props->max_scatter = 0.08f;
+  props->max_skipped_modules = 1;
+  props->max_chi2 = 20.0f;
+}
+
+VeloStatus velo_device_check(void)
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(VELO_ERR_NO_DEVICE, "no CUDA device");
+  cudaDeviceProp prop {};
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return fail(VELO_ERR_NO_DEVICE, "cannot query the device");
+  if (prop.major != 10) return fail(VELO_ERR_NO_DEVICE, std::string("sm_100 required, found ") + prop.name);
+  cudaFuncAttributes attr {};
+  if (cudaFuncGetAttributes(&attr, velo::search_by_triplet_kernel) != cudaSuccess)
+    return fail(VELO_ERR_NO_DEVICE, "kernels not loadable on this device");
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_create(
+  const void* geometry, size_t geometry_size, const VeloChainProperties* props, VeloChain** out)
+{
+  if (!geometry || !out) return fail(VELO_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  const VeloStatus dev_ok = velo_device_check();
+  if (dev_ok != VELO_OK) return dev_ok;
+  velo::Geometry g {};
+  if (!parse_geometry(static_cast<const char*>(geometry), geometry_size, g))
+    return fail(VELO_ERR_ARGUMENT, "malformed velo geometry blob");
+  build_sp_tables(g.sp_patterns, g.sp_fx, g.sp_fy);
+
+  VeloChainProperties pr;
+  velo_default_properties(&pr);
+  if (props) pr = *props;
+
+  auto* c = new VeloChain;
+  cudaGetDevice(&c->device);
+  // IEEE single-precision constants, as the reference's constexpr values (VeloTools.cuh:18-63)
+  const float pi_f = 3.141592654f;
+  c->k.convert_factor_i16 = 32768.f / pi_f;
+  c->k.c1 = .25f * pi_f;
+  c->k.c2 = .75f * pi_f;
+  c->k.max_scatter = pr.max_scatter;
+  c->k.max_chi2 = pr.max_chi2;
+  c->k.max_skipped_modules = pr.max_skipped_modules;
+  // hit_phi_float_to_16 (VeloTools.cuh:55-60): float -> int16 through int32
+  c->k.phi_tolerance_i16 = static_cast<int16_t>(static_cast<int32_t>(pr.phi_tolerance * c->k.convert_factor_i16));
+
+  auto cleanup = [&](VeloStatus s) {
+    velo_chain_destroy(c);
+    return s;
+  };
+  if (c->geo.reserve(1) != cudaSuccess) return cleanup(fail(VELO_ERR_CUDA, "geometry allocation failed"));
+  if (cudaMemcpy(c->geo.p, &g, sizeof(g), cudaMemcpyHostToDevice) != cudaSuccess)
+    return cleanup(fail(VELO_ERR_CUDA, "geometry upload failed"));
+  if (c->bank_index_key.reserve(velo::n_sensors) != cudaSuccess || c->status.reserve(1) != cudaSuccess ||
+      c->totals_dev.reserve(1) != cudaSuccess)
+    return cleanup(fail(VELO_ERR_CUDA, "allocation failed"));
+  if (cudaMallocHost(&c->totals_host, sizeof(DeviceTotals)) != cudaSuccess)
+    return cleanup(fail(VELO_ERR_CUDA, "pinned allocation failed"));
+  std::memset(c->totals_host, 0, sizeof(DeviceTotals));
+  if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess)
+    return cleanup(fail(VELO_ERR_CUDA, "event creation failed"));
+  if (cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(VELO_ERR_CUDA, "stream creation failed"));
+  const VeloStatus cfg = configure_kernels(c);
+  if (cfg != VELO_OK) return cleanup(cfg);
+  *out = c;
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_reserve(
+  VeloChain* c, unsigned max_events, unsigned long long max_super_pixels, unsigned long long max_raw_bytes)
+{
+  if (!c || max_events == 0) return fail(VELO_ERR_ARGUMENT, "bad reserve arguments");
+  c->release_graph();
+  const size_t n = max_events;
+  // every super pixel yields at most two estimated clusters (EstimateInputSize.cu:66,176-203)
+  const size_t T = 2 * size_t(max_super_pixels) + 64;
+  if (T > 0xFFFFFFFFull / velo::element_size) return fail(VELO_ERR_CAPACITY, "slice too large for 32-bit offsets");
+  const size_t tracks = std::max<size_t>(size_t(double(T) * 0.34) + 64, n * velo::minimum_container_size + 64);
+  const size_t track_hits = T;
+  c->cap_events = max_events;
+  c->cap_clusters = T;
+  c->cap_tracks = tracks;
+  c->cap_track_hits = track_hits;
+#define RES(buf, count)                                                        \
+  if ((buf).reserve(count) != cudaSuccess) return fail(VELO_ERR_CUDA, "workspace allocation failed: " #buf);
+  RES(c->number_of_candidates, n)
+  RES(c->candidates_offsets, n + 1)
+  RES(c->estimated, 26 * n)
+  RES(c->candidate_num, n)
+  RES(c->event_estimate, n)
+  RES(c->event_base, n + 1)
+  RES(c->offsets_est, 26 * n + 1)
+  RES(c->cluster_num, 26 * n)
+  RES(c->atomics, 3 * n)
+  RES(c->n_tracks, n)
+  RES(c->offsets_tracks, n + 1)
+  RES(c->n_three_out, n)
+  RES(c->offsets_three, n + 1)
+  RES(c->event_track_hits, n)
+  RES(c->event_track_hit_base, n + 1)
+  RES(c->offsets_all, n + 1)
+  RES(c->track_hit_number, tracks)
+  RES(c->offsets_hit_number, tracks + 1)
+  RES(c->sorted, velo::element_size * T)
+  RES(c->staging, 20 * T)
+  RES(c->track_hits, velo::element_size * track_hits)
+  RES(c->tracks, tracks)
+  RES(c->three_hit, tracks)
+  RES(c->three_out, tracks)
+  RES(c->hit_used, T)
+  RES(c->accepted, 2 * tracks)
+  if (max_raw_bytes) {
+    RES(c->in_raw, max_raw_bytes + 16)
+  }
+#undef RES
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_run(VeloChain* c, const VeloDeviceSlice* s, VeloStream stream_, int use_graph)
+{
+  if (!c || !s || !s->raw || !s->offsets || !s->sizes || !s->types) return fail(VELO_ERR_ARGUMENT, "null argument");
+  if (s->bank_version != 2 && s->bank_version != 3 && s->bank_version != 4)
+    return fail(VELO_ERR_ARGUMENT, "VELO SP bank version not supported (" + std::to_string(s->bank_version) + ")");
+  if (s->n_events == 0) return fail(VELO_ERR_ARGUMENT, "empty slice");
+  if (s->n_events > c->cap_events) return fail(VELO_ERR_CAPACITY, "slice has more events than reserved");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  c->last_n = s->n_events;
+  if (!use_graph) {
+    if (c->timing && !c->direct_ev[0])
+      for (auto& e : c->direct_ev)
+        VELO_CUDA(cudaEventCreate(&e));
+    const VeloStatus st = enqueue_chain(c, *s, stream, c->timing ? c->direct_ev : nullptr);
+    if (st != VELO_OK) return st;
+    c->direct_timed = c->timing;
+    VELO_CUDA(cudaEventRecord(c->done, stream));
+    return VELO_OK;
+  }
+  VeloChain::GraphEntry* entry = nullptr;
+  for (auto& g : c->graphs) {
+    const VeloDeviceSlice& k = g.key;
+    if (k.raw == s->raw && k.offsets == s->offsets && k.sizes == s->sizes && k.types == s->types &&
+        k.event_start == s->event_start && k.n_events == s->n_events && k.bank_version == s->bank_version) {
+      entry = &g;
+      break;
+    }
+  }
+  if (!entry) {
+    if (c->graphs.size() >= 64) c->release_graph();
+    c->graphs.emplace_back();
+    entry = &c->graphs.back();
+    entry->key = *s;
+    if (c->timing)
+      for (auto& e : entry->ev)
+        VELO_CUDA(cudaEventCreate(&e));
+    cudaGraph_t graph;
+    VELO_CUDA(cudaStreamBeginCapture(c->capture_stream, cudaStreamCaptureModeThreadLocal));
+    const VeloStatus st = enqueue_chain(c, *s, c->capture_stream, c->timing ? entry->ev : nullptr);
+    const cudaError_t end = cudaStreamEndCapture(c->capture_stream, &graph);
+    if (st != VELO_OK) {
+      c->graphs.pop_back();
+      return st;
+    }
+    if (end != cudaSuccess) {
+      c->graphs.pop_back();
+      return fail(VELO_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(end));
+    }
+    const cudaError_t inst = cudaGraphInstantiate(&entry->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (inst != cudaSuccess) {
+      c->graphs.pop_back();
+      return fail(VELO_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(inst));
+    }
+  }
+  VELO_CUDA(cudaGraphLaunch(entry->exec, stream));
+  VELO_CUDA(cudaEventRecord(c->done, stream));
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_set_timing(VeloChain* c, int enable)
+{
+  if (!c) return fail(VELO_ERR_ARGUMENT, "null chain");
+  if (bool(enable) != c->timing) c->release_graph();
+  c->timing = enable != 0;
+  return VELO_OK;
+}
+
+unsigned velo_chain_kernel_count(void) { return n_timed_kernels; }
+
+const char* velo_chain_kernel_name(unsigned i) { return i < n_timed_kernels ? kernel_names[i] : ""; }
+
+VeloStatus velo_chain_kernel_times(VeloChain* c, float* ms_sum, unsigned* n_runs)
+{
+  if (!c || !ms_sum) return fail(VELO_ERR_ARGUMENT, "null argument");
+  for (unsigned k = 0; k < n_timed_kernels; ++k)
+    ms_sum[k] = 0.f;
+  unsigned runs = 0;
+  auto add = [&](cudaEvent_t* ev) -> VeloStatus {
+    for (unsigned k = 0; k < n_timed_kernels; ++k) {
+      float ms = 0.f;
+      VELO_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      ms_sum[k] += ms;
+    }
+    ++runs;
+    return VELO_OK;
+  };
+  VELO_CUDA(cudaEventSynchronize(c->done));
+  for (auto& g : c->graphs)
+    if (g.ev[0]) {
+      const VeloStatus st = add(g.ev);
+      if (st != VELO_OK) return st;
+    }
+  if (c->direct_timed) {
+    const VeloStatus st = add(c->direct_ev);
+    if (st != VELO_OK) return st;
+  }
+  if (n_runs) *n_runs = runs;
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_synchronize(VeloChain* c, VeloChainTotals* t)
+{
+  if (!c) return fail(VELO_ERR_ARGUMENT, "null chain");
+  VELO_CUDA(cudaEventSynchronize(c->done));
+  const DeviceTotals& d = *c->totals_host;
+  if (t) {
+    t->n_events = d.n_events;
+    t->host_total_number_of_velo_clusters = d.total_clusters;
+    t->host_number_of_cluster_candidates = d.candidates;
+    t->host_number_of_velo_tracks_at_least_four_hits = d.four_hit;
+    t->host_number_of_three_hit_tracks_filtered = d.three_hit;
+    t->host_number_of_reconstructed_velo_tracks = d.reconstructed;
+    t->host_accumulated_number_of_hits_in_velo_tracks = d.track_hits;
+    t->track_container_size = d.track_container_size;
+    t->device_flags = d.flags;
+  }
+  if (d.flags) return fail(VELO_ERR_DEVICE_FLAGS, "device flags raised: " + std::to_string(d.flags));
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_outputs(const VeloChain* c, VeloChainOutputs* o)
+{
+  if (!c || !o) return fail(VELO_ERR_ARGUMENT, "null argument");
+  o->dev_number_of_candidates = c->number_of_candidates.p;
+  o->dev_estimated_input_size = c->estimated.p;
+  o->dev_module_candidate_num = c->candidate_num.p;
+  o->dev_offsets_estimated_input_size = c->offsets_est.p;
+  o->dev_module_cluster_num = c->cluster_num.p;
+  o->dev_sorted_velo_cluster_container = c->sorted.p;
+  o->dev_tracks = c->tracks.p;
+  o->dev_three_hit_tracks = c->three_hit.p;
+  o->dev_hit_used = c->hit_used.p;
+  o->dev_atomics_velo = c->atomics.p;
+  o->dev_number_of_velo_tracks = c->n_tracks.p;
+  o->dev_offsets_velo_tracks = c->offsets_tracks.p;
+  o->dev_three_hit_tracks_output = c->three_out.p;
+  o->dev_number_of_three_hit_tracks_output = c->n_three_out.p;
+  o->dev_offsets_number_of_three_hit_tracks_filtered = c->offsets_three.p;
+  o->dev_offsets_all_velo_tracks = c->offsets_all.p;
+  o->dev_velo_track_hit_number = c->track_hit_number.p;
+  o->dev_offsets_velo_track_hit_number = c->offsets_hit_number.p;
+  o->dev_velo_track_hits = c->track_hits.p;
+  o->dev_accepted_velo_tracks = c->accepted.p;
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_run_host(
+  VeloChain* c,
+  const VeloHostSlice* s,
+  VeloStream stream_,
+  unsigned* host_offsets_all,
+  size_t offsets_all_capacity,
+  unsigned* host_offsets_hit_number,
+  size_t offsets_hit_number_capacity,
+  char* host_track_hits,
+  size_t track_hits_capacity,
+  VeloChainTotals* totals,
+  unsigned long long* h2d_bytes,
+  unsigned long long* d2h_bytes)
+{
+  if (!c || !s || !s->raw || !s->offsets || !s->sizes || !s->types) return fail(VELO_ERR_ARGUMENT, "null argument");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  const size_t n = s->n_events;
+  if (c->in_raw.reserve(s->raw_bytes + 16) != cudaSuccess || c->in_offsets.reserve(n + 1) != cudaSuccess ||
+      c->in_sizes.reserve(s->sizes_bytes / 4 + 1) != cudaSuccess || c->in_types.reserve(s->types_bytes / 4 + 1) != cudaSuccess)
+    return fail(VELO_ERR_CUDA, "input staging allocation failed");
+  VELO_CUDA(cudaMemcpyAsync(c->in_raw.p, s->raw, s->raw_bytes, cudaMemcpyHostToDevice, stream));
+  VELO_CUDA(cudaMemcpyAsync(c->in_offsets.p, s->offsets, (n + 1) * sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+  VELO_CUDA(cudaMemcpyAsync(c->in_sizes.p, s->sizes, s->sizes_bytes, cudaMemcpyHostToDevice, stream));
+  VELO_CUDA(cudaMemcpyAsync(c->in_types.p, s->types, s->types_bytes, cudaMemcpyHostToDevice, stream));
+  unsigned long long up = s->raw_bytes + (n + 1) * sizeof(unsigned) + s->sizes_bytes + s->types_bytes;
+  VeloDeviceSlice ds {c->in_raw.p, c->in_offsets.p, c->in_sizes.p, c->in_types.p, 0, s->n_events, s->bank_version};
+  VeloStatus st = velo_chain_run(c, &ds, stream, 1);
+  if (st != VELO_OK) return st;
+  VeloChainTotals t {};
+  st = velo_chain_synchronize(c, &t);
+  if (totals) *totals = t;
+  if (st != VELO_OK) return st;
+  const size_t n_tracks = t.host_number_of_reconstructed_velo_tracks;
+  const size_t b_all = (n + 1) * sizeof(unsigned);
+  const size_t b_hn = (n_tracks + 1) * sizeof(unsigned);
+  const size_t b_hits = size_t(t.host_accumulated_number_of_hits_in_velo_tracks) * velo::element_size;
+  if (b_all > offsets_all_capacity || b_hn > offsets_hit_number_capacity || b_hits > track_hits_capacity)
+    return fail(VELO_ERR_CAPACITY, "host output buffers too small");
+  VELO_CUDA(cudaMemcpyAsync(host_offsets_all, c->offsets_all.p, b_all, cudaMemcpyDeviceToHost, stream));
+  VELO_CUDA(cudaMemcpyAsync(host_offsets_hit_number, c->offsets_hit_number.p, b_hn, cudaMemcpyDeviceToHost, stream));
+  VELO_CUDA(cudaMemcpyAsync(host_track_hits, c->track_hits.p, b_hits, cudaMemcpyDeviceToHost, stream));
+  VELO_CUDA(cudaStreamSynchronize(stream));
+  if (h2d_bytes) *h2d_bytes = up;
+  if (d2h_bytes) *d2h_bytes = b_all + b_hn + b_hits + sizeof(DeviceTotals);
+  return VELO_OK;
+}
+
+VeloStatus velo_copy_to_host(void* host, const void* device, size_t bytes)
+{
+  VELO_CUDA(cudaMemcpy(host, device, bytes, cudaMemcpyDeviceToHost));
+  return VELO_OK;
+}
+
+VeloStatus velo_copy_to_device(void* device, const void* host, size_t bytes)
+{
+  VELO_CUDA(cudaMemcpy(device, host, bytes, cudaMemcpyHostToDevice));
+  return VELO_OK;
+}
+
+void velo_chain_destroy(VeloChain* c)
+{
+  if (!c) return;
+  c->release_graph();
+  for (auto& e : c->direct_ev)
+    if (e) cudaEventDestroy(e);
+  c->geo.release();
+  c->bank_index_key.release();
+  c->status.release();
+  c->number_of_candidates.release();
+  c->candidates_offsets.release();
+  c->estimated.release();
+  c->candidate_num.release();
+  c->event_estimate.release();
+  c->event_base.release();
+  c->offsets_est.release();
+  c->cluster_num.release();
+  c->atomics.release();
+  c->n_tracks.release();
+  c->offsets_tracks.release();
+  c->n_three_out.release();
+  c->offsets_three.release();
+  c->event_track_hits.release();
+  c->event_track_hit_base.release();
+  c->offsets_all.release();
+  c->track_hit_number.release();
+  c->offsets_hit_number.release();
+  c->sorted.release();
+  c->staging.release();
+  c->track_hits.release();
+  c->tracks.release();
+  c->three_hit.release();
+  c->three_out.release();
+  c->hit_used.release();
+  c->accepted.release();
+  c->totals_dev.release();
+  c->in_raw.release();
+  c->in_offsets.release();
+  c->in_sizes.release();
+  c->in_types.release();
+  if (c->totals_host) cudaFreeHost(c->totals_host);
+  if (c->done) cudaEventDestroy(c->done);
+  if (c->capture_stream) cudaStreamDestroy(c->capture_stream);
+  delete c;
+}
+
+} // extern "C"

@@ -1,0 +1,206 @@
+// Device-side definitions shared by the VELO kernels (sm_100a).
+//
+// Layout contract (identical to the reference so that the buffers drop into an
+// Allen sequence): the cluster container of VeloEventModel.cuh:92-189 with FP32
+// coordinates (the reference CPU build's half_t == float), 18 bytes per hit:
+//   u32 id[T] | f32 xyz[3T] interleaved | i16 phi[T],   T = total estimated clusters.
+// Track hits (Velo::TrackHits, VeloEventModel.cuh:67-86): u16 hits[26], u8 hitsNum,
+// one padding byte = 54 bytes.  Three-hit tracklets: u16 hits[3] = 6 bytes.
+//
+// All floating point in this library is compiled with -fmad=false: every multiply
+// and add rounds separately, in the reference's expression order, so positions,
+// phi values and fits are bit-identical to the reference CPU build.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace velo {
+
+  constexpr unsigned n_modules = 52;
+  constexpr unsigned n_module_pairs = 26;
+  constexpr unsigned n_sensors = 208;
+  constexpr unsigned n_cols = 768;
+  constexpr unsigned max_track_size = 26;
+  constexpr unsigned max_tracks_to_follow = 2048;
+  constexpr unsigned minimum_container_size = 10;
+  constexpr unsigned element_size = 18;
+  constexpr unsigned bank_type_velo = 8;
+  constexpr unsigned bank_type_vp = 63;
+
+  // Error flags (bit set in the chain's device status word; read by the host after a run).
+  enum ErrorBits : unsigned {
+    err_cluster_capacity = 1u << 0,  // more clusters than the estimate reserved for a module pair
+    err_track_capacity = 1u << 1,    // an event produced more tracks than its container slice
+    err_ttf_overflow = 1u << 2,      // more than 2048 tracks in flight in one event
+    err_bad_sensor = 1u << 3,        // a candidate names a sensor outside the geometry
+    err_bulk_copy_timeout = 1u << 4, // a bulk copy into shared memory did not complete in time
+    err_output_capacity = 1u << 5,   // consolidated output larger than the reserved buffer
+    err_input_capacity = 1u << 6,    // slice larger than the reserved workspace
+    err_hits_per_event = 1u << 7,    // more than 65535 estimated hits in one event (u16 indices)
+  };
+
+  // Detector description and super-pixel lookup tables, one copy in global memory
+  // (read through the read-only cache: sensors and patterns differ across a warp).
+  struct Geometry {
+    float module_zs[n_modules];
+    float local_x[n_cols];
+    float x_pitch[n_cols];
+    float ltg[n_sensors * 12];
+    uint8_t sp_patterns[256];
+    float sp_fx[512];
+    float sp_fy[512];
+  };
+
+  // Scalars computed once on the host (IEEE single precision, as the reference's
+  // constexpr values and properties), passed by value to the kernels.
+  struct Constants {
+    float convert_factor_i16; // 2^15 / pi
+    float c1;                 // pi / 4
+    float c2;                 // 3 pi / 4
+    float max_scatter;
+    float max_chi2;
+    int phi_tolerance_i16;
+    unsigned max_skipped_modules;
+  };
+
+  struct TrackHits {
+    uint16_t hits[max_track_size];
+    uint8_t hits_num;
+    uint8_t pad;
+  };
+  static_assert(sizeof(TrackHits) == 54, "TrackHits layout");
+
+  struct TrackletHits {
+    uint16_t hits[3];
+  };
+  static_assert(sizeof(TrackletHits) == 6, "TrackletHits layout");
+
+  // ---------------------------------------------------------------------------------
+  // phi (VeloTools.cuh:18-63): approximate atan2 scaled to int16.
+  // ---------------------------------------------------------------------------------
+  __device__ __forceinline__ float fast_atan2f(const Constants& k, float y, float x)
+  {
+    const float abs_y = fabsf(y);
+    const float x_plus_y = x + abs_y;
+    const float x_sub_y = x - abs_y;
+    const float y_sub_x = abs_y - x;
+    const float nom = (x > 0) ? x_sub_y : x_plus_y;
+    const float den = (x > 0) ? x_plus_y : y_sub_x;
+    const float r = __fdiv_rn(nom, den);
+    const float angle = ((x > 0) ? k.c1 : k.c2) - k.c1 * r;
+    return copysignf(angle, y);
+  }
+
+  // float -> int16 through a 32-bit truncation (the reference's x86 conversion:
+  // values in (-2^31, 2^31) truncate identically, NaN gives 0 on both).
+  __device__ __forceinline__ int16_t float_to_i16(float v) { return static_cast<int16_t>(__float2int_rz(v)); }
+
+  __device__ __forceinline__ int16_t hit_phi_16(const Constants& k, float x, float y)
+  {
+    return float_to_i16(fast_atan2f(k, y, x) * k.convert_factor_i16);
+  }
+
+  // BinarySearch.cuh:15-30
+  __device__ __forceinline__ int binary_search_leftmost(const int16_t* a, unsigned n, int16_t value)
+  {
+    int l = 0, r = static_cast<int>(n);
+    while (l < r) {
+      const int m = (l + r) / 2;
+      if (value > a[m]) l = m + 1;
+      else r = m;
+    }
+    return l;
+  }
+
+  // VeloEventModel.cuh:192-196
+  __device__ __forceinline__ unsigned track_offset(const unsigned* offsets_est, unsigned event)
+  {
+    return static_cast<unsigned>(__uint2float_rn(offsets_est[event * n_module_pairs]) * 0.34f);
+  }
+
+  __device__ __forceinline__ uint32_t lhcb_id(uint32_t cid) { return (2u << 28) | (cid & 0x0FFFFFFFu); }
+
+  __device__ __forceinline__ uint32_t channel_id(uint32_t sensor, uint32_t chip, uint32_t col, uint32_t row)
+  {
+    return (sensor << 18) | (chip << 16) | (col << 8) | row;
+  }
+
+  // Cluster container view over a base pointer (global or shared memory alike).
+  struct ClusterView {
+    char* base;
+    unsigned total;
+    __device__ __forceinline__ uint32_t& id(unsigned i) const { return reinterpret_cast<uint32_t*>(base)[i]; }
+    __device__ __forceinline__ float& x(unsigned i) const { return reinterpret_cast<float*>(base)[total + 3 * i]; }
+    __device__ __forceinline__ float& y(unsigned i) const { return reinterpret_cast<float*>(base)[total + 3 * i + 1]; }
+    __device__ __forceinline__ float& z(unsigned i) const { return reinterpret_cast<float*>(base)[total + 3 * i + 2]; }
+    __device__ __forceinline__ int16_t& phi(unsigned i) const
+    {
+      return reinterpret_cast<int16_t*>(base)[8u * total + i];
+    }
+    __device__ __forceinline__ int16_t* phi_begin() const { return reinterpret_cast<int16_t*>(base) + 8u * total; }
+  };
+
+  // ---------------------------------------------------------------------------------
+  // Raw event access (Allen layout; ClusteringDefinitions.cuh:61-144, MEPTools.h:26-53)
+  // ---------------------------------------------------------------------------------
+  struct RawInput {
+    const char* raw;
+    const unsigned* offsets;
+    const unsigned* sizes;
+    const unsigned* types;
+    unsigned event_start;
+    unsigned n_events;
+    int bank_version;
+  };
+
+  __device__ __forceinline__ const uint16_t* bank_sizes(const RawInput& in, unsigned event)
+  {
+    return reinterpret_cast<const uint16_t*>(in.sizes) + in.sizes[event];
+  }
+  __device__ __forceinline__ const uint8_t* bank_types(const RawInput& in, unsigned event)
+  {
+    return reinterpret_cast<const uint8_t*>(in.types) + in.types[event];
+  }
+
+  // ---------------------------------------------------------------------------------
+  // Block-wide helpers
+  // ---------------------------------------------------------------------------------
+  // Exclusive scan of one value per thread over the block (blockDim.x a multiple of 32,
+  // at most 1024).  `warp_sums` needs 33 entries of shared memory.  Returns the exclusive
+  // prefix; *total receives the block total.
+  __device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* warp_sums, unsigned* total)
+  {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned warp = threadIdx.x >> 5;
+    const unsigned n_warps = blockDim.x >> 5;
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= static_cast<unsigned>(o)) incl += t;
+    }
+    __syncthreads();
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      unsigned s = lane < n_warps ? warp_sums[lane] : 0u;
+      unsigned si = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xFFFFFFFFu, si, o);
+        if (lane >= static_cast<unsigned>(o)) si += t;
+      }
+      warp_sums[lane] = si - s;
+      if (lane == 31) warp_sums[32] = si;
+    }
+    __syncthreads();
+    const unsigned result = warp_sums[warp] + incl - v;
+    *total = warp_sums[32];
+    __syncthreads();
+    return result;
+  }
+
+  __device__ __forceinline__ void set_error(unsigned* status, unsigned bit) { atomicOr(status, bit); }
+
+} // namespace velo

@@ -1,0 +1,709 @@
+// VELO super-pixel decoding on sm_100a: candidate counting and input-size estimate
+// (velo_calculate_number_of_candidates + velo_estimate_input_size), masked clustering,
+// phi and the sort by phi (velo_masked_clustering + velo_sort_by_phi), one event per CTA.
+//
+// Each CTA stages its event's raw blob (bank offsets + SP words) into shared memory
+// with one bulk copy through the TMA engine (cp.async.bulk, 16-byte aligned span, the
+// ragged tail by plain loads), so the O(n_sp^2) neighbour scans of the reference
+// (EstimateInputSize.cu:111-141, MaskedVeloClustering.cu:361-402) run out of shared
+// memory.  Work is spread one thread per super pixel over the flattened bank list.
+//
+// The sorted container is independent of the order in which clusters are produced
+// (rank by (phi, id), SortByPhi.cu:104-122), so clusters are appended to their module
+// pair with shared-memory atomics and ranked in place; no unsorted container is written.
+#include "velo_kernels.cuh"
+
+namespace velo {
+
+  constexpr unsigned max_banks = 512;
+
+  // ------------------------------------------------------------------------------------
+  // Bulk copy (TMA engine) into shared memory, completion tracked by an mbarrier.
+  // ------------------------------------------------------------------------------------
+  __device__ __forceinline__ uint32_t smem_u32(const void* p)
+  {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+  }
+
+  __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+  {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+
+  __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+  {
+    uint64_t state;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                 : "=l"(state)
+                 : "r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    (void) state;
+  }
+
+  __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+  {
+    asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src),
+      "r"(bytes),
+      "r"(smem_u32(bar))
+      : "memory");
+  }
+
+  __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase)
+  {
+    uint32_t done;
+    asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+    return done != 0;
+  }
+
+  constexpr unsigned bulk_wait_limit = 1u << 22; // try_wait rounds before giving up
+
+  // Stages the event blob into `smem_blob` (16-byte aligned) when it fits; returns the
+  // address of the event's first word (shared or global) and its length in words.
+  // Ends with a __syncthreads().  `bar` must have been initialised with count 1.
+  __device__ const uint32_t* stage_event(
+    const RawInput& in,
+    unsigned ev,
+    unsigned char* smem_blob,
+    unsigned smem_blob_bytes,
+    uint64_t* bar,
+    unsigned* status,
+    unsigned& n_words)
+  {
+    const unsigned begin = in.offsets[ev];
+    const unsigned end = in.offsets[ev + 1];
+    n_words = (end - begin) / 4;
+    const char* src = in.raw + begin;
+    const uintptr_t s = reinterpret_cast<uintptr_t>(src);
+    const uintptr_t e = s + (end - begin);
+    const uintptr_t s_al = s & ~uintptr_t(15);
+    const uintptr_t e_al = e & ~uintptr_t(15);
+    const unsigned need = static_cast<unsigned>(((e + 15) & ~uintptr_t(15)) - s_al);
+    const bool base_aligned = (reinterpret_cast<uintptr_t>(in.raw) & 15u) == 0;
+    if (!base_aligned || need > smem_blob_bytes) {
+      __syncthreads();
+      return reinterpret_cast<const uint32_t*>(src);
+    }
+    const unsigned bulk = e_al > s_al ? static_cast<unsigned>(e_al - s_al) : 0u;
+    if (threadIdx.x == 0 && bulk > 0) {
+      mbar_expect_tx(bar, bulk);
+      bulk_copy_g2s(smem_blob, reinterpret_cast<const void*>(s_al), bulk, bar);
+    }
+    // ragged tail (whole 32-bit words) by plain loads
+    const uintptr_t tail = e_al > s ? e_al : s;
+    for (uintptr_t a = tail + 4 * threadIdx.x; a < e; a += 4 * blockDim.x) {
+      *reinterpret_cast<uint32_t*>(smem_blob + (a - s_al)) = *reinterpret_cast<const uint32_t*>(a);
+    }
+    bool ok = true;
+    if (bulk > 0) {
+      unsigned rounds = 0;
+      while (!mbar_try_wait(bar, 0)) {
+        if (++rounds > bulk_wait_limit) {
+          ok = false;
+          break;
+        }
+      }
+    }
+    __syncthreads();
+    if (!ok) {
+      if (threadIdx.x == 0) set_error(status, err_bulk_copy_timeout);
+      return reinterpret_cast<const uint32_t*>(src);
+    }
+    return reinterpret_cast<const uint32_t*>(smem_blob + (s - s_al));
+  }
+
+  // ------------------------------------------------------------------------------------
+  // Bank table of one event (ClusteringDefinitions.cuh:61-144)
+  // ------------------------------------------------------------------------------------
+  struct BankTable {
+    unsigned n_banks;
+    unsigned total_sp;
+    unsigned count_total;
+    unsigned words_off[max_banks]; // first SP word of the bank, in words from the event start
+    unsigned n_sp[max_banks];      // SP words of the bank (any bank type)
+    unsigned flat[max_banks + 1];  // exclusive scan of n_sp over VP/Velo banks
+    unsigned source_id[max_banks];
+    uint8_t velo[max_banks];
+  };
+
+  __device__ __forceinline__ unsigned bank_module_pair(unsigned source_id, int version)
+  {
+    return (version == 2 || version == 3) ? (source_id & 0x1FFu) / 8 : ((source_id & 0x1FFu) << 1) / 8;
+  }
+
+  // Fills the table; ends with a __syncthreads().
+  __device__ void parse_banks(
+    const RawInput& in,
+    unsigned ev,
+    const uint32_t* words,
+    unsigned n_words,
+    BankTable& bt,
+    unsigned* warp_sums,
+    unsigned* status)
+  {
+    const bool v23 = in.bank_version == 2 || in.bank_version == 3;
+    const unsigned n_banks_raw = n_words > 0 ? words[0] : 0u;
+    const unsigned n_banks = n_banks_raw < max_banks ? n_banks_raw : max_banks;
+    if (n_banks_raw > max_banks && threadIdx.x == 0) set_error(status, err_input_capacity);
+    const uint16_t* sizes = bank_sizes(in, ev);
+    const uint8_t* types = bank_types(in, ev);
+    unsigned carry = 0, count = 0;
+    for (unsigned base = 0; base < n_banks; base += blockDim.x) {
+      const unsigned b = base + threadIdx.x;
+      unsigned nsp_flat = 0;
+      if (b < n_banks) {
+        const unsigned off = (1 + b < n_words) ? words[1 + b] : 0u;
+        const unsigned w = 2 + n_banks_raw + off / 4;
+        const unsigned type = types[b];
+        const bool velo_bank = type == bank_type_vp || type == bank_type_velo;
+        const unsigned src = w < n_words ? words[w] : 0u;
+        unsigned nsp, first;
+        if (v23) {
+          nsp = (w + 1 < n_words) ? words[w + 1] : 0u;
+          first = w + 2;
+        }
+        else {
+          nsp = sizes[b] / 4u;
+          first = w + 1;
+        }
+        if (velo_bank) count += nsp;
+        if (first > n_words) first = n_words;
+        if (first + nsp > n_words || first + nsp < first) {
+          set_error(status, err_input_capacity);
+          nsp = n_words - first;
+        }
+        bt.words_off[b] = first;
+        bt.n_sp[b] = nsp;
+        bt.source_id[b] = src;
+        bt.velo[b] = velo_bank;
+        nsp_flat = velo_bank ? nsp : 0u;
+      }
+      unsigned total;
+      const unsigned excl = block_exclusive_scan(nsp_flat, warp_sums, &total);
+      if (b < n_banks) bt.flat[b] = carry + excl;
+      carry += total;
+    }
+    // count of SP words of VP/Velo banks, unclamped (reference: raw_bank.count or size / 4)
+    unsigned total_count;
+    block_exclusive_scan(count, warp_sums, &total_count);
+    if (threadIdx.x == 0) {
+      bt.n_banks = n_banks;
+      bt.total_sp = carry;
+      bt.flat[n_banks] = carry;
+      bt.count_total = total_count;
+    }
+    __syncthreads();
+  }
+
+  __device__ __forceinline__ unsigned bank_of(const BankTable& bt, unsigned f)
+  {
+    // last bank b with flat[b] <= f (banks with no SP share their start with the next)
+    unsigned lo = 0, hi = bt.n_banks;
+    while (hi - lo > 1) {
+      const unsigned mid = (lo + hi) / 2;
+      if (bt.flat[mid] <= f) lo = mid;
+      else hi = mid;
+    }
+    return lo;
+  }
+
+  // ------------------------------------------------------------------------------------
+  // Candidate search of a non-isolated SP (EstimateInputSize.cu:72-204).  Every SP of
+  // the bank is a potential neighbour: the reference reads the current SP's own
+  // no-neighbour bit instead of the other's (line 113), which is always 0 here.
+  // Returns up to two candidate pixel codes: bit 8 set = present, bits 0..2 = pixel.
+  // ------------------------------------------------------------------------------------
+  __device__ __forceinline__ uint32_t sp_candidates(uint32_t sp_word, const uint32_t* bank_words, unsigned n_sp)
+  {
+    const uint32_t sp_addr = (sp_word & 0x007FFF00u) >> 8;
+    const uint32_t sp = sp_word & 0xFFu;
+    uint32_t pixels = (sp & 0x0Fu) | ((sp & 0xF0u) << 2);
+    const uint32_t sp_row = sp_addr & 0x3Fu;
+    const uint32_t sp_col = sp_addr >> 6;
+    for (unsigned k = 0; k < n_sp; ++k) {
+      const uint32_t ow = bank_words[k];
+      const uint32_t oaddr = (ow & 0x007FFF00u) >> 8;
+      const uint32_t orow = oaddr & 0x3Fu;
+      const uint32_t ocol = oaddr >> 6;
+      const uint32_t osp = ow & 0xFFu;
+      const bool col_same = ocol == sp_col;
+      const bool col_right = ocol == sp_col + 1;
+      if (!(col_same || col_right)) continue;
+      if (orow == sp_row + 1) {
+        if (col_same) pixels |= (((osp & 0x01u) | ((osp & 0x10u) << 2)) << 4);
+        else pixels |= ((osp & 0x01u) << 16);
+      }
+      else if (orow == sp_row) {
+        if (col_right) pixels |= ((osp & 0x0Fu) << 12);
+      }
+      else if (orow == sp_row - 1) {
+        if (col_right) pixels |= ((osp & 0x08u) << 8);
+        else pixels |= ((osp & 0x80u) >> 2);
+      }
+    }
+    const uint32_t inside = pixels & 0x3CFu;
+    const uint32_t mask = (inside << 1) | (inside << 5) | (inside << 6) | (inside << 7);
+    const uint32_t working = mask & (~pixels);
+    const uint32_t cand_tmp = (working >> 1) & (working >> 5) & (working >> 6) & (working >> 7);
+    const uint32_t cands = cand_tmp & pixels;
+    const uint32_t consolidated = (cands & 0x0Fu) | ((cands >> 2) & 0xF0u);
+    const uint32_t first = consolidated & 0x33u;
+    const uint32_t second = consolidated & 0xCCu;
+    uint32_t r = 0;
+    if (first) r |= 0x100u | (__clz(first) - 24);
+    if (second) r |= (0x100u | (__clz(second) - 24)) << 16;
+    return r;
+  }
+
+  __device__ __forceinline__ bool isolated_two_clusters(uint32_t sp)
+  {
+    const bool pattern_0 = (sp & 0x88u) && !(sp & 0x44u) && (sp & 0x33u);
+    const bool pattern_1 = (sp & 0xCCu) && !(sp & 0x22u) && (sp & 0x11u);
+    return pattern_0 || pattern_1;
+  }
+
+  // ------------------------------------------------------------------------------------
+  // estimate_kernel: dev_number_of_candidates, dev_velo_bank_index (as a max-reduced
+  // key), dev_estimated_input_size and dev_module_candidate_num.
+  // ------------------------------------------------------------------------------------
+  __global__ void __launch_bounds__(decode_threads) estimate_kernel(EstimateParams p)
+  {
+    extern __shared__ __align__(128) unsigned char dsmem[];
+    __shared__ BankTable bt;
+    __shared__ unsigned est_mp[n_module_pairs];
+    __shared__ unsigned cand_count;
+    __shared__ unsigned warp_sums[33];
+    __shared__ __align__(8) uint64_t bar;
+
+    const unsigned e = blockIdx.x;
+    const unsigned ev = e + p.in.event_start;
+    const bool v23 = p.in.bank_version == 2 || p.in.bank_version == 3;
+    if (threadIdx.x < n_module_pairs) est_mp[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+      cand_count = 0;
+      mbar_init(&bar, 1);
+    }
+    __syncthreads();
+
+    unsigned n_words;
+    const uint32_t* words = stage_event(p.in, ev, dsmem, p.smem_blob_bytes, &bar, p.status, n_words);
+    parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
+
+    // velo_calculate_number_of_candidates: block 0 of the reference's launch (grid of
+    // ceil(N / 256) blocks, one thread per event) handles events 0, stride, 2 stride, ...
+    // and the last of them to write an entry wins.
+    if (p.designated_stride > 0 && e % p.designated_stride == 0) {
+      const unsigned long long key_hi = static_cast<unsigned long long>(e) << 32;
+      for (unsigned b = threadIdx.x; b < bt.n_banks; b += blockDim.x) {
+        const unsigned src = bt.source_id[b] & 0x1FFu;
+        if (p.in.bank_version > 3) {
+          if ((src << 1) < n_sensors) atomicMax(p.bank_index_key + (src << 1), key_hi | b);
+          if (((src << 1) | 1u) < n_sensors) atomicMax(p.bank_index_key + ((src << 1) | 1u), key_hi | b);
+        }
+        else if (src < n_sensors) {
+          atomicMax(p.bank_index_key + src, key_hi | b);
+        }
+      }
+    }
+
+    for (unsigned f = threadIdx.x; f < bt.total_sp; f += blockDim.x) {
+      const unsigned b = bank_of(bt, f);
+      const unsigned mp = bank_module_pair(bt.source_id[b], p.in.bank_version);
+      const uint32_t* bank_words = words + bt.words_off[b];
+      const uint32_t word = bank_words[f - bt.flat[b]];
+      unsigned add;
+      if (word & 0x80000000u) {
+        add = isolated_two_clusters(word & 0xFFu) ? 2u : 1u;
+      }
+      else {
+        const uint32_t c = sp_candidates(word, bank_words, bt.n_sp[b]);
+        add = ((c >> 8) & 1u) + ((c >> 24) & 1u);
+        if (add) atomicAdd(&cand_count, add);
+      }
+      if (mp < n_module_pairs) atomicAdd(&est_mp[mp], add);
+      else set_error(p.status, err_input_capacity);
+    }
+    __syncthreads();
+    if (threadIdx.x < n_module_pairs) {
+      p.estimated_input_size[e * n_module_pairs + threadIdx.x] = est_mp[threadIdx.x];
+    }
+    if (threadIdx.x == 0) {
+      unsigned s = 0;
+      for (unsigned mp = 0; mp < n_module_pairs; ++mp)
+        s += est_mp[mp];
+      p.event_estimate[e] = s;
+      p.number_of_candidates[e] = 2 * bt.count_total;
+      p.module_candidate_num[e] = cand_count;
+    }
+    (void) v23;
+  }
+
+  // ------------------------------------------------------------------------------------
+  // Mask clustering of one candidate (MaskedVeloClustering.cu:21-84, 290-496)
+  // ------------------------------------------------------------------------------------
+  __device__ __forceinline__ uint64_t make_8con_mask(uint64_t c)
+  {
+    return c | ((c & 0x7FFF7FFF7FFF7FFFull) << 1) | ((c & 0xFFFEFFFEFFFEFFFEull) << 15) | (c << 16) |
+           ((c & 0xFFFCFFFCFFFCFFFCull) << 17) | ((c & 0xFFFEFFFEFFFEFFFEull) >> 1) |
+           ((c & 0x7FFF7FFF7FFF7FFFull) >> 15) | (c >> 16) | ((c & 0x3FFF3FFF3FFF3FFFull) >> 17);
+  }
+
+  __device__ __forceinline__ uint64_t mask_east(uint64_t c)
+  {
+    const uint64_t m = c >> 48;
+    return m | ((m & 0x7FFF7FFF7FFF7FFFull) << 1) | (m >> 1);
+  }
+
+  __device__ __forceinline__ uint64_t mask_west(uint64_t c)
+  {
+    const uint64_t m = c << 48;
+    return m | (m << 1) | ((m & 0xFFFEFFFEFFFEFFFEull) >> 1);
+  }
+
+  struct PixelCluster {
+    uint64_t pixels;
+    uint32_t x, y, n;
+  };
+
+  __device__ __forceinline__ PixelCluster
+  make_cluster(uint64_t map, uint64_t start, uint32_t col_lower, uint32_t row_lower)
+  {
+    uint64_t cur = 0, next = start;
+    while (cur != next) {
+      cur = next;
+      next = map & make_8con_mask(cur);
+    }
+    PixelCluster c;
+    c.pixels = cur;
+    c.n = __popcll(cur);
+    c.x = col_lower * c.n + __popcll(cur & 0x00000000FFFF0000ull) + __popcll(cur & 0x0000FFFF00000000ull) * 2 +
+          __popcll(cur & 0xFFFF000000000000ull) * 3;
+    uint32_t y = row_lower * c.n;
+#pragma unroll
+    for (unsigned r = 1; r <= 14; ++r)
+      y += __popcll(cur & (0x0001000100010001ull << r)) * r;
+    c.y = y;
+    return c;
+  }
+
+  struct ClusterOut {
+    uint32_t id;
+    float x, y, z;
+    int16_t phi;
+  };
+
+  __device__ __forceinline__ void
+  local_to_global(const Geometry* g, const float* ltg, float local_x, float local_y, ClusterOut& o)
+  {
+    o.x = __ldg(ltg + 0) * local_x + __ldg(ltg + 1) * local_y + __ldg(ltg + 9);
+    o.y = __ldg(ltg + 3) * local_x + __ldg(ltg + 4) * local_y + __ldg(ltg + 10);
+    o.z = __ldg(ltg + 6) * local_x + __ldg(ltg + 7) * local_y + __ldg(ltg + 11);
+  }
+
+  __device__ bool rest_of_clusters(
+    const Geometry* g,
+    const Constants& k,
+    uint32_t candidate,
+    const uint32_t* bank_words,
+    unsigned n_sp,
+    int version,
+    ClusterOut& o)
+  {
+    const uint32_t sp_index = candidate >> 11;
+    const uint32_t sensor_number = (candidate >> 3) & 0xFFu;
+    const uint32_t start_loc = candidate & 0x7u;
+    const float* ltg = g->ltg + 12 * sensor_number;
+    const uint32_t sp_word = bank_words[sp_index];
+    const uint32_t sp_addr = (sp_word & 0x007FFF00u) >> 8;
+    const int32_t sp_row = static_cast<int32_t>(sp_addr & 0x3Fu);
+    const int32_t sp_col = static_cast<int32_t>(sp_addr >> 6);
+
+    uint32_t pa[5] = {0, 0, 0, 0, 0};
+    const int32_t r_lo = sp_row - 2, r_hi = sp_row + 1;
+    const int32_t c_lo = sp_col - 3, c_hi = sp_col + 1;
+    const int32_t row_lower = r_lo * 4;
+    const int32_t col_lower = c_lo * 2;
+    for (unsigned j = 0; j < n_sp; ++j) {
+      const uint32_t ow = bank_words[j];
+      if (version > 3) {
+        const uint32_t other_bit = (ow & 0x800000u) ? 1u : 0u;
+        if (other_bit != (sensor_number & 0x1u)) continue;
+      }
+      if (ow & 0x80000000u) continue;
+      const uint32_t oaddr = (ow & 0x007FFF00u) >> 8;
+      const int32_t orow = static_cast<int32_t>(oaddr & 0x3Fu);
+      const int32_t ocol = static_cast<int32_t>(oaddr >> 6);
+      if (orow >= r_lo && orow <= r_hi && ocol >= c_lo && ocol <= c_hi) {
+        const uint32_t osp = ow & 0xFFu;
+        const int rel_row = orow - r_lo;
+        const int rel_col = ocol - c_lo;
+        const uint32_t bits = ((osp & 0x0Fu) << (4 * rel_row)) | ((osp & 0xF0u) << (12 + 4 * rel_row));
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+          if (c == rel_col) pa[c] |= bits;
+      }
+    }
+
+    const uint32_t rel_row0 = start_loc & 0x3u;
+    const uint32_t rel_col0 = start_loc < 4 ? 1u : 0u;
+    const uint32_t col = static_cast<uint32_t>(sp_col) * 2 + rel_col0;
+    const uint64_t start = (static_cast<uint64_t>(0x01u << (11 - rel_row0)) << (16 * (col & 0x01u))) << 32;
+    const uint64_t map = (static_cast<uint64_t>(pa[3]) << 32) | pa[2];
+    const PixelCluster cl = make_cluster(map, start, static_cast<uint32_t>(col_lower + 4), static_cast<uint32_t>(row_lower));
+    const uint64_t precedence = (mask_east(cl.pixels) & pa[4]) | (cl.pixels & (start ^ (0ull - start)));
+    bool keep = precedence == 0 && !(cl.pixels & 0x8000800080008000ull) && !(cl.pixels & 0x0001000100010001ull);
+    if (!keep) return false;
+    uint32_t x = cl.x, y = cl.y, n = cl.n;
+    if (cl.pixels & 0xFFFFull) {
+      const uint64_t west_map = (static_cast<uint64_t>(pa[1]) << 32) | pa[0];
+      const uint64_t west_start = mask_west(cl.pixels) & west_map;
+      const PixelCluster ext =
+        make_cluster(west_map, west_start, static_cast<uint32_t>(col_lower), static_cast<uint32_t>(row_lower));
+      x += ext.x;
+      y += ext.y;
+      n += ext.n;
+      keep = !(ext.pixels & 0x8000800080008000ull) && !(ext.pixels & 0xFFFFull) &&
+             !(cl.pixels & 0x0001000100010001ull);
+    }
+    if (!keep) return false;
+    const uint32_t cx = x / n;
+    const uint32_t cy = y / n;
+    const float fx = __fdiv_rn(__uint2float_rn(x), __uint2float_rn(n)) - __uint2float_rn(cx);
+    const float fy = __fdiv_rn(__uint2float_rn(y), __uint2float_rn(n)) - __uint2float_rn(cy);
+    const uint32_t chip = cx >> 8;
+    o.id = lhcb_id(channel_id(sensor_number, chip, cx & 0xFFu, cy));
+    const float local_x = __ldg(g->local_x + cx) + fx * __ldg(g->x_pitch + cx);
+    const float local_y = (__uint2float_rn(cy) + 0.5f + fy) * 0.055f;
+    local_to_global(g, ltg, local_x, local_y, o);
+    o.phi = hit_phi_16(k, o.x, o.y);
+    return true;
+  }
+
+  // Isolated SP through the lookup tables (MaskedVeloClustering.cu:131-288); which = 0/1.
+  __device__ __forceinline__ void isolated_cluster(
+    const Geometry* g,
+    const Constants& k,
+    uint32_t sp_word,
+    unsigned source_id,
+    int version,
+    unsigned which,
+    ClusterOut& o)
+  {
+    const bool v23 = version == 2 || version == 3;
+    const bool bit23 = (sp_word & 0x800000u) != 0;
+    const uint32_t pair = source_id & 0x1FFu;
+    const uint32_t sensor_index = v23 ? source_id : (bit23 ? ((pair << 1) | 1u) : (pair << 1));
+    const float* ltg = g->ltg + 12 * (v23 ? pair : (bit23 ? ((pair << 1) | 1u) : (pair << 1)));
+    const uint32_t sp_addr = (sp_word & 0x007FFF00u) >> 8;
+    const int32_t sp_row = static_cast<int32_t>(sp_addr & 0x3Fu);
+    const int32_t sp_col = static_cast<int32_t>(sp_addr >> 6);
+    const uint32_t sp = sp_word & 0xFFu;
+    const uint32_t idx = __ldg(g->sp_patterns + sp);
+    const uint32_t chip = static_cast<uint32_t>(sp_col) >> 7;
+    const uint32_t row = which ? (idx >> 4) & 3u : idx & 3u;
+    const uint32_t col = which ? (idx >> 6) & 1u : (idx >> 2) & 1u;
+    const uint32_t cx = static_cast<uint32_t>(sp_col) * 2 + col;
+    const uint32_t cy = static_cast<uint32_t>(sp_row) * 4 + row;
+    o.id = lhcb_id(channel_id(sensor_index, chip, cx & 0xFFu, cy));
+    const float fx = __ldg(g->sp_fx + sp * 2 + which);
+    const float fy = __ldg(g->sp_fy + sp * 2 + which);
+    const float local_x = __ldg(g->local_x + cx) + fx * __ldg(g->x_pitch + cx);
+    const float local_y = (__uint2float_rn(cy) + 0.5f + fy) * 0.055f;
+    local_to_global(g, ltg, local_x, local_y, o);
+    o.phi = hit_phi_16(k, o.x, o.y);
+  }
+
+  // ------------------------------------------------------------------------------------
+  // cluster_sort_kernel
+  // ------------------------------------------------------------------------------------
+  __global__ void __launch_bounds__(decode_threads) cluster_sort_kernel(ClusterSortParams p)
+  {
+    extern __shared__ __align__(128) unsigned char dsmem[];
+    __shared__ BankTable bt;
+    __shared__ unsigned region[n_module_pairs + 1]; // estimated start of each module pair, event-relative
+    __shared__ unsigned mp_count[n_module_pairs];
+    __shared__ unsigned warp_sums[33];
+    __shared__ __align__(8) uint64_t bar;
+
+    const unsigned e = blockIdx.x;
+    const unsigned ev = e + p.in.event_start;
+    const unsigned n = p.in.n_events;
+    const int version = p.in.bank_version;
+    const unsigned base = p.event_base[e];
+    const unsigned T = p.event_base[n];
+    if (T > p.cluster_capacity) {
+      // the slice needs more clusters than reserved: nothing is written
+      if (threadIdx.x == 0) set_error(p.status, err_input_capacity);
+      return;
+    }
+
+    if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      unsigned s = 0;
+      for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
+        region[mp] = s;
+        s += p.estimated_input_size[e * n_module_pairs + mp];
+      }
+      region[n_module_pairs] = s;
+    }
+    if (threadIdx.x < n_module_pairs) mp_count[threadIdx.x] = 0;
+    __syncthreads();
+    if (threadIdx.x < n_module_pairs) {
+      p.offsets_estimated_input_size[e * n_module_pairs + threadIdx.x] = base + region[threadIdx.x];
+    }
+    if (e == n - 1 && threadIdx.x == 0) p.offsets_estimated_input_size[n * n_module_pairs] = T;
+
+    const unsigned est_total = region[n_module_pairs];
+    // Staging of the unsorted clusters: shared memory when they fit, else the event's
+    // slice of the global staging buffer (20 bytes per estimated cluster, so that every
+    // event's slice starts 4-byte aligned).  The blob sits after the staging area.
+    const bool staged_in_smem = est_total <= p.smem_cluster_capacity;
+    const unsigned staging_bytes = ((p.smem_cluster_capacity * element_size) + 15u) & ~15u;
+    ClusterView st {staged_in_smem ? reinterpret_cast<char*>(dsmem) : p.staging + size_t(20) * base, est_total};
+    unsigned char* blob = dsmem + staging_bytes;
+
+    unsigned n_words;
+    const uint32_t* words = stage_event(p.in, ev, blob, p.smem_blob_bytes, &bar, p.status, n_words);
+    parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
+
+    const Geometry* g = p.geo;
+    for (unsigned f = threadIdx.x; f < bt.total_sp; f += blockDim.x) {
+      const unsigned b = bank_of(bt, f);
+      const unsigned mp = bank_module_pair(bt.source_id[b], version);
+      if (mp >= n_module_pairs) continue;
+      const uint32_t* bank_words = words + bt.words_off[b];
+      const unsigned sp_index = f - bt.flat[b];
+      const uint32_t word = bank_words[sp_index];
+      if (word & 0x80000000u) {
+        const unsigned n_clusters = (__ldg(g->sp_patterns + (word & 0xFFu)) & 8u) ? 2u : 1u;
+        for (unsigned which = 0; which < n_clusters; ++which) {
+          ClusterOut o;
+          isolated_cluster(g, p.k, word, bt.source_id[b], version, which, o);
+          const unsigned slot = atomicAdd(&mp_count[mp], 1u);
+          if (region[mp] + slot < region[mp + 1]) {
+            const unsigned i = region[mp] + slot;
+            st.id(i) = o.id;
+            st.x(i) = o.x;
+            st.y(i) = o.y;
+            st.z(i) = o.z;
+            st.phi(i) = o.phi;
+          }
+          else {
+            set_error(p.status, err_cluster_capacity);
+          }
+        }
+      }
+      else {
+        const uint32_t c = sp_candidates(word, bank_words, bt.n_sp[b]);
+        const bool v23 = version == 2 || version == 3;
+        const uint32_t sensor_number =
+          v23 ? (bt.source_id[b] & 0x1FFu) : (((bt.source_id[b] & 0x1FFu) << 1) | ((word >> 23) & 0x1u));
+        for (unsigned which = 0; which < 2; ++which) {
+          const uint32_t code = which ? (c >> 16) : c;
+          if (!(code & 0x100u)) continue;
+          const uint32_t candidate = (sp_index << 11) | (sensor_number << 3) | (code & 0x7u);
+          // MaskedVeloClustering.cu:567-572: the candidate's bank is looked up by sensor
+          const uint32_t cand_sensor = (candidate >> 3) & 0xFFu;
+          if (cand_sensor >= n_sensors) {
+            set_error(p.status, err_bad_sensor);
+            continue;
+          }
+          const unsigned b2 = static_cast<unsigned>(p.bank_index_key[cand_sensor] & 0xFFFFFFFFull);
+          if (b2 >= bt.n_banks || (candidate >> 11) >= bt.n_sp[b2]) {
+            set_error(p.status, err_input_capacity);
+            continue;
+          }
+          ClusterOut o;
+          if (!rest_of_clusters(g, p.k, candidate, words + bt.words_off[b2], bt.n_sp[b2], version, o)) continue;
+          const unsigned cmp = cand_sensor / 8;
+          const unsigned slot = atomicAdd(&mp_count[cmp], 1u);
+          if (region[cmp] + slot < region[cmp + 1]) {
+            const unsigned i = region[cmp] + slot;
+            st.id(i) = o.id;
+            st.x(i) = o.x;
+            st.y(i) = o.y;
+            st.z(i) = o.z;
+            st.phi(i) = o.phi;
+          }
+          else {
+            set_error(p.status, err_cluster_capacity);
+          }
+        }
+      }
+    }
+    __syncthreads();
+
+    // Rank by (phi, id) inside each module pair (SortByPhi.cu:104-122) and write the
+    // sorted container at its final position.
+    ClusterView out {p.sorted_container, T};
+    for (unsigned i = threadIdx.x; i < est_total; i += blockDim.x) {
+      unsigned mp = 0;
+#pragma unroll 1
+      while (mp + 1 < n_module_pairs && region[mp + 1] <= i)
+        ++mp;
+      const unsigned count = min(mp_count[mp], region[mp + 1] - region[mp]);
+      const unsigned local = i - region[mp];
+      if (local >= count) continue;
+      const int16_t phi = st.phi(i);
+      const uint32_t id = st.id(i);
+      unsigned position = 0;
+      const unsigned r0 = region[mp];
+      for (unsigned j = 0; j < count; ++j) {
+        const int16_t other = st.phi(r0 + j);
+        const uint32_t other_id = st.id(r0 + j);
+        position += phi > other || (j != local && phi == other && id > other_id);
+      }
+      const unsigned dst = base + r0 + position;
+      out.id(dst) = id;
+      out.phi(dst) = phi;
+      out.x(dst) = st.x(i);
+      out.y(dst) = st.y(i);
+      out.z(dst) = st.z(i);
+    }
+    if (threadIdx.x < n_module_pairs) {
+      const unsigned mp = threadIdx.x;
+      p.module_cluster_num[e * n_module_pairs + mp] = min(mp_count[mp], region[mp + 1] - region[mp]);
+    }
+  }
+
+  // ------------------------------------------------------------------------------------
+  // exclusive_scan_kernel: one CTA per job; out[0] = 0, out[i + 1] = sum(in[0..i])
+  // (host_prefix_sum_t, HostPrefixSum.cpp:76-108, without the host round trip).
+  // ------------------------------------------------------------------------------------
+  __global__ void __launch_bounds__(scan_threads) exclusive_scan_kernel(ScanParams p)
+  {
+    __shared__ unsigned warp_sums[33];
+    const ScanJob job = p.jobs[blockIdx.x];
+    if (job.in == nullptr) return;
+    unsigned carry = 0;
+    constexpr unsigned per_thread = 4;
+    const unsigned tile = blockDim.x * per_thread;
+    for (unsigned t0 = 0; t0 < job.n; t0 += tile) {
+      unsigned v[per_thread];
+      unsigned s = 0;
+#pragma unroll
+      for (unsigned q = 0; q < per_thread; ++q) {
+        const unsigned i = t0 + threadIdx.x * per_thread + q;
+        v[q] = i < job.n ? job.in[i] : 0u;
+        s += v[q];
+      }
+      unsigned total;
+      unsigned excl = block_exclusive_scan(s, warp_sums, &total);
+#pragma unroll
+      for (unsigned q = 0; q < per_thread; ++q) {
+        const unsigned i = t0 + threadIdx.x * per_thread + q;
+        if (i < job.n) job.out[i] = carry + excl;
+        excl += v[q];
+      }
+      carry += total;
+    }
+    if (threadIdx.x == 0) job.out[job.n] = carry;
+  }
+
+} // namespace velo

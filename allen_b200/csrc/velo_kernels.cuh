@@ -1,0 +1,103 @@
+// Kernel parameter blocks and launch declarations of the VELO chain (sm_100a).
+#pragma once
+
+#include "velo_common.cuh"
+
+namespace velo {
+
+  // ---- decoding: velo_calculate_number_of_candidates + velo_estimate_input_size ----
+  struct EstimateParams {
+    RawInput in;
+    unsigned* estimated_input_size;       // [26 N] dev_estimated_input_size
+    unsigned* number_of_candidates;       // [N]    dev_number_of_candidates
+    unsigned* module_candidate_num;       // [N]    dev_module_candidate_num
+    unsigned* event_estimate;             // [N]    sum of the event's 26 estimates
+    unsigned long long* bank_index_key;   // [208]  (event << 32 | bank), max-reduced
+    unsigned designated_stride;           // events e with e % stride == 0 set the bank index
+    unsigned* status;
+    unsigned smem_blob_bytes;
+  };
+
+  // ---- masked clustering + phi + sort by phi, one event per CTA ----
+  struct ClusterSortParams {
+    RawInput in;
+    const Geometry* geo;
+    Constants k;
+    const unsigned* estimated_input_size;       // [26 N]
+    const unsigned* event_base;                 // [N + 1] exclusive scan of event_estimate
+    const unsigned long long* bank_index_key;   // [208]
+    unsigned* offsets_estimated_input_size;     // [26 N + 1] dev_offsets_estimated_input_size
+    unsigned* module_cluster_num;               // [26 N]     dev_module_cluster_num
+    char* sorted_container;                     // [18 T]     dev_sorted_velo_cluster_container
+    char* staging;                              // [20 T]     fallback staging for large events
+    unsigned* status;
+    unsigned smem_blob_bytes;
+    unsigned smem_cluster_capacity;             // clusters staged in shared memory per event
+    unsigned cluster_capacity;                  // allocated T of the containers
+  };
+
+  // ---- search by triplet + three-hit filter, one event per CTA ----
+  struct SearchParams {
+    Geometry const* geo;
+    Constants k;
+    unsigned n_events;
+    const unsigned* offsets_estimated_input_size; // [26 N + 1]
+    const unsigned* module_cluster_num;           // [26 N]
+    const char* sorted_container;                 // [18 T]
+    unsigned track_capacity;                      // allocated entries of the track containers
+    TrackHits* tracks;                            // dev_tracks
+    TrackletHits* three_hit_tracks;               // dev_three_hit_tracks
+    bool* hit_used;                               // [T] dev_hit_used
+    unsigned* atomics_velo;                       // [3 N] dev_atomics_velo
+    unsigned* number_of_velo_tracks;              // [N] dev_number_of_velo_tracks
+    TrackletHits* three_hit_tracks_output;        // dev_three_hit_tracks_output
+    unsigned* number_of_three_hit_tracks_output;  // [N]
+    unsigned* event_track_hits;                   // [N] hits of the event's consolidated tracks
+    unsigned* status;
+    unsigned smem_hit_capacity;                   // hits staged in shared memory per event
+    unsigned cluster_capacity;                    // allocated T of the containers
+  };
+
+  // ---- copy_track_hit_number + consolidate_tracks, one event per CTA ----
+  struct ConsolidateParams {
+    unsigned n_events;
+    const unsigned* offsets_estimated_input_size;
+    const char* sorted_container;
+    const TrackHits* tracks;
+    const TrackletHits* three_hit_tracks_output;
+    const unsigned* offsets_velo_tracks;                  // [N + 1]
+    const unsigned* offsets_three_hit;                    // [N + 1]
+    const unsigned* event_track_hit_base;                 // [N + 1]
+    unsigned* offsets_all_velo_tracks;                    // [N + 1]
+    unsigned* velo_track_hit_number;                      // [tracks]
+    unsigned* offsets_velo_track_hit_number;              // [tracks + 1]
+    char* velo_track_hits;                                // [18 TH]
+    bool* accepted_velo_tracks;
+    unsigned track_capacity;            // consolidated tracks
+    unsigned track_container_capacity;  // entries of dev_tracks / three-hit containers
+    unsigned track_hit_capacity;
+    unsigned cluster_capacity;
+    unsigned* status;
+  };
+
+  struct ScanJob {
+    const unsigned* in;
+    unsigned* out; // n + 1 entries: exclusive scan, total in the last
+    unsigned n;
+  };
+  struct ScanParams {
+    ScanJob jobs[4];
+  };
+
+  __global__ void estimate_kernel(EstimateParams p);
+  __global__ void cluster_sort_kernel(ClusterSortParams p);
+  __global__ void search_by_triplet_kernel(SearchParams p);
+  __global__ void consolidate_kernel(ConsolidateParams p);
+  __global__ void exclusive_scan_kernel(ScanParams p);
+
+  constexpr unsigned decode_threads = 256;
+  constexpr unsigned scan_threads = 1024;
+  constexpr unsigned consolidate_threads = 256;
+  constexpr unsigned search_threads = 128;
+
+} // namespace velo

@@ -1,0 +1,191 @@
+/*
+ * C ABI of the B200 (sm_100a) VELO super-pixel reconstruction (libvelo_b200.so).
+ *
+ * Drop-in boundary.  The reference runs this path as the Allen algorithms of
+ * configuration/python/AllenConf/velo_reconstruction.py:72-292, each a
+ * `struct X_t : DeviceAlgorithm, Parameters` with set_arguments_size()/operator()
+ * (stream/gear/include/Algorithm.cuh:319-461), host prefix sums in between
+ * (host/prefix_sum/src/HostPrefixSum.cpp:76-108).  This library replaces that whole
+ * chain with one call that an Allen algorithm wrapper (or any C caller) makes:
+ *
+ *   inputs  (device pointers, Allen non-MEP layout, as data_provider_t produces them,
+ *            host/data_provider/include/DataProvider.h:11-19):
+ *       dev_velo_raw_input, dev_velo_raw_input_offsets, dev_velo_raw_input_sizes,
+ *       dev_velo_raw_input_types, host_raw_bank_version, the event slice;
+ *   outputs (device pointers into the chain's workspace, same layouts and names as the
+ *            reference's DEVICE_OUTPUTs, velo_reconstruction.py:269-292 and :153-164):
+ *       dev_offsets_estimated_input_size, dev_module_cluster_num,
+ *       dev_sorted_velo_cluster_container, dev_velo_track_hits,
+ *       dev_offsets_all_velo_tracks, dev_offsets_velo_track_hit_number,
+ *       dev_accepted_velo_tracks, ... and the host scalars
+ *       host_total_number_of_velo_clusters, host_number_of_reconstructed_velo_tracks,
+ *       host_accumulated_number_of_hits_in_velo_tracks.
+ *
+ * Conventions: plain pointers and sizes only; every function returns a VeloStatus
+ * (0 = success) instead of throwing (the reference throws from cudaCheck,
+ * backend/include/CUDABackend.h:23-41); the caller owns the CUDA stream; the chain owns
+ * its device workspace, sized once by velo_chain_reserve().
+ */
+#ifndef VELO_B200_H
+#define VELO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct VeloChain VeloChain;
+typedef void* VeloStream; /* a cudaStream_t */
+
+typedef enum {
+  VELO_OK = 0,
+  VELO_ERR_ARGUMENT = 1,       /* null pointer, bad geometry blob, unsupported bank version */
+  VELO_ERR_CUDA = 2,           /* a CUDA runtime call failed; see velo_last_error_string() */
+  VELO_ERR_CAPACITY = 3,       /* the slice does not fit the reserved workspace */
+  VELO_ERR_DEVICE_FLAGS = 4,   /* the last run raised device status flags (velo_chain_totals) */
+  VELO_ERR_NO_DEVICE = 5       /* no sm_100 device or the kernels are not loadable */
+} VeloStatus;
+
+/* Algorithm properties (reference defaults: SearchByTriplet.cuh:129-131,
+ * ThreeHitTracksFilter.cuh:44). */
+typedef struct {
+  float phi_tolerance;          /* 0.045 */
+  float max_scatter;            /* 0.08 */
+  unsigned max_skipped_modules; /* 1 */
+  float max_chi2;               /* 20 */
+} VeloChainProperties;
+
+/* An event slice in Allen's non-MEP raw-bank layout, on the device. */
+typedef struct {
+  const char* raw;          /* dev_velo_raw_input (16-byte aligned base enables bulk staging) */
+  const unsigned* offsets;  /* dev_velo_raw_input_offsets [n_events + 1] */
+  const unsigned* sizes;    /* dev_velo_raw_input_sizes */
+  const unsigned* types;    /* dev_velo_raw_input_types */
+  unsigned event_start;     /* first event of the slice (RuntimeOptions::event_interval) */
+  unsigned n_events;
+  int bank_version;         /* host_raw_bank_version: 2, 3 or 4 */
+} VeloDeviceSlice;
+
+/* The same slice on the host (page-locked memory gives asynchronous copies). */
+typedef struct {
+  const char* raw;
+  size_t raw_bytes;
+  const unsigned* offsets;
+  const unsigned* sizes;
+  size_t sizes_bytes;
+  const unsigned* types;
+  size_t types_bytes;
+  unsigned n_events;
+  int bank_version;
+} VeloHostSlice;
+
+/* Device pointers of the last run's outputs (valid until the next run or destroy). */
+typedef struct {
+  unsigned* dev_number_of_candidates;              /* [N] */
+  unsigned* dev_estimated_input_size;              /* [26 N] */
+  unsigned* dev_module_candidate_num;              /* [N] */
+  unsigned* dev_offsets_estimated_input_size;      /* [26 N + 1] */
+  unsigned* dev_module_cluster_num;                /* [26 N] */
+  char* dev_sorted_velo_cluster_container;         /* [18 T] */
+  void* dev_tracks;                                /* Velo::TrackHits (54 B) per entry */
+  void* dev_three_hit_tracks;                      /* Velo::TrackletHits (6 B) per entry */
+  uint8_t* dev_hit_used;                           /* [T] */
+  unsigned* dev_atomics_velo;                      /* [3 N] */
+  unsigned* dev_number_of_velo_tracks;             /* [N] */
+  unsigned* dev_offsets_velo_tracks;               /* [N + 1] */
+  void* dev_three_hit_tracks_output;               /* Velo::TrackletHits per entry */
+  unsigned* dev_number_of_three_hit_tracks_output; /* [N] */
+  unsigned* dev_offsets_number_of_three_hit_tracks_filtered; /* [N + 1] */
+  unsigned* dev_offsets_all_velo_tracks;           /* [N + 1] */
+  unsigned* dev_velo_track_hit_number;             /* [tracks] */
+  unsigned* dev_offsets_velo_track_hit_number;     /* [tracks + 1] */
+  char* dev_velo_track_hits;                       /* [18 TH] */
+  uint8_t* dev_accepted_velo_tracks;               /* [tracks + three-hit tracks] */
+} VeloChainOutputs;
+
+/* Host scalars of the last run, available after velo_chain_synchronize(). */
+typedef struct {
+  unsigned n_events;
+  unsigned host_total_number_of_velo_clusters;           /* T: estimated clusters */
+  unsigned host_number_of_cluster_candidates;
+  unsigned host_number_of_velo_tracks_at_least_four_hits;
+  unsigned host_number_of_three_hit_tracks_filtered;
+  unsigned host_number_of_reconstructed_velo_tracks;
+  unsigned host_accumulated_number_of_hits_in_velo_tracks; /* TH */
+  unsigned track_container_size;
+  unsigned device_flags;                                 /* velo::ErrorBits raised by the kernels */
+} VeloChainTotals;
+
+/* Library */
+const char* velo_last_error_string(void);
+VeloStatus velo_device_check(void); /* an sm_100 device is current and the kernels load */
+void velo_default_properties(VeloChainProperties* props);
+
+/* Replaces the per-algorithm Allen objects and Constants::dev_velo_geometry /
+ * dev_velo_sp_patterns / dev_velo_sp_fx / dev_velo_sp_fy
+ * (integration/non_event_data/src/VPGeometry.cpp:21-63): parses the velo_geometry.bin
+ * blob and builds the super-pixel tables on the current device. */
+VeloStatus velo_chain_create(
+  const void* geometry, size_t geometry_size, const VeloChainProperties* props, VeloChain** chain);
+
+/* Sizes the workspace for slices of up to max_events events and max_super_pixels
+ * super pixels in total (the count follows from the bank sizes alone) and, for the
+ * host-buffer path, max_raw_bytes of raw input.  Replaces the scheduler's per-algorithm
+ * set_arguments_size() + arena reservation (stream/gear/include/Scheduler.cuh:353-387). */
+VeloStatus velo_chain_reserve(
+  VeloChain* chain, unsigned max_events, unsigned long long max_super_pixels, unsigned long long max_raw_bytes);
+
+/* Enqueues the whole chain on `stream` for a device-resident slice: velo_calculate_number_of_candidates,
+ * velo_estimate_input_size, velo_masked_clustering, velo_sort_by_phi, velo_search_by_triplet,
+ * velo_three_hit_tracks_filter, velo_copy_track_hit_number, velo_consolidate_tracks and the
+ * five prefix sums, with no host synchronisation.  When use_graph != 0 the launches are captured
+ * once per (slice pointers, sizes) into a CUDA graph and replayed. */
+VeloStatus velo_chain_run(VeloChain* chain, const VeloDeviceSlice* slice, VeloStream stream, int use_graph);
+
+/* End-to-end entry for host buffers: copies the slice to the device, runs the chain and
+ * copies the consolidated tracks back (dev_offsets_all_velo_tracks,
+ * dev_offsets_velo_track_hit_number and dev_velo_track_hits into the host buffers given,
+ * each with its capacity in bytes), then synchronises.  Reports the bytes moved. */
+VeloStatus velo_chain_run_host(
+  VeloChain* chain,
+  const VeloHostSlice* slice,
+  VeloStream stream,
+  unsigned* host_offsets_all_velo_tracks,
+  size_t offsets_all_capacity,
+  unsigned* host_offsets_velo_track_hit_number,
+  size_t offsets_hit_number_capacity,
+  char* host_velo_track_hits,
+  size_t track_hits_capacity,
+  VeloChainTotals* totals,
+  unsigned long long* h2d_bytes,
+  unsigned long long* d2h_bytes);
+
+/* Waits for the last run on its stream and returns its host scalars.  Returns
+ * VELO_ERR_DEVICE_FLAGS when the kernels raised a flag (capacity, overflow). */
+VeloStatus velo_chain_synchronize(VeloChain* chain, VeloChainTotals* totals);
+
+VeloStatus velo_chain_outputs(const VeloChain* chain, VeloChainOutputs* outputs);
+
+/* Per-kernel CUDA-event timing (no counterpart in the reference; its CI profiles with ncu,
+ * scripts/ci/jobs/run_throughput.sh:61-67).  When enabled, every run records an event
+ * between consecutive kernels, inside the captured graphs too; velo_chain_kernel_times()
+ * sums, per kernel, the last execution of every cached graph (and of the last direct run)
+ * and reports how many executions were summed. */
+VeloStatus velo_chain_set_timing(VeloChain* chain, int enable);
+unsigned velo_chain_kernel_count(void);
+const char* velo_chain_kernel_name(unsigned kernel);
+VeloStatus velo_chain_kernel_times(VeloChain* chain, float* ms_sum, unsigned* n_runs);
+
+void velo_chain_destroy(VeloChain* chain);
+
+/* Utilities (synchronous copies on the current device), for callers without a CUDA runtime binding. */
+VeloStatus velo_copy_to_host(void* host, const void* device, size_t bytes);
+VeloStatus velo_copy_to_device(void* device, const void* host, size_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

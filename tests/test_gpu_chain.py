@@ -1,0 +1,78 @@
+"""Parity of the B200 chain (through the C ABI) with the oracle, bit for bit."""
+import numpy as np
+import pytest
+
+import golden_io
+import parity
+from allen_b200 import generator
+from allen_b200.chain import upload
+
+pytestmark = pytest.mark.gpu
+
+
+def run_chain(chain, s, use_graph=False):
+    chain.reserve_for(s)
+    d = upload(s)
+    chain.run(d, use_graph=use_graph)
+    totals = chain.synchronize()
+    return totals, chain.outputs_to_host(totals)
+
+
+@pytest.mark.parametrize("name", golden_io.FIXTURES)
+def test_golden_fixture(chain, oracle, geometry, name):
+    s, ref = golden_io.load(name)
+    totals, out = run_chain(chain, s)
+    assert totals["device_flags"] == 0
+    # against the reference's own outputs committed with the fixture
+    for k in parity.EXACT:
+        if k in ref:
+            assert np.array_equal(parity._u8(out[k]), parity._u8(ref[k])), k
+    # against the oracle, every buffer
+    assert parity.compare(out, oracle.run(s, geometry), s.n_events) == []
+
+
+CONFIGS = {
+    "nu7.6": dict(),
+    "v3": dict(bank_version=3),
+    "v4": dict(bank_version=4),
+    "uneven": dict(pileup_min=1.0, pileup_max=15.0),
+    "nu15_noise": dict(mean_pileup=15.0, noise_rate=1e-4, hit_efficiency=0.95),
+}
+
+
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_synthetic(chain, oracle, geometry, cfg):
+    g = generator.generate(150, seed=100 + len(cfg), **CONFIGS[cfg])
+    totals, out = run_chain(chain, g.raw)
+    assert totals["device_flags"] == 0
+    assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
+
+
+def test_graph_replay_and_host_path(chain, oracle, geometry):
+    g = generator.generate(64, seed=5)
+    t1, a = run_chain(chain, g.raw, use_graph=True)
+    d = upload(g.raw)
+    chain.run(d, use_graph=True)
+    chain.run(d, use_graph=True)  # replay of the cached graph
+    t2 = chain.synchronize()
+    b = chain.outputs_to_host(t2)
+    assert t1 == t2
+    assert parity.compare(a, b, g.raw.n_events) == []
+    t3, host_out, up, down = chain.run_host(g.raw)
+    assert up >= g.raw.raw.nbytes and down > 0
+    ref = oracle.run(g.raw, geometry)
+    assert np.array_equal(host_out["dev_offsets_all_velo_tracks"], ref["dev_offsets_all_velo_tracks"])
+    TH = int(ref["dev_offsets_velo_track_hit_number"][-1])
+    assert np.array_equal(host_out["dev_velo_track_hits"][:16 * TH], parity._u8(ref["dev_velo_track_hits"])[:16 * TH])
+
+
+def test_event_slice_offset(chain, oracle, geometry):
+    """A slice that starts inside the arrays (RuntimeOptions::event_interval)."""
+    g = generator.generate(40, seed=9)
+    d = upload(g.raw).sub(10, 25)
+    chain.reserve_for(g.raw)
+    chain.run(d)
+    totals = chain.synchronize()
+    out = chain.outputs_to_host(totals)
+    ref = oracle.run(g.raw, geometry, event_start=10, n_events=25)
+    assert parity.compare(out, ref, 25) == []
