@@ -105,6 +105,13 @@ def _lib():
     lib.velo_copy_to_host.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.velo_copy_to_device.restype = C.c_int
     lib.velo_copy_to_device.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.velo_chain_set_timing.restype = C.c_int
+    lib.velo_chain_set_timing.argtypes = [C.c_void_p, C.c_int]
+    lib.velo_chain_kernel_count.restype = C.c_uint
+    lib.velo_chain_kernel_name.restype = C.c_char_p
+    lib.velo_chain_kernel_name.argtypes = [C.c_uint]
+    lib.velo_chain_kernel_times.restype = C.c_int
+    lib.velo_chain_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint)]
     lib._typed = True
     return lib
 
@@ -194,6 +201,17 @@ class VeloChain:
         if check:
             _check(self.lib, status, totals["device_flags"])
         return totals
+
+    def set_timing(self, enable: bool):
+        _check(self.lib, self.lib.velo_chain_set_timing(self.handle, int(enable)))
+
+    def kernel_times(self) -> tuple[dict, int]:
+        """Per kernel: summed duration (ms) of the last execution of every cached graph."""
+        n = self.lib.velo_chain_kernel_count()
+        ms = (C.c_float * n)()
+        runs = C.c_uint()
+        _check(self.lib, self.lib.velo_chain_kernel_times(self.handle, ms, C.byref(runs)))
+        return {self.lib.velo_chain_kernel_name(i).decode(): float(ms[i]) for i in range(n)}, runs.value
 
     def device_outputs(self) -> dict:
         o = OutputsC()

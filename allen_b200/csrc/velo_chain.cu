@@ -238,13 +238,18 @@ struct VeloChain {
 };
 
 namespace {
-  VeloStatus enqueue_chain(VeloChain* c, const VeloDeviceSlice& s, cudaStream_t stream, cudaEvent_t* ev)
+  VeloStatus enqueue_chain(VeloChain* c, const VeloDeviceSlice& s, cudaStream_t stream, cudaEvent_t* ev, bool capturing)
   {
     using namespace velo;
     const unsigned n = s.n_events;
     RawInput in {s.raw, s.offsets, s.sizes, s.types, s.event_start, s.n_events, s.bank_version};
     unsigned stage = 0;
-    auto mark = [&]() -> cudaError_t { return ev ? cudaEventRecord(ev[stage++], stream) : cudaSuccess; };
+    // inside a capture the records must become graph nodes of their own (external events)
+    auto mark = [&]() -> cudaError_t {
+      if (!ev) return cudaSuccess;
+      return capturing ? cudaEventRecordWithFlags(ev[stage++], stream, cudaEventRecordExternal) :
+                         cudaEventRecord(ev[stage++], stream);
+    };
 
     VELO_CUDA(cudaMemsetAsync(c->bank_index_key.p, 0, n_sensors * sizeof(unsigned long long), stream));
     VELO_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(unsigned), stream));
@@ -513,7 +518,7 @@ VeloStatus velo_chain_run(VeloChain* c, const VeloDeviceSlice* s, VeloStream str
     if (c->timing && !c->direct_ev[0])
       for (auto& e : c->direct_ev)
         VELO_CUDA(cudaEventCreate(&e));
-    const VeloStatus st = enqueue_chain(c, *s, stream, c->timing ? c->direct_ev : nullptr);
+    const VeloStatus st = enqueue_chain(c, *s, stream, c->timing ? c->direct_ev : nullptr, false);
     if (st != VELO_OK) return st;
     c->direct_timed = c->timing;
     VELO_CUDA(cudaEventRecord(c->done, stream));
@@ -538,7 +543,7 @@ VeloStatus velo_chain_run(VeloChain* c, const VeloDeviceSlice* s, VeloStream str
         VELO_CUDA(cudaEventCreate(&e));
     cudaGraph_t graph;
     VELO_CUDA(cudaStreamBeginCapture(c->capture_stream, cudaStreamCaptureModeThreadLocal));
-    const VeloStatus st = enqueue_chain(c, *s, c->capture_stream, c->timing ? entry->ev : nullptr);
+    const VeloStatus st = enqueue_chain(c, *s, c->capture_stream, c->timing ? entry->ev : nullptr, true);
     const cudaError_t end = cudaStreamEndCapture(c->capture_stream, &graph);
     if (st != VELO_OK) {
       c->graphs.pop_back();

@@ -1,0 +1,78 @@
+"""Tracking efficiency, ghost and clone rates against generator truth.
+
+Rules of the reference's TrackChecker (checker/tracking/include/TrackChecker.h:180-320,
+TrackCheckerCategories.h:28-30), applied to synthetic truth:
+  * a track is matched to the particle owning at least 70% of its hits (m_minweight);
+  * a track matched to no particle is a ghost;
+  * further tracks matched to an already matched particle are clones;
+  * efficiency denominator ("01_velo"): particles with hits on at least 3 distinct
+    modules (the generator's stand-in for hasVelo) and 2 < eta < 5 (no electrons are
+    generated).
+A hit belongs to the particle that owns the pixel of the cluster's channel id (the
+centroid pixel); noise pixels belong to nobody.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+MIN_WEIGHT = 0.7
+
+
+def hit_owner_tables(gen):
+    """Per event: (sorted lhcb ids, owning particle) from the generator's truth pixels."""
+    tables = []
+    tp, to = gen.truth_pixels, gen.truth_offsets
+    for e in range(to.size - 1):
+        sl = tp[to[e]:to[e + 1]]
+        order = np.argsort(sl["lhcb_id"], kind="stable")
+        tables.append((sl["lhcb_id"][order], sl["particle"][order]))
+    return tables
+
+
+def match_tracks(tracks_ids, table):
+    """tracks_ids: list of tuples of LHCb ids for one event.  Returns the matched particle
+    index per track (-1 for a ghost)."""
+    ids, owner = table
+    out = []
+    for t in tracks_ids:
+        a = np.asarray(t, dtype=np.uint32)
+        pos = np.searchsorted(ids, a)
+        pos = np.minimum(pos, max(ids.size - 1, 0))
+        found = (ids.size > 0) & (ids[pos] == a) if ids.size else np.zeros(a.size, bool)
+        parts = owner[pos][found] if ids.size else np.zeros(0, np.uint32)
+        if parts.size == 0:
+            out.append(-1)
+            continue
+        vals, cnt = np.unique(parts, return_counts=True)
+        best = int(np.argmax(cnt))
+        out.append(int(vals[best]) if cnt[best] >= MIN_WEIGHT * a.size else -1)
+    return out
+
+
+def evaluate(gen, tracks_per_event) -> dict:
+    """gen: allen_b200.generator.Generated; tracks_per_event: list (per event) of lists
+    of LHCb-id tuples.  Returns counts and rates."""
+    tables = hit_owner_tables(gen)
+    n_tracks = n_ghost = n_clone = 0
+    n_recoble = n_reco = 0
+    po = gen.particle_offsets
+    for e, tracks in enumerate(tracks_per_event):
+        parts = gen.particles[po[e]:po[e + 1]]
+        matched = match_tracks(tracks, tables[e])
+        n_tracks += len(matched)
+        n_ghost += sum(1 for m in matched if m < 0)
+        seen = {}
+        for m in matched:
+            if m >= 0:
+                seen[m] = seen.get(m, 0) + 1
+        recoble = (parts["n_modules"] >= 3) & (parts["eta"] > 2) & (parts["eta"] < 5)
+        n_recoble += int(recoble.sum())
+        for p, c in seen.items():
+            if p < parts.size and recoble[p]:
+                n_reco += 1
+                n_clone += c - 1
+    return {
+        "tracks": n_tracks, "ghosts": n_ghost, "ghost_rate": n_ghost / max(n_tracks, 1),
+        "reconstructible": n_recoble, "reconstructed": n_reco, "efficiency": n_reco / max(n_recoble, 1),
+        "clones": n_clone, "clone_rate": n_clone / max(n_reco + n_clone, 1),
+    }

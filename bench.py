@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""VELO events/s on B200: the plain chain (SP decoding + clustering, phi sort,
+search_by_triplet, three-hit filter, consolidation) over synthetic events.
+
+Workload (one step): 100k generated events at nu = 7.6 (Poisson PVs, beam spot
+sigma 0.04/45 mm, Poisson(25) tracks per PV, eta in [2, 5], 98% hit efficiency,
+0.01 mm smear, 1-4 pixel clusters, 1e-5 noise), processed in slices of 16000 events,
+the raw banks resident in HBM (1.3 GB per step, larger than L2).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  Under torchrun (N > 1) every rank processes its own events
+(replicas, weak scaling) and the time is the max over ranks.  `--impl reference` times
+the reference's own VELO kernels built as CPU C++ (oracle/_ref; the plain-C oracle if
+that build is absent) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "VELO events/s on 1 B200, learned+batched vs plain at equal eff & ghost rate"
+UNIT = "events/s"
+N_MP = 26
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--events", type=int, default=100_000)
+    p.add_argument("--slice", type=int, default=16_000)
+    p.add_argument("--seed", type=int, default=2024)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------------
+# helpers
+# ----------------------------------------------------------------------------------
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def generate_slices(n_events, slice_size, seed, pinned=False):
+    from allen_b200 import generator
+    out = []
+    for first in range(0, n_events, slice_size):
+        n = min(slice_size, n_events - first)
+        out.append(generator.generate(n, seed=seed, first_event=first).raw)
+    return out
+
+
+def pin(s):
+    """Copies a RawSlice into page-locked host memory (numpy views of pinned torch tensors)."""
+    import torch
+    from allen_b200.rawbanks import RawSlice
+
+    def p(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy()
+        v[:] = a.view(np.uint8)
+        return v.view(a.dtype), t
+
+    raw, t0 = p(s.raw)
+    off, t1 = p(s.offsets)
+    siz, t2 = p(s.sizes)
+    typ, t3 = p(s.types)
+    r = RawSlice(raw, off, siz, typ, s.bank_version)
+    r._keep = (t0, t1, t2, t3)
+    return r
+
+
+def kernel_bytes(n, raw_bytes, T, H, n4, n3_all, n3_out, TH, tracks_all):
+    """Algorithmic bytes per launch of each kernel for one slice (no re-reads counted)."""
+    return {
+        "estimate_kernel": raw_bytes + 4 * (N_MP * n + 3 * n),
+        "cluster_sort_kernel": raw_bytes + 4 * N_MP * n + 18 * H + 4 * (2 * N_MP * n + 1),
+        "search_by_triplet_kernel": 18 * H + 8 * N_MP * n + T + 54 * n4 + 6 * (n3_all + n3_out) + 24 * n,
+        "consolidate_kernel": 54 * n4 + 6 * n3_out + 16 * TH + 16 * TH + 4 * (2 * tracks_all + 1) + tracks_all
+                              + 4 * 4 * (n + 1),
+    }
+
+
+def chain_bytes(n, raw_bytes, H, TH, tracks_all):
+    """Algorithmic bytes of the chain per slice: raw in, sorted hits out, consolidated tracks out."""
+    return raw_bytes + 18 * H + 2 * 4 * N_MP * n + 18 * TH + 4 * tracks_all + 4 * (tracks_all + 1) + tracks_all
+
+
+def cpu_baseline(slices, geometry, target_s):
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import cpu_checkers
+    kind = "reference" if cpu_checkers.available("ref") else "port"
+    chk = cpu_checkers.load("ref" if kind == "reference" else "oracle")
+    threads = os.cpu_count() or 1
+    s = slices[0]
+    cal_n = min(100, s.n_events)
+    t1 = chk.time(s, geometry, cal_n, 1, 1)
+    rate1 = cal_n / max(t1, 1e-6)
+    slice_size = 500
+    n_slices = max(threads, int(rate1 * threads * target_s / slice_size))
+    n_slices = min(n_slices, s.n_events // slice_size)
+    wall = chk.time(s, geometry, slice_size, n_slices, threads)
+    value = n_slices * slice_size / wall
+    cpu_model = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                cpu_model = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{n_slices * slice_size} events of the same workload (slices of {slice_size}, "
+                      f"one slice per thread at a time), {wall:.1f} s wall; single-thread "
+                      f"{rate1:.0f} events/s; CPU: {cpu_model}"}
+
+
+# ----------------------------------------------------------------------------------
+# reference arm: the reference's CPU build on the host cores
+# ----------------------------------------------------------------------------------
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from allen_b200 import _native
+    geometry = _native.default_geometry()
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import cpu_checkers
+    kind = "reference" if cpu_checkers.available("ref") else "port"
+    chk = cpu_checkers.load("ref" if kind == "reference" else "oracle")
+    # bounded sample per step, sized from a single-thread calibration
+    cal = generate_slices(200, 200, args.seed)[0]
+    t1 = chk.time(cal, geometry, 100, 1, 1)
+    rate1 = 100 / max(t1, 1e-6)
+    slice_size = 500
+    per_step = max(threads * slice_size, int(rate1 * threads * 8.0 / slice_size) * slice_size)
+    per_step = min(per_step, args.events)
+    s = generate_slices(per_step, per_step, args.seed)[0]
+    for _ in range(args.warmup):
+        chk.time(s, geometry, slice_size, per_step // slice_size, threads)
+    times = [chk.time(s, geometry, slice_size, per_step // slice_size, threads) for _ in range(args.steps)]
+    total = sum(times)
+    value = args.steps * per_step / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"VELO plain chain, synthetic events nu=7.6, CPU sample of {per_step} events per step "
+                               f"(slices of {slice_size}) of the 100k-event workload", "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{per_step} events per step, slices of {slice_size}, one slice per thread"},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    world, rank, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    from allen_b200 import _native
+    from allen_b200.chain import VeloChain, upload
+    from allen_b200.rawbanks import super_pixels_per_event
+
+    geometry = _native.default_geometry()
+    seed = args.seed + 1_000_003 * rank
+    slices = generate_slices(args.events, args.slice, seed)
+    dev = [upload(s) for s in slices]
+    sp_max = max(int(super_pixels_per_event(s).sum()) for s in slices)
+    chain = VeloChain(geometry)
+    chain.reserve(max(s.n_events for s in slices), sp_max + 64, max(s.raw.nbytes for s in slices) + 64)
+    chain.set_timing(True)
+    stream = torch.cuda.current_stream()
+
+    # per-slice counts for the byte model (one untimed pass)
+    counts = []
+    for s, d in zip(slices, dev):
+        chain.run(d, use_graph=True)
+        t = chain.synchronize()
+        out = chain.device_outputs()
+        n = s.n_events
+        cn = chain._fetch(out["dev_module_cluster_num"], 4 * N_MP * n, np.uint32)
+        at = chain._fetch(out["dev_atomics_velo"], 4 * 3 * n, np.uint32).reshape(-1, 3)
+        raw_bytes = s.raw.nbytes + s.offsets.nbytes + s.sizes.nbytes + s.types.nbytes
+        counts.append(dict(n=n, raw_bytes=raw_bytes, T=t["host_total_number_of_velo_clusters"], H=int(cn.sum()),
+                           n4=t["host_number_of_velo_tracks_at_least_four_hits"], n3_all=int(at[:, 0].sum()),
+                           n3_out=t["host_number_of_three_hit_tracks_filtered"],
+                           TH=t["host_accumulated_number_of_hits_in_velo_tracks"],
+                           tracks_all=t["host_number_of_reconstructed_velo_tracks"]))
+
+    def step():
+        for d in dev:
+            chain.run(d, use_graph=True)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    totals_last = chain.synchronize(check=False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    events_step = sum(c["n"] for c in counts)
+    value = world * events_step * args.steps / (ms / 1e3)
+
+    # per-kernel durations of the last step (CUDA events captured inside the graphs)
+    try:
+        ktimes, runs = chain.kernel_times()
+    except Exception as exc:  # keep the throughput line even without per-kernel timing
+        print(f"kernel timing unavailable: {exc}", file=sys.stderr)
+        ktimes, runs = {}, 0
+    kb = [kernel_bytes(**c) for c in counts]
+    per_kernel = {}
+    for name, total_ms in ktimes.items():
+        avg = total_ms / max(runs, 1)
+        entry = {"ms_per_launch": round(avg, 4), "share": None}
+        if name in kb[0]:
+            b = sum(k[name] for k in kb) / len(kb)
+            entry["bytes_per_launch"] = int(b)
+            entry["gbs"] = round(b / (avg / 1e3) / 1e9, 1) if avg > 0 else None
+        per_kernel[name] = entry
+    tot = sum(v["ms_per_launch"] for v in per_kernel.values())
+    for v in per_kernel.values():
+        v["share"] = round(v["ms_per_launch"] / tot, 4) if tot else None
+    timed = [k for k in per_kernel if "bytes_per_launch" in per_kernel[k]]
+    dominant = max(timed, key=lambda k: per_kernel[k]["ms_per_launch"]) if timed else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    ach = per_kernel[dominant]["gbs"] if dominant else None
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(REPO, "profiles", "dram_traffic.json")))
+        per_unit = prof.get(dominant, {}).get("dram_bytes_per_event")
+        if per_unit:
+            traffic = int(per_unit * events_step / len(counts))
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4) if ach else None, "traffic": traffic,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    chain_gbs = sum(chain_bytes(c["n"], c["raw_bytes"], c["H"], c["TH"], c["tracks_all"]) for c in counts) \
+        * args.steps / (ms / 1e3) / 1e9
+
+    # end to end through the public API from page-locked host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        pinned = [pin(s) for s in slices]
+        for s in pinned:
+            chain.run_host(s)
+        torch.cuda.synchronize()
+        e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        up = down = 0
+        e_steps = max(1, min(args.steps, 3))
+        e_start.record(stream)
+        for _ in range(e_steps):
+            for s in pinned:
+                _, _, u, d = chain.run_host(s)
+                up += u
+                down += d
+        e_end.record(stream)
+        torch.cuda.synchronize()
+        e_ms = e_start.elapsed_time(e_end)
+        if world > 1:
+            t = torch.tensor([e_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": round(world * events_step * e_steps / (e_ms / 1e3), 1), "unit": UNIT,
+               "h2d_bytes_per_step": int(up / e_steps), "d2h_bytes_per_step": int(down / e_steps),
+               "steps": e_steps}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(slices, geometry, args.cpu_seconds)
+
+    if rank == 0:
+        c0 = counts[0]
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {
+                "workload": f"VELO plain chain (SP decode + masked clustering, phi sort, search_by_triplet, "
+                            f"three-hit filter, consolidation), {args.events} synthetic events per GPU at nu=7.6 "
+                            f"in slices of {args.slice}, raw banks resident in HBM",
+                "events_per_step": events_step * world, "slice": args.slice,
+                "l2": "inputs larger than L2 (raw banks of a step: %.2f GB)" % (sum(c['raw_bytes'] for c in counts) / 1e9),
+                "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                "mode": "plain", "cuda_graph": True,
+                "per_event": {"super_pixels": round(sp_max / max(s.n_events for s in slices), 1),
+                              "clusters": round(c0["H"] / c0["n"], 1),
+                              "tracks": round(c0["tracks_all"] / c0["n"], 1)},
+            },
+            "roofline": roofline,
+            "chain_hbm_gbs": round(chain_gbs, 1),
+            "kernels": per_kernel,
+            "gpu_launches": len(per_kernel) * len(dev) * args.steps,
+            "clocks": clocks.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "device_flags": totals_last["device_flags"],
+        }
+        print(json.dumps(line), flush=True)
+    chain.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
