@@ -189,9 +189,9 @@ struct VeloChain {
 
   // launch configuration (autotuned by the Python layer)
   unsigned estimate_blob_bytes = 32 * 1024;
-  unsigned cluster_blob_bytes = 24 * 1024;
+  unsigned cluster_blob_bytes = 16 * 1024;
   unsigned cluster_stage_capacity = 3072;
-  unsigned search_hit_capacity = 2560;
+  unsigned search_hit_capacity = 3072;
 
   // workspace
   DeviceBuffer<unsigned long long> bank_index_key;
@@ -199,7 +199,7 @@ struct VeloChain {
   DeviceBuffer<unsigned> number_of_candidates, candidates_offsets, estimated, candidate_num, event_estimate,
     event_base, offsets_est, cluster_num, atomics, n_tracks, offsets_tracks, n_three_out, offsets_three,
     event_track_hits, event_track_hit_base, offsets_all, track_hit_number, offsets_hit_number;
-  DeviceBuffer<char> sorted, staging, track_hits;
+  DeviceBuffer<char> sorted, staging, track_hits, hit_scratch;
   DeviceBuffer<velo::TrackHits> tracks;
   DeviceBuffer<velo::TrackletHits> three_hit, three_out;
   DeviceBuffer<uint8_t> hit_used, accepted;
@@ -291,7 +291,7 @@ namespace {
     cp.smem_blob_bytes = c->cluster_blob_bytes;
     cp.smem_cluster_capacity = c->cluster_stage_capacity;
     cp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
-    const unsigned cluster_smem = ((c->cluster_stage_capacity * element_size + 15u) & ~15u) + c->cluster_blob_bytes;
+    const unsigned cluster_smem = cluster_sort_blob_offset(c->cluster_stage_capacity) + c->cluster_blob_bytes;
     cluster_sort_kernel<<<n, decode_threads, cluster_smem, stream>>>(cp);
     VELO_CUDA(cudaGetLastError());
     VELO_CUDA(mark());
@@ -314,8 +314,9 @@ namespace {
     sp.event_track_hits = c->event_track_hits.p;
     sp.status = c->status.p;
     sp.smem_hit_capacity = c->search_hit_capacity;
+    sp.hit_scratch = c->hit_scratch.p;
     sp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
-    const unsigned search_smem = ((c->search_hit_capacity * element_size + 15u) & ~15u) + c->search_hit_capacity;
+    const unsigned search_smem = c->search_hit_capacity * search_hit_bytes;
     search_by_triplet_kernel<<<n, search_threads, search_smem, stream>>>(sp);
     VELO_CUDA(cudaGetLastError());
     VELO_CUDA(mark());
@@ -369,8 +370,8 @@ namespace {
   VeloStatus configure_kernels(VeloChain* c)
   {
     using namespace velo;
-    const int cluster_smem = int(((c->cluster_stage_capacity * element_size + 15u) & ~15u) + c->cluster_blob_bytes);
-    const int search_smem = int(((c->search_hit_capacity * element_size + 15u) & ~15u) + c->search_hit_capacity);
+    const int cluster_smem = int(cluster_sort_blob_offset(c->cluster_stage_capacity) + c->cluster_blob_bytes);
+    const int search_smem = int(c->search_hit_capacity * search_hit_bytes);
     VELO_CUDA(cudaFuncSetAttribute(estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c->estimate_blob_bytes)));
     VELO_CUDA(cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cluster_smem));
     VELO_CUDA(cudaFuncSetAttribute(search_by_triplet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, search_smem));
@@ -491,7 +492,8 @@ VeloStatus velo_chain_reserve(
   RES(c->track_hit_number, tracks)
   RES(c->offsets_hit_number, tracks + 1)
   RES(c->sorted, velo::element_size * T)
-  RES(c->staging, 20 * T)
+  RES(c->staging, 24 * T)
+  RES(c->hit_scratch, 16 * T)
   RES(c->track_hits, velo::element_size * track_hits)
   RES(c->tracks, tracks)
   RES(c->three_hit, tracks)
@@ -740,6 +742,7 @@ void velo_chain_destroy(VeloChain* c)
   c->offsets_hit_number.release();
   c->sorted.release();
   c->staging.release();
+  c->hit_scratch.release();
   c->track_hits.release();
   c->tracks.release();
   c->three_hit.release();

@@ -522,6 +522,15 @@ namespace velo {
   // ------------------------------------------------------------------------------------
   // cluster_sort_kernel
   // ------------------------------------------------------------------------------------
+  __device__ __forceinline__ unsigned sort_bucket(int16_t phi) { return static_cast<unsigned>(phi + 32768) >> 9; }
+
+  // u16 counters packed two per 32-bit word; returns the previous count of counter b.
+  __device__ __forceinline__ uint16_t count_in_bucket(uint16_t* counters, unsigned b)
+  {
+    const unsigned shift = 16 * (b & 1u);
+    const uint32_t old = atomicAdd(reinterpret_cast<uint32_t*>(counters) + (b >> 1), 1u << shift);
+    return static_cast<uint16_t>(old >> shift);
+  }
   __global__ void __launch_bounds__(decode_threads) cluster_sort_kernel(ClusterSortParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
@@ -529,6 +538,7 @@ namespace velo {
     __shared__ unsigned region[n_module_pairs + 1]; // estimated start of each module pair, event-relative
     __shared__ unsigned mp_count[n_module_pairs];
     __shared__ unsigned warp_sums[33];
+    __shared__ unsigned sorted_total;
     __shared__ __align__(8) uint64_t bar;
 
     const unsigned e = blockIdx.x;
@@ -560,13 +570,19 @@ namespace velo {
     if (e == n - 1 && threadIdx.x == 0) p.offsets_estimated_input_size[n * n_module_pairs] = T;
 
     const unsigned est_total = region[n_module_pairs];
-    // Staging of the unsorted clusters: shared memory when they fit, else the event's
-    // slice of the global staging buffer (20 bytes per estimated cluster, so that every
-    // event's slice starts 4-byte aligned).  The blob sits after the staging area.
+    // Staging of the unsorted clusters (18 bytes each) plus two u16 per cluster for the
+    // sort: shared memory when they fit, else the event's slice of the global staging
+    // buffer (24 bytes per estimated cluster).  Bucket counters and the blob follow.
     const bool staged_in_smem = est_total <= p.smem_cluster_capacity;
-    const unsigned staging_bytes = ((p.smem_cluster_capacity * element_size) + 15u) & ~15u;
-    ClusterView st {staged_in_smem ? reinterpret_cast<char*>(dsmem) : p.staging + size_t(20) * base, est_total};
-    unsigned char* blob = dsmem + staging_bytes;
+    const unsigned cap = staged_in_smem ? p.smem_cluster_capacity : est_total;
+    char* stage_base = staged_in_smem ? reinterpret_cast<char*>(dsmem) : p.staging + size_t(24) * base;
+    ClusterView st {stage_base, est_total};
+    uint16_t* slot_in_bucket = reinterpret_cast<uint16_t*>(stage_base + size_t(element_size) * cap);
+    uint16_t* members = slot_in_bucket + cap;
+    uint16_t* bucket_start = reinterpret_cast<uint16_t*>(dsmem + cluster_sort_counter_offset(p.smem_cluster_capacity));
+    unsigned char* blob = dsmem + cluster_sort_blob_offset(p.smem_cluster_capacity);
+    for (unsigned i = threadIdx.x; i < sort_counters / 2; i += blockDim.x)
+      reinterpret_cast<uint32_t*>(bucket_start)[i] = 0;
 
     unsigned n_words;
     const uint32_t* words = stage_event(p.in, ev, blob, p.smem_blob_bytes, &bar, p.status, n_words);
@@ -593,6 +609,7 @@ namespace velo {
             st.y(i) = o.y;
             st.z(i) = o.z;
             st.phi(i) = o.phi;
+            slot_in_bucket[i] = count_in_bucket(bucket_start, mp * sort_buckets + sort_bucket(o.phi));
           }
           else {
             set_error(p.status, err_cluster_capacity);
@@ -630,6 +647,7 @@ namespace velo {
             st.y(i) = o.y;
             st.z(i) = o.z;
             st.phi(i) = o.phi;
+            slot_in_bucket[i] = count_in_bucket(bucket_start, cmp * sort_buckets + sort_bucket(o.phi));
           }
           else {
             set_error(p.status, err_cluster_capacity);
@@ -639,27 +657,69 @@ namespace velo {
     }
     __syncthreads();
 
-    // Rank by (phi, id) inside each module pair (SortByPhi.cu:104-122) and write the
-    // sorted container at its final position.
+    // Sort by (phi, id) inside each module pair (SortByPhi.cu:104-122).  The reference
+    // ranks every pair of clusters; here clusters were counted into 128 phi buckets per
+    // module pair while staged, so a scan of the counters places every bucket and a
+    // cluster's rank is its bucket's start plus the number of smaller (phi, id) keys in the
+    // same bucket - the same position as the reference's full count.
+    {
+      const unsigned per = (sort_counters + blockDim.x - 1) / blockDim.x;
+      unsigned v[16];
+      unsigned sum = 0;
+      for (unsigned q = 0; q < per; ++q) {
+        const unsigned b = threadIdx.x * per + q;
+        v[q & 15] = b < sort_counters ? bucket_start[b] : 0u;
+        sum += v[q & 15];
+      }
+      unsigned total;
+      unsigned excl = block_exclusive_scan(sum, warp_sums, &total);
+      if (threadIdx.x == 0) sorted_total = total;
+      for (unsigned q = 0; q < per; ++q) {
+        const unsigned b = threadIdx.x * per + q;
+        if (b < sort_counters) bucket_start[b] = static_cast<uint16_t>(excl);
+        excl += v[q & 15];
+      }
+    }
+    __syncthreads();
+    auto module_pair_of = [&](unsigned i) {
+      unsigned lo = 0, hi = n_module_pairs;
+      while (hi - lo > 1) {
+        const unsigned mid = (lo + hi) / 2;
+        if (region[mid] <= i) lo = mid;
+        else hi = mid;
+      }
+      return lo;
+    };
+    for (unsigned i = threadIdx.x; i < est_total; i += blockDim.x) {
+      const unsigned mp = module_pair_of(i);
+      const unsigned count = min(mp_count[mp], region[mp + 1] - region[mp]);
+      if (i - region[mp] >= count) continue;
+      const unsigned b = mp * sort_buckets + sort_bucket(st.phi(i));
+      const unsigned q = bucket_start[b] + slot_in_bucket[i];
+      if (q < cap) members[q] = static_cast<uint16_t>(i);
+    }
+    __syncthreads();
     ClusterView out {p.sorted_container, T};
     for (unsigned i = threadIdx.x; i < est_total; i += blockDim.x) {
-      unsigned mp = 0;
-#pragma unroll 1
-      while (mp + 1 < n_module_pairs && region[mp + 1] <= i)
-        ++mp;
+      const unsigned mp = module_pair_of(i);
       const unsigned count = min(mp_count[mp], region[mp + 1] - region[mp]);
-      const unsigned local = i - region[mp];
-      if (local >= count) continue;
+      if (i - region[mp] >= count) continue;
       const int16_t phi = st.phi(i);
       const uint32_t id = st.id(i);
-      unsigned position = 0;
-      const unsigned r0 = region[mp];
-      for (unsigned j = 0; j < count; ++j) {
-        const int16_t other = st.phi(r0 + j);
-        const uint32_t other_id = st.id(r0 + j);
-        position += phi > other || (j != local && phi == other && id > other_id);
+      const unsigned b = mp * sort_buckets + sort_bucket(phi);
+      const unsigned b_end = min(b + 1 < sort_counters ? unsigned(bucket_start[b + 1]) : sorted_total, cap);
+      unsigned position = bucket_start[b] - bucket_start[mp * sort_buckets];
+      for (unsigned q = bucket_start[b]; q < b_end; ++q) {
+        const unsigned j = members[q];
+        if (j == i || j >= est_total) continue;
+        const int16_t other = st.phi(j);
+        position += phi > other || (phi == other && id > st.id(j));
       }
-      const unsigned dst = base + r0 + position;
+      if (position >= count) {
+        set_error(p.status, err_cluster_capacity);
+        continue;
+      }
+      const unsigned dst = base + region[mp] + position;
       out.id(dst) = id;
       out.phi(dst) = phi;
       out.x(dst) = st.x(i);

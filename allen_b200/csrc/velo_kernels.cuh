@@ -29,7 +29,7 @@ namespace velo {
     unsigned* offsets_estimated_input_size;     // [26 N + 1] dev_offsets_estimated_input_size
     unsigned* module_cluster_num;               // [26 N]     dev_module_cluster_num
     char* sorted_container;                     // [18 T]     dev_sorted_velo_cluster_container
-    char* staging;                              // [20 T]     fallback staging for large events
+    char* staging;                              // [24 T]     fallback staging for large events
     unsigned* status;
     unsigned smem_blob_bytes;
     unsigned smem_cluster_capacity;             // clusters staged in shared memory per event
@@ -56,6 +56,7 @@ namespace velo {
     unsigned* status;
     unsigned smem_hit_capacity;                   // hits staged in shared memory per event
     unsigned cluster_capacity;                    // allocated T of the containers
+    char* hit_scratch;                            // [16 T] staging of events above the capacity
   };
 
   // ---- copy_track_hit_number + consolidate_tracks, one event per CTA ----
@@ -89,6 +90,19 @@ namespace velo {
     ScanJob jobs[4];
   };
 
+  // Dynamic shared memory of cluster_sort_kernel for a staging capacity of `cap` clusters:
+  // [cap x 18 B clusters][cap x u16 slot in bucket][cap x u16 members][u16 bucket counters][blob]
+  constexpr unsigned sort_buckets = 128;
+  constexpr unsigned sort_counters = n_module_pairs * sort_buckets;
+  __host__ __device__ constexpr unsigned cluster_sort_counter_offset(unsigned cap)
+  {
+    return ((cap * (element_size + 4)) + 15u) & ~15u;
+  }
+  __host__ __device__ constexpr unsigned cluster_sort_blob_offset(unsigned cap)
+  {
+    return cluster_sort_counter_offset(cap) + ((sort_counters * 2 + 15u) & ~15u);
+  }
+
   __global__ void estimate_kernel(EstimateParams p);
   __global__ void cluster_sort_kernel(ClusterSortParams p);
   __global__ void search_by_triplet_kernel(SearchParams p);
@@ -98,6 +112,8 @@ namespace velo {
   constexpr unsigned decode_threads = 256;
   constexpr unsigned scan_threads = 1024;
   constexpr unsigned consolidate_threads = 256;
-  constexpr unsigned search_threads = 128;
+  constexpr unsigned search_threads = 256;
+  constexpr unsigned search_lanes_per_seed = 2;
+  constexpr unsigned search_hit_bytes = 15; // x, y, z, phi, flags per staged hit
 
 } // namespace velo

@@ -5,27 +5,43 @@
 // find_forward_candidate, track_seeding, track_forwarding) and
 // ThreeHitTracksFilter.cu:48-169.
 //
-// Design.  The event's sorted hits (id, x, y, z, phi) and the hit_used flags are staged
-// in shared memory, together with the 2048-entry ring of tracks to follow and the
-// tracklets, so the 24 barrier-separated steps run out of shared memory.  Within a step
-// every seed candidate (h1) and every track to follow is independent: seeding only reads
-// hit_used, forwarding only writes it, and each track to follow owns its track.  So each
-// step runs one thread per item and then assigns output slots (ring entries, track numbers,
-// three-hit entries) with a block-wide ordered scan, in item order.  That is the order the
-// reference's sequential execution produces, so the track containers come out
-// bit-identical to the reference CPU build, not merely equal as sets.
+// Design.
+//  * The event's sorted hits are staged once as structure-of-arrays (x, y, z, phi and a
+//    flag byte holding hit_used and the module parity that forwarding needs) in shared
+//    memory: 15 bytes per hit.  Events above the shared-memory capacity use the same
+//    layout in a global scratch slice, through the same generic pointers.
+//  * Within a step every seed candidate (h1) and every track to follow is independent:
+//    seeding only reads hit_used, forwarding only writes it, and each track to follow
+//    owns its track.  Seeding runs LPH lanes per h1: the lanes walk the pendulum of h0
+//    candidates together (ballot), each lane extrapolates its own candidates, and a
+//    shuffle reduction keeps the best (scatter, candidate order) - the same choice as the
+//    reference's sequential loop.  Forwarding runs one thread per track.
+//  * Output slots (ring entries, track numbers, three-hit entries) are assigned by a
+//    block-wide ordered scan in item order, which is the reference's sequential order, so
+//    the track containers come out bit-identical to the reference CPU build.
+//  * The ring of tracks to follow (2048 entries, as the reference) keeps a seed's three
+//    hits in the entry itself; each track's last two hits and hit count live in shared
+//    memory, so forwarding reads no global memory.  Tracks are written to dev_tracks
+//    as they grow.
+//  * Leftmost binary searches over a module pair's phi go through a 128-bucket table
+//    per module pair, built once per event, plus a short scan: same index, fewer loads.
 #include "velo_kernels.cuh"
 
 namespace velo {
 
-  constexpr unsigned seed_bit = 0x80000000u;
-  constexpr unsigned track_number_mask = 0x0FFFFFFFu;
-  constexpr unsigned skipped_mask = 0x70000000u;
+  constexpr uint64_t seed_flag = 1ull << 63;
+  constexpr unsigned skipped_shift = 60;
+  constexpr uint64_t track_number_mask64 = 0x0FFFFFFFull;
+  constexpr unsigned max_tail_tracks = 1024; // tracks whose tail lives in shared memory
+  constexpr unsigned n_buckets = 128;
+  constexpr uint8_t flag_used = 1;
+  constexpr uint8_t flag_odd_module = 2;
 
   struct ModulePair {
     unsigned hit_start;
     unsigned hit_num;
     float z[2];
+    unsigned mp;
   };
 
   struct SearchShared {
@@ -36,41 +52,31 @@ namespace velo {
     unsigned local_hits;  // atomics::local_number_of_hits
     unsigned n_tracks;
     unsigned track_hits; // sum of hitsNum over the >= 4 hit tracks
-    unsigned ttf[max_tracks_to_follow];
-    TrackletHits tracklets[max_tracks_to_follow];
+    unsigned filter_count;
+    uint64_t ring[max_tracks_to_follow];
+    uint32_t tail[max_tail_tracks]; // last two hits of a track (hit[n-2] | hit[n-1] << 16)
+    uint8_t tail_n[max_tail_tracks];
+    uint16_t bucket[n_module_pairs][n_buckets + 1];
   };
 
-  // Hits of one event: a cluster view with an index offset (0 in shared memory,
-  // the event's hit offset in the global container).
-  struct Hits {
-    ClusterView v;
-    unsigned offset;
-    __device__ __forceinline__ float x(unsigned i) const { return v.x(offset + i); }
-    __device__ __forceinline__ float y(unsigned i) const { return v.y(offset + i); }
-    __device__ __forceinline__ float z(unsigned i) const { return v.z(offset + i); }
-    __device__ __forceinline__ uint32_t id(unsigned i) const { return v.id(offset + i); }
-    __device__ __forceinline__ int16_t phi(unsigned i) const { return v.phi(offset + i); }
-    __device__ __forceinline__ const int16_t* phis() const { return v.phi_begin() + offset; }
+  struct HitsSoA {
+    const float* x;
+    const float* y;
+    const float* z;
+    const int16_t* phi;
+    uint8_t* flags;
   };
 
-  struct Forward {
-    int16_t candidate;
-    int16_t phi;
-  };
+  __device__ __forceinline__ unsigned bucket_of(int16_t v) { return static_cast<unsigned>(v + 32768) >> 9; }
 
-  // SearchByTriplet.cu:272-292
-  __device__ __forceinline__ Forward find_forward_candidate(
-    const Constants& k, const ModulePair& mp, const int16_t* phis, float h0x, float h0y, float tx, float ty, float dz)
+  // binary_search_leftmost (BinarySearch.cuh:15-30) through the bucket table of the
+  // module pair: the first index with phi >= value.
+  __device__ __forceinline__ int leftmost(const uint16_t* table, const int16_t* phis, unsigned n, int16_t value)
   {
-    const float predx = tx * dz;
-    const float predy = ty * dz;
-    const float xp = h0x + predx;
-    const float yp = h0y + predy;
-    Forward f;
-    f.phi = hit_phi_16(k, xp, yp);
-    f.candidate = static_cast<int16_t>(binary_search_leftmost(
-      phis + mp.hit_start, mp.hit_num, static_cast<int16_t>(f.phi - static_cast<int16_t>(k.phi_tolerance_i16))));
-    return f;
+    unsigned i = table[bucket_of(value)];
+    while (i < n && phis[i] < value)
+      ++i;
+    return static_cast<int>(i);
   }
 
   __device__ __forceinline__ bool phi_outside(int16_t phi, int16_t extrapolated, int16_t tol)
@@ -80,91 +86,140 @@ namespace velo {
     return abs_diff > tol;
   }
 
-  // One seed candidate h1 (SearchByTriplet.cu:325-445); returns true with the best
-  // (h0, h2) when a triplet below max_scatter exists.
-  __device__ __forceinline__ bool seed_one(
+  struct Extrapolation {
+    int start;   // first h2 candidate (find_forward_candidate, SearchByTriplet.cu:272-292)
+    int16_t phi; // extrapolated phi
+  };
+
+  __device__ __forceinline__ Extrapolation extrapolate(
     const Constants& k,
-    const Hits& h,
-    const uint8_t* used,
-    const ModulePair& prev,
+    const SearchShared& s,
+    const HitsSoA& h,
     const ModulePair& next,
-    unsigned h1,
-    unsigned n_candidates,
-    uint16_t& best_h0,
-    uint16_t& best_h2)
+    float h0x,
+    float h0y,
+    float tx,
+    float ty,
+    float dz)
   {
-    const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
-    float best_fit = k.max_scatter;
-    best_h0 = 0;
-    best_h2 = 0;
-    const float h1x = h.x(h1), h1y = h.y(h1), h1z = h.z(h1);
-    const int16_t h1_phi = h.phi(h1);
-    const int16_t* phis = h.phis();
-    int phi_index = binary_search_leftmost(phis + prev.hit_start, prev.hit_num, h1_phi);
-    const float dz_next = next.z[0] - prev.z[0];
-    unsigned found = 0;
-    for (unsigned i = 0; i < prev.hit_num && found < n_candidates; ++i) {
-      const int diff = (i & 1u) ? static_cast<int>(i) : -static_cast<int>(i);
-      phi_index += diff;
-      const unsigned in_bounds =
-        phi_index < 0 ? static_cast<unsigned>(phi_index) + prev.hit_num :
-                        (phi_index >= static_cast<int>(prev.hit_num) ?
-                           static_cast<unsigned>(phi_index - static_cast<int>(prev.hit_num)) :
-                           static_cast<unsigned>(phi_index));
-      const unsigned h0 = prev.hit_start + in_bounds;
-      if (used[h0]) continue;
-      ++found;
-      // the reference collects the candidates first and then visits them in the same order
-      const float h0x = h.x(h0), h0y = h.y(h0), h0z = h.z(h0);
-      const float td = __fdiv_rn(1.0f, h1z - h0z);
-      const float txn = h1x - h0x;
-      const float tyn = h1y - h0y;
-      const float tx = txn * td;
-      const float ty = tyn * td;
-      const Forward f = find_forward_candidate(k, next, phis, h0x, h0y, tx, ty, dz_next);
-      for (unsigned j = 0; j < next.hit_num; ++j) {
-        const unsigned ib = (static_cast<unsigned>(static_cast<int>(f.candidate)) + j) % next.hit_num;
-        const unsigned h2 = next.hit_start + ib;
-        if (phi_outside(h.phi(h2), f.phi, tol)) break;
-        if (used[h2]) continue;
-        const float dz = h.z(h2) - h0z;
-        const float predx = h0x + tx * dz;
-        const float predy = h0y + ty * dz;
-        const float dx = predx - h.x(h2);
-        const float dy = predy - h.y(h2);
-        const float scatter = dx * dx + dy * dy;
-        if (scatter < best_fit) {
-          best_fit = scatter;
-          best_h0 = static_cast<uint16_t>(h0);
-          best_h2 = static_cast<uint16_t>(h2);
-        }
-      }
-    }
-    return best_fit < k.max_scatter;
+    const float predx = tx * dz;
+    const float predy = ty * dz;
+    const float xp = h0x + predx;
+    const float yp = h0y + predy;
+    Extrapolation x;
+    x.phi = hit_phi_16(k, xp, yp);
+    const int16_t lo = static_cast<int16_t>(x.phi - static_cast<int16_t>(k.phi_tolerance_i16));
+    // find_forward_candidate returns the index as int16
+    x.start = static_cast<int16_t>(leftmost(s.bucket[next.mp], h.phi + next.hit_start, next.hit_num, lo));
+    return x;
   }
 
-  // Seeding over the current module pair (SearchByTriplet.cu:298-446).
-  __device__ void seeding(SearchShared& s, const Constants& k, const Hits& h, const uint8_t* used, unsigned n_candidates)
+  // One h0 candidate of a seed (SearchByTriplet.cu:374-432): updates (best_fit, best_c,
+  // best_h0, best_h2) with strict improvement, in window order.
+  __device__ __forceinline__ void seed_candidate(
+    const Constants& k,
+    const SearchShared& s,
+    const HitsSoA& h,
+    const ModulePair& prev,
+    const ModulePair& next,
+    float h1x,
+    float h1y,
+    float h1z,
+    unsigned h0,
+    unsigned c,
+    float& best_fit,
+    unsigned& best_c,
+    unsigned& best_h0,
+    unsigned& best_h2)
+  {
+    const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
+    const float h0x = h.x[h0], h0y = h.y[h0], h0z = h.z[h0];
+    const float td = __fdiv_rn(1.0f, h1z - h0z);
+    const float txn = h1x - h0x;
+    const float tyn = h1y - h0y;
+    const float tx = txn * td;
+    const float ty = tyn * td;
+    const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[0] - prev.z[0]);
+    for (unsigned j = 0; j < next.hit_num; ++j) {
+      const unsigned h2 = next.hit_start + (static_cast<unsigned>(f.start) + j) % next.hit_num;
+      if (phi_outside(h.phi[h2], f.phi, tol)) break;
+      if (h.flags[h2] & flag_used) continue;
+      const float dz = h.z[h2] - h0z;
+      const float predx = h0x + tx * dz;
+      const float predy = h0y + ty * dz;
+      const float dx = predx - h.x[h2];
+      const float dy = predy - h.y[h2];
+      const float scatter = dx * dx + dy * dy;
+      if (scatter < best_fit) {
+        best_fit = scatter;
+        best_c = c;
+        best_h0 = h0;
+        best_h2 = h2;
+      }
+    }
+  }
+
+  // Seeding over the current module pair (SearchByTriplet.cu:298-446), LPH lanes per h1.
+  template<unsigned LPH>
+  __device__ void seeding(SearchShared& s, const Constants& k, const HitsSoA& h, unsigned n_candidates)
   {
     const ModulePair prev = s.md[0], cur = s.md[1], next = s.md[2];
-    for (unsigned c0 = 0; c0 < cur.hit_num; c0 += blockDim.x) {
-      const unsigned r = c0 + threadIdx.x;
-      bool ok = false;
-      unsigned unused = 0;
-      uint16_t bh0 = 0, bh2 = 0;
+    const unsigned groups = blockDim.x / LPH;
+    const unsigned g = threadIdx.x / LPH;
+    const unsigned l = threadIdx.x % LPH;
+    const unsigned lane0 = (threadIdx.x & 31u) & ~(LPH - 1);
+    const unsigned gmask = (LPH == 32 ? 0xFFFFFFFFu : ((1u << LPH) - 1u)) << lane0;
+    for (unsigned c0 = 0; c0 < cur.hit_num; c0 += groups) {
+      const unsigned r = c0 + g;
       const unsigned h1 = cur.hit_start + r;
-      if (r < cur.hit_num && !used[h1]) {
-        unused = 1;
-        ok = seed_one(k, h, used, prev, next, h1, n_candidates, bh0, bh2);
+      const bool valid = r < cur.hit_num && !(h.flags[h1] & flag_used);
+      float best_fit = k.max_scatter;
+      unsigned best_c = 0xFFFFFFFFu, best_h0 = 0, best_h2 = 0;
+      if (valid) {
+        const float h1x = h.x[h1], h1y = h.y[h1], h1z = h.z[h1];
+        const int p0 = leftmost(s.bucket[prev.mp], h.phi + prev.hit_start, prev.hit_num, h.phi[h1]);
+        const int n_prev = static_cast<int>(prev.hit_num);
+        unsigned found = 0;
+        for (unsigned i0 = 0; i0 < prev.hit_num && found < n_candidates; i0 += LPH) {
+          const unsigned i = i0 + l;
+          bool ok = false;
+          unsigned h0 = 0;
+          if (i < prev.hit_num) {
+            // pendulum p0, p0 + 1, p0 - 1, p0 + 2, ... with one wrap (SearchByTriplet.cu:351-370)
+            const int pos = p0 + ((i & 1u) ? static_cast<int>((i + 1) / 2) : -static_cast<int>(i / 2));
+            const int in_bounds = pos < 0 ? pos + n_prev : (pos >= n_prev ? pos - n_prev : pos);
+            h0 = prev.hit_start + static_cast<unsigned>(in_bounds);
+            ok = !(h.flags[h0] & flag_used);
+          }
+          const unsigned ballot = (__ballot_sync(gmask, ok) & gmask) >> lane0;
+          const unsigned rank = __popc(ballot & ((1u << l) - 1u));
+          if (ok && found + rank < n_candidates) {
+            seed_candidate(k, s, h, prev, next, h1x, h1y, h1z, h0, found + rank, best_fit, best_c, best_h0, best_h2);
+          }
+          found += __popc(ballot);
+        }
+#pragma unroll
+        for (unsigned o = LPH / 2; o >= 1; o /= 2) {
+          const float of = __shfl_xor_sync(gmask, best_fit, o);
+          const unsigned oc = __shfl_xor_sync(gmask, best_c, o);
+          const unsigned o0 = __shfl_xor_sync(gmask, best_h0, o);
+          const unsigned o2 = __shfl_xor_sync(gmask, best_h2, o);
+          if (of < best_fit || (of == best_fit && oc < best_c)) {
+            best_fit = of;
+            best_c = oc;
+            best_h0 = o0;
+            best_h2 = o2;
+          }
+        }
       }
+      const bool ok = valid && l == 0 && best_fit < k.max_scatter;
+      const unsigned unused = (valid && l == 0) ? 1u : 0u;
       unsigned total;
       const unsigned excl = block_exclusive_scan((ok ? 1u : 0u) | (unused << 16), s.warp_sums, &total);
       if (ok) {
         const unsigned tn = (s.ttf_counter + (excl & 0xFFFFu)) % max_tracks_to_follow;
-        s.tracklets[tn].hits[0] = bh0;
-        s.tracklets[tn].hits[1] = static_cast<uint16_t>(h1);
-        s.tracklets[tn].hits[2] = bh2;
-        s.ttf[tn] = seed_bit | tn;
+        s.ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
+                     (uint64_t(best_h2 & 0xFFFFu) << 32);
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -175,127 +230,140 @@ namespace velo {
     }
   }
 
-  // Forwarding of the tracks to follow (SearchByTriplet.cu:451-609).
+  // Forwarding of the tracks to follow (SearchByTriplet.cu:451-609), one thread per track.
   __device__ void forwarding(
     SearchShared& s,
     const Constants& k,
-    const Hits& h,
-    uint8_t* used,
+    const HitsSoA& h,
     unsigned prev_ttf,
     unsigned diff_ttf,
     TrackHits* tracks,
     unsigned track_limit,
     TrackletHits* three_hit,
-    unsigned three_limit,
     unsigned* status)
   {
     const ModulePair next = s.md[2];
     const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
-    const int16_t* phis = h.phis();
     for (unsigned c0 = 0; c0 < diff_ttf; c0 += blockDim.x) {
       const unsigned kk = c0 + threadIdx.x;
       const bool active = kk < diff_ttf;
-      unsigned full = 0, nh = 0, tn = 0;
+      uint64_t entry = 0;
+      unsigned nh = 0, tn = 0, h0n = 0, h1n = 0;
       bool is_seed = false, found = false;
-      int best_h2 = -1;
-      uint16_t t0 = 0, t1 = 0, t2 = 0;
+      unsigned best_h2 = 0;
       if (active) {
-        full = s.ttf[(prev_ttf + kk) % max_tracks_to_follow];
-        is_seed = (full & seed_bit) == seed_bit;
-        tn = full & track_number_mask;
-        uint16_t h0n, h1n;
+        entry = s.ring[(prev_ttf + kk) % max_tracks_to_follow];
+        is_seed = (entry & seed_flag) != 0;
         if (is_seed) {
-          const TrackletHits t = s.tracklets[tn];
-          t0 = t.hits[0];
-          t1 = t.hits[1];
-          t2 = t.hits[2];
           nh = 3;
-          h0n = t1;
-          h1n = t2;
-        }
-        else if (tn < track_limit) {
-          nh = tracks[tn].hits_num;
-          if (nh < 2 || nh > max_track_size) nh = 2; // unreachable with consistent containers
-          h0n = tracks[tn].hits[nh - 2];
-          h1n = tracks[tn].hits[nh - 1];
+          h0n = static_cast<unsigned>(entry >> 16) & 0xFFFFu;
+          h1n = static_cast<unsigned>(entry >> 32) & 0xFFFFu;
         }
         else {
-          // a track that did not fit its container (flagged when it was created)
-          nh = 3;
-          h0n = 0;
-          h1n = 0;
+          tn = static_cast<unsigned>(entry & track_number_mask64);
+          if (tn < max_tail_tracks) {
+            nh = s.tail_n[tn];
+            h0n = s.tail[tn] & 0xFFFFu;
+            h1n = s.tail[tn] >> 16;
+          }
+          else if (tn < track_limit) {
+            nh = tracks[tn].hits_num;
+            if (nh < 2 || nh > max_track_size) nh = 2;
+            h0n = tracks[tn].hits[nh - 2];
+            h1n = tracks[tn].hits[nh - 1];
+          }
+          else {
+            nh = 3; // a track that did not fit its container, flagged when created
+          }
         }
-        const float h0x = h.x(h0n), h0y = h.y(h0n), h0z = h.z(h0n);
-        const unsigned h0_module = ((h.id(h0n) & 0x3FC0000u) >> 18) / 4;
-        const float h1x = h.x(h1n), h1y = h.y(h1n), h1z = h.z(h1n);
+        const float h0x = h.x[h0n], h0y = h.y[h0n], h0z = h.z[h0n];
+        const unsigned odd = (h.flags[h0n] & flag_odd_module) ? 1u : 0u;
+        const float h1x = h.x[h1n], h1y = h.y[h1n], h1z = h.z[h1n];
         const float td = __fdiv_rn(1.0f, h1z - h0z);
         const float txn = h1x - h0x;
         const float tyn = h1y - h0y;
         const float tx = txn * td;
         const float ty = tyn * td;
         float best_fit = k.max_scatter;
-        const Forward f = find_forward_candidate(k, next, phis, h0x, h0y, tx, ty, next.z[h0_module % 2] - h0z);
+        const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[odd] - h0z);
         for (unsigned j = 0; j < next.hit_num; ++j) {
-          const unsigned ib = (static_cast<unsigned>(static_cast<int>(f.candidate)) + j) % next.hit_num;
-          const unsigned h2 = next.hit_start + ib;
-          if (phi_outside(h.phi(h2), f.phi, tol)) break;
-          const float dz = h.z(h2) - h0z;
+          const unsigned h2 = next.hit_start + (static_cast<unsigned>(f.start) + j) % next.hit_num;
+          if (phi_outside(h.phi[h2], f.phi, tol)) break;
+          const float dz = h.z[h2] - h0z;
           const float predx = h0x + tx * dz;
           const float predy = h0y + ty * dz;
-          const float dx = predx - h.x(h2);
-          const float dy = predy - h.y(h2);
+          const float dx = predx - h.x[h2];
+          const float dy = predy - h.y[h2];
           const float scatter = dx * dx + dy * dy;
           if (scatter < best_fit) {
             best_fit = scatter;
-            best_h2 = static_cast<int>(h2);
+            best_h2 = h2;
+            found = true;
           }
         }
-        found = best_h2 != -1;
       }
-      const unsigned skipped = (full & skipped_mask) >> 28;
+      const unsigned skipped = static_cast<unsigned>(entry >> skipped_shift) & 0x7u;
       const bool new_track = active && found && is_seed;
       const bool enqueue =
         active && ((found && nh + 1 < max_track_size) || (!found && skipped < k.max_skipped_modules));
-      const bool three = active && !found && !(skipped < k.max_skipped_modules) && nh == 3;
+      const bool three = active && !found && !(skipped < k.max_skipped_modules) && nh == 3 && is_seed;
       unsigned total;
       const unsigned excl = block_exclusive_scan(
         (new_track ? 1u : 0u) | ((enqueue ? 1u : 0u) << 10) | ((three ? 1u : 0u) << 20), s.warp_sums, &total);
       if (active) {
         unsigned track_number = tn;
         if (found) {
-          used[best_h2] = 1;
+          h.flags[best_h2] |= flag_used;
           if (is_seed) {
-            used[t0] = 1;
-            used[t1] = 1;
-            used[t2] = 1;
+            const unsigned t0 = static_cast<unsigned>(entry) & 0xFFFFu;
+            h.flags[t0] |= flag_used;
+            h.flags[h0n] |= flag_used;
+            h.flags[h1n] |= flag_used;
             track_number = s.n_tracks + (excl & 0x3FFu);
             if (track_number < track_limit) {
               TrackHits& t = tracks[track_number];
-              t.hits[0] = t0;
-              t.hits[1] = t1;
-              t.hits[2] = t2;
+              t.hits[0] = static_cast<uint16_t>(t0);
+              t.hits[1] = static_cast<uint16_t>(h0n);
+              t.hits[2] = static_cast<uint16_t>(h1n);
               t.hits[3] = static_cast<uint16_t>(best_h2);
               t.hits_num = 4;
             }
             else {
               set_error(status, err_track_capacity);
             }
+            if (track_number < max_tail_tracks) {
+              s.tail[track_number] = h1n | (best_h2 << 16);
+              s.tail_n[track_number] = 4;
+            }
           }
-          else if (tn < track_limit) {
-            tracks[tn].hits[nh] = static_cast<uint16_t>(best_h2);
-            tracks[tn].hits_num = static_cast<uint8_t>(nh + 1);
+          else {
+            if (tn < track_limit) {
+              tracks[tn].hits[nh] = static_cast<uint16_t>(best_h2);
+              tracks[tn].hits_num = static_cast<uint8_t>(nh + 1);
+            }
+            if (tn < max_tail_tracks) {
+              s.tail[tn] = h1n | (best_h2 << 16);
+              s.tail_n[tn] = static_cast<uint8_t>(nh + 1);
+            }
           }
           atomicAdd(&s.track_hits, is_seed ? 4u : 1u);
         }
         if (enqueue) {
-          const unsigned value =
-            found ? track_number : (((skipped + 1) << 28) | (full & (seed_bit | track_number_mask)));
-          s.ttf[(s.ttf_counter + ((excl >> 10) & 0x3FFu)) % max_tracks_to_follow] = value;
+          // requeued entries keep the seed's hits or the track number, with skipped + 1
+          const uint64_t value =
+            found ? uint64_t(track_number) :
+                    ((entry & ~(uint64_t(0x7) << skipped_shift)) | (uint64_t(skipped + 1) << skipped_shift));
+          s.ring[(s.ttf_counter + ((excl >> 10) & 0x3FFu)) % max_tracks_to_follow] = value;
         }
         if (three) {
           const unsigned slot = s.n_three + ((excl >> 20) & 0x3FFu);
-          if (slot < three_limit) three_hit[slot] = TrackletHits {{t0, t1, t2}};
-          else set_error(status, err_track_capacity);
+          if (slot < track_limit) {
+            three_hit[slot] = TrackletHits {
+              {static_cast<uint16_t>(entry & 0xFFFFu), static_cast<uint16_t>(h0n), static_cast<uint16_t>(h1n)}};
+          }
+          else {
+            set_error(status, err_track_capacity);
+          }
         }
       }
       __syncthreads();
@@ -309,7 +377,7 @@ namespace velo {
   }
 
   // ThreeHitTracksFilter.cu:48-107
-  __device__ __forceinline__ float means_square_fit_chi2(const Hits& h, const TrackletHits& t)
+  __device__ __forceinline__ float means_square_fit_chi2(const HitsSoA& h, const TrackletHits& t)
   {
     const float w = 6400.f;
     float s0, sx, sz, sxz, sz2, u0, uy, uz, uyz, uz2;
@@ -318,7 +386,7 @@ namespace velo {
 #pragma unroll
     for (unsigned i = 0; i < 3; ++i) {
       const unsigned hn = t.hits[i];
-      const float x = h.x(hn), y = h.y(hn), z = h.z(hn);
+      const float x = h.x[hn], y = h.y[hn], z = h.z[hn];
       const float wx_t_x = w * x, wx_t_z = w * z;
       s0 += w;
       sx += wx_t_x;
@@ -342,11 +410,11 @@ namespace velo {
 #pragma unroll
     for (unsigned i = 0; i < 3; ++i) {
       const unsigned hn = t.hits[i];
-      const float z = h.z(hn);
+      const float z = h.z[hn];
       const float x = state_x + state_tx * z;
       const float y = state_y + state_ty * z;
-      const float dx = x - h.x(hn);
-      const float dy = y - h.y(hn);
+      const float dx = x - h.x[hn];
+      const float dy = y - h.y[hn];
       chi2 += dx * dx * w + dy * dy * w;
     }
     return chi2 * 0.5f;
@@ -361,15 +429,13 @@ namespace velo {
       s.md[threadIdx.x].hit_num = num[mp];
       s.md[threadIdx.x].z[0] = __ldg(g->module_zs + 2 * mp);
       s.md[threadIdx.x].z[1] = __ldg(g->module_zs + 2 * mp + 1);
+      s.md[threadIdx.x].mp = mp;
     }
   }
 
-  __global__ void __launch_bounds__(search_threads) search_by_triplet_kernel(SearchParams p)
+  template<unsigned LPH>
+  __device__ void search_event(const SearchParams& p, SearchShared& s, unsigned char* dsmem)
   {
-    extern __shared__ __align__(128) unsigned char dsmem[];
-    __shared__ SearchShared s;
-    __shared__ unsigned filter_count;
-
     const unsigned e = blockIdx.x;
     const unsigned n = p.n_events;
     const unsigned* start = p.offsets_estimated_input_size + e * n_module_pairs;
@@ -396,44 +462,56 @@ namespace velo {
     TrackHits* tracks = p.tracks + to;
     TrackletHits* three_hit = p.three_hit_tracks + to;
 
-    // Stage hits and hit_used flags
+    // Stage the hits as SoA: shared memory when they fit, else the event's global slice
+    // (16 bytes per estimated hit, so every slice starts 16-byte aligned).
     const bool in_smem = n_hits <= p.smem_hit_capacity;
-    Hits h;
-    uint8_t* used;
-    if (in_smem) {
-      h.v = ClusterView {reinterpret_cast<char*>(dsmem), n_hits};
-      h.offset = 0;
-      used = dsmem + ((size_t(n_hits) * element_size + 15) & ~size_t(15));
+    unsigned char* base = in_smem ? dsmem : reinterpret_cast<unsigned char*>(p.hit_scratch) + size_t(16) * hit_offset;
+    const unsigned cap = in_smem ? p.smem_hit_capacity : n_hits;
+    float* xs = reinterpret_cast<float*>(base);
+    float* ys = xs + cap;
+    float* zs = ys + cap;
+    int16_t* phis = reinterpret_cast<int16_t*>(zs + cap);
+    uint8_t* flags = reinterpret_cast<uint8_t*>(phis + cap);
+    {
       const ClusterView g {const_cast<char*>(p.sorted_container), T};
       for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x) {
-        h.v.id(i) = g.id(hit_offset + i);
-        h.v.phi(i) = g.phi(hit_offset + i);
-        used[i] = 0;
+        const unsigned gi = hit_offset + i;
+        xs[i] = g.x(gi);
+        ys[i] = g.y(gi);
+        zs[i] = g.z(gi);
+        phis[i] = g.phi(gi);
+        const unsigned module = ((g.id(gi) & 0x3FC0000u) >> 18) / 4;
+        flags[i] = (module & 1u) ? flag_odd_module : 0;
       }
-      const float* src = &g.x(hit_offset);
-      float* dst = &h.v.x(0);
-      for (unsigned i = threadIdx.x; i < 3 * n_hits; i += blockDim.x)
-        dst[i] = src[i];
     }
-    else {
-      h.v = ClusterView {const_cast<char*>(p.sorted_container), T};
-      h.offset = hit_offset;
-      used = reinterpret_cast<uint8_t*>(p.hit_used) + hit_offset;
-      for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x)
-        used[i] = 0;
-    }
+    const HitsSoA h {xs, ys, zs, phis, flags};
     if (threadIdx.x == 0) {
       s.ttf_counter = 0;
       s.n_three = 0;
       s.local_hits = 0;
       s.n_tracks = 0;
       s.track_hits = 0;
+      s.filter_count = 0;
     }
+    __syncthreads();
+    // bucket tables: bucket[mp][b] = first index of the module pair with phi >= b * 512 - 32768
+    for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
+      const unsigned s0 = start[mp] - hit_offset;
+      const unsigned cnt = num[mp];
+      uint16_t* table = s.bucket[mp];
+      for (unsigned i = threadIdx.x; i <= cnt; i += blockDim.x) {
+        const unsigned lo = i == 0 ? 0u : bucket_of(phis[s0 + i - 1]) + 1;
+        const unsigned hi = i == cnt ? n_buckets : bucket_of(phis[s0 + i]);
+        for (unsigned b = lo; b <= hi; ++b)
+          table[b] = static_cast<uint16_t>(i);
+      }
+    }
+
     unsigned first = n_module_pairs - 1;
     load_module_pairs(s, p.geo, first, start, num, hit_offset);
     __syncthreads();
 
-    seeding(s, k, h, used, 8);
+    seeding<LPH>(s, k, h, 8);
 
     unsigned last_ttf = 0;
     --first;
@@ -444,11 +522,11 @@ namespace velo {
       const unsigned diff = last_ttf - prev_ttf;
       if (threadIdx.x == 0) s.local_hits = 0;
       __syncthreads();
-      forwarding(s, k, h, used, prev_ttf, diff, tracks, track_limit, three_hit, track_limit, p.status);
+      forwarding(s, k, h, prev_ttf, diff, tracks, track_limit, three_hit, p.status);
       // The ring holds 2048 entries; beyond that the reference overwrites entries it has
       // not read yet, an order-dependent outcome this kernel does not reproduce.
       if (threadIdx.x == 0 && s.ttf_counter - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
-      seeding(s, k, h, used, 4);
+      seeding<LPH>(s, k, h, 4);
       if (threadIdx.x == 0 && s.ttf_counter - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       --first;
     }
@@ -460,18 +538,24 @@ namespace velo {
       const unsigned diff = last_ttf - prev_ttf;
       for (unsigned c0 = 0; c0 < diff; c0 += blockDim.x) {
         const unsigned kk = c0 + threadIdx.x;
-        unsigned full = 0;
+        uint64_t entry = 0;
         bool seed = false;
         if (kk < diff) {
-          full = s.ttf[(prev_ttf + kk) % max_tracks_to_follow];
-          seed = (full & seed_bit) == seed_bit;
+          entry = s.ring[(prev_ttf + kk) % max_tracks_to_follow];
+          seed = (entry & seed_flag) != 0;
         }
         unsigned total;
         const unsigned excl = block_exclusive_scan(seed ? 1u : 0u, s.warp_sums, &total);
         if (seed) {
           const unsigned slot = s.n_three + excl;
-          if (slot < track_limit) three_hit[slot] = s.tracklets[full & track_number_mask];
-          else set_error(p.status, err_track_capacity);
+          if (slot < track_limit) {
+            three_hit[slot] = TrackletHits {{static_cast<uint16_t>(entry & 0xFFFFu),
+                                             static_cast<uint16_t>((entry >> 16) & 0xFFFFu),
+                                             static_cast<uint16_t>((entry >> 32) & 0xFFFFu)}};
+          }
+          else {
+            set_error(p.status, err_track_capacity);
+          }
         }
         __syncthreads();
         if (threadIdx.x == 0) s.n_three += total;
@@ -486,12 +570,11 @@ namespace velo {
       atomics[2] = s.local_hits;
       p.number_of_velo_tracks[e] = s.n_tracks;
       if (s.n_tracks > to_next - to) set_error(p.status, err_track_capacity);
-      filter_count = 0;
     }
-    if (in_smem) {
+    {
       uint8_t* g_used = reinterpret_cast<uint8_t*>(p.hit_used) + hit_offset;
       for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x)
-        g_used[i] = used[i];
+        g_used[i] = flags[i] & flag_used;
     }
     __syncthreads();
 
@@ -504,21 +587,29 @@ namespace velo {
       TrackletHits t {};
       if (i < n_in) {
         t = three_hit[i];
-        const bool any_used = used[t.hits[0]] || used[t.hits[1]] || used[t.hits[2]];
+        const bool any_used =
+          (flags[t.hits[0]] & flag_used) || (flags[t.hits[1]] & flag_used) || (flags[t.hits[2]] & flag_used);
         const float chi2 = means_square_fit_chi2(h, t);
         keep = !any_used && chi2 < k.max_chi2;
       }
       unsigned total;
       const unsigned excl = block_exclusive_scan(keep ? 1u : 0u, s.warp_sums, &total);
-      if (keep) out[filter_count + excl] = t;
+      if (keep) out[s.filter_count + excl] = t;
       __syncthreads();
-      if (threadIdx.x == 0) filter_count += total;
+      if (threadIdx.x == 0) s.filter_count += total;
       __syncthreads();
     }
     if (threadIdx.x == 0) {
-      p.number_of_three_hit_tracks_output[e] = filter_count;
-      p.event_track_hits[e] = s.track_hits + 3 * filter_count;
+      p.number_of_three_hit_tracks_output[e] = s.filter_count;
+      p.event_track_hits[e] = s.track_hits + 3 * s.filter_count;
     }
+  }
+
+  __global__ void __launch_bounds__(search_threads) search_by_triplet_kernel(SearchParams p)
+  {
+    extern __shared__ __align__(128) unsigned char dsmem[];
+    __shared__ SearchShared s;
+    search_event<search_lanes_per_seed>(p, s, dsmem);
   }
 
 } // namespace velo

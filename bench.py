@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--seed", type=int, default=2024)
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
     return p.parse_args()
 
 
@@ -335,7 +336,7 @@ def run_ours(args):
 
     # end to end through the public API from page-locked host buffers
     e2e = None
-    if rank == 0 or world > 1:
+    if not args.no_e2e:
         pinned = [pin(s) for s in slices]
         for s in pinned:
             chain.run_host(s)
