@@ -45,14 +45,8 @@ namespace velo {
   };
 
   struct SearchShared {
-    ModulePair md[3];
-    unsigned warp_sums[33];
-    unsigned ttf_counter; // atomics::tracks_to_follow
-    unsigned n_three;     // atomics::number_of_three_hit_tracks
-    unsigned local_hits;  // atomics::local_number_of_hits
-    unsigned n_tracks;
-    unsigned track_hits; // sum of hitsNum over the >= 4 hit tracks
-    unsigned filter_count;
+    unsigned scan_sums[2][32]; // double-buffered warp totals of the block scans
+    unsigned track_hits;       // sum of hitsNum over the >= 4 hit tracks
     uint64_t ring[max_tracks_to_follow];
     uint32_t tail[max_tail_tracks]; // last two hits of a track (hit[n-2] | hit[n-1] << 16)
     uint8_t tail_n[max_tail_tracks];
@@ -66,6 +60,41 @@ namespace velo {
     const int16_t* phi;
     uint8_t* flags;
   };
+
+  // The event's counters (the reference's dev_atomics_velo and track count), kept in
+  // registers: every thread holds the same values and advances them by scan totals.
+  struct Counters {
+    unsigned ttf;        // atomics::tracks_to_follow
+    unsigned n_three;    // atomics::number_of_three_hit_tracks
+    unsigned local_hits; // atomics::local_number_of_hits
+    unsigned n_tracks;   // dev_number_of_velo_tracks
+    unsigned scan_parity;
+  };
+
+  // Block-wide exclusive scan with a single barrier: warp totals go to one of two
+  // buffers, alternating per call, so a call never overwrites totals still being read.
+  __device__ __forceinline__ unsigned scan1(SearchShared& s, Counters& c, unsigned v, unsigned& total)
+  {
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= static_cast<unsigned>(o)) incl += t;
+    }
+    unsigned* buf = s.scan_sums[c.scan_parity];
+    c.scan_parity ^= 1u;
+    if (lane == 31) buf[warp] = incl;
+    __syncthreads();
+    unsigned before = 0, all = 0;
+    for (unsigned w = 0; w < n_warps; ++w) {
+      const unsigned t = buf[w];
+      before += w < warp ? t : 0u;
+      all += t;
+    }
+    total = all;
+    return before + incl - v;
+  }
 
   __device__ __forceinline__ unsigned bucket_of(int16_t v) { return static_cast<unsigned>(v + 32768) >> 9; }
 
@@ -161,9 +190,10 @@ namespace velo {
 
   // Seeding over the current module pair (SearchByTriplet.cu:298-446), LPH lanes per h1.
   template<unsigned LPH>
-  __device__ void seeding(SearchShared& s, const Constants& k, const HitsSoA& h, unsigned n_candidates)
+  __device__ void seeding(
+    SearchShared& s, Counters& cnt, const Constants& k, const HitsSoA& h, const ModulePair* md, unsigned n_candidates)
   {
-    const ModulePair prev = s.md[0], cur = s.md[1], next = s.md[2];
+    const ModulePair prev = md[0], cur = md[1], next = md[2];
     const unsigned groups = blockDim.x / LPH;
     const unsigned g = threadIdx.x / LPH;
     const unsigned l = threadIdx.x % LPH;
@@ -215,26 +245,24 @@ namespace velo {
       const bool ok = valid && l == 0 && best_fit < k.max_scatter;
       const unsigned unused = (valid && l == 0) ? 1u : 0u;
       unsigned total;
-      const unsigned excl = block_exclusive_scan((ok ? 1u : 0u) | (unused << 16), s.warp_sums, &total);
+      const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | (unused << 16), total);
       if (ok) {
-        const unsigned tn = (s.ttf_counter + (excl & 0xFFFFu)) % max_tracks_to_follow;
+        const unsigned tn = (cnt.ttf + (excl & 0xFFFFu)) % max_tracks_to_follow;
         s.ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
                      (uint64_t(best_h2 & 0xFFFFu) << 32);
       }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        s.ttf_counter += total & 0xFFFFu;
-        s.local_hits += total >> 16;
-      }
-      __syncthreads();
+      cnt.ttf += total & 0xFFFFu;
+      cnt.local_hits += total >> 16;
     }
   }
 
   // Forwarding of the tracks to follow (SearchByTriplet.cu:451-609), one thread per track.
   __device__ void forwarding(
     SearchShared& s,
+    Counters& cnt,
     const Constants& k,
     const HitsSoA& h,
+    const ModulePair& next,
     unsigned prev_ttf,
     unsigned diff_ttf,
     TrackHits* tracks,
@@ -242,7 +270,6 @@ namespace velo {
     TrackletHits* three_hit,
     unsigned* status)
   {
-    const ModulePair next = s.md[2];
     const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
     for (unsigned c0 = 0; c0 < diff_ttf; c0 += blockDim.x) {
       const unsigned kk = c0 + threadIdx.x;
@@ -308,8 +335,8 @@ namespace velo {
         active && ((found && nh + 1 < max_track_size) || (!found && skipped < k.max_skipped_modules));
       const bool three = active && !found && !(skipped < k.max_skipped_modules) && nh == 3 && is_seed;
       unsigned total;
-      const unsigned excl = block_exclusive_scan(
-        (new_track ? 1u : 0u) | ((enqueue ? 1u : 0u) << 10) | ((three ? 1u : 0u) << 20), s.warp_sums, &total);
+      const unsigned excl =
+        scan1(s, cnt, (new_track ? 1u : 0u) | ((enqueue ? 1u : 0u) << 10) | ((three ? 1u : 0u) << 20), total);
       if (active) {
         unsigned track_number = tn;
         if (found) {
@@ -319,7 +346,7 @@ namespace velo {
             h.flags[t0] |= flag_used;
             h.flags[h0n] |= flag_used;
             h.flags[h1n] |= flag_used;
-            track_number = s.n_tracks + (excl & 0x3FFu);
+            track_number = cnt.n_tracks + (excl & 0x3FFu);
             if (track_number < track_limit) {
               TrackHits& t = tracks[track_number];
               t.hits[0] = static_cast<uint16_t>(t0);
@@ -353,10 +380,10 @@ namespace velo {
           const uint64_t value =
             found ? uint64_t(track_number) :
                     ((entry & ~(uint64_t(0x7) << skipped_shift)) | (uint64_t(skipped + 1) << skipped_shift));
-          s.ring[(s.ttf_counter + ((excl >> 10) & 0x3FFu)) % max_tracks_to_follow] = value;
+          s.ring[(cnt.ttf + ((excl >> 10) & 0x3FFu)) % max_tracks_to_follow] = value;
         }
         if (three) {
-          const unsigned slot = s.n_three + ((excl >> 20) & 0x3FFu);
+          const unsigned slot = cnt.n_three + ((excl >> 20) & 0x3FFu);
           if (slot < track_limit) {
             three_hit[slot] = TrackletHits {
               {static_cast<uint16_t>(entry & 0xFFFFu), static_cast<uint16_t>(h0n), static_cast<uint16_t>(h1n)}};
@@ -366,13 +393,9 @@ namespace velo {
           }
         }
       }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        s.n_tracks += total & 0x3FFu;
-        s.ttf_counter += (total >> 10) & 0x3FFu;
-        s.n_three += (total >> 20) & 0x3FFu;
-      }
-      __syncthreads();
+      cnt.n_tracks += total & 0x3FFu;
+      cnt.ttf += (total >> 10) & 0x3FFu;
+      cnt.n_three += (total >> 20) & 0x3FFu;
     }
   }
 
@@ -420,16 +443,18 @@ namespace velo {
     return chi2 * 0.5f;
   }
 
-  __device__ __forceinline__ void load_module_pairs(
-    SearchShared& s, const Geometry* g, unsigned first, const unsigned* start, const unsigned* num, unsigned hit_offset)
+  // The three module pairs of a step (first, first - 1, first - 2), read by every thread.
+  __device__ __forceinline__ void module_pairs(
+    ModulePair* md, const Geometry* g, unsigned first, const unsigned* start, const unsigned* num, unsigned hit_offset)
   {
-    if (threadIdx.x < 3) {
-      const unsigned mp = first - threadIdx.x;
-      s.md[threadIdx.x].hit_start = start[mp] - hit_offset;
-      s.md[threadIdx.x].hit_num = num[mp];
-      s.md[threadIdx.x].z[0] = __ldg(g->module_zs + 2 * mp);
-      s.md[threadIdx.x].z[1] = __ldg(g->module_zs + 2 * mp + 1);
-      s.md[threadIdx.x].mp = mp;
+#pragma unroll
+    for (unsigned i = 0; i < 3; ++i) {
+      const unsigned mp = first - i;
+      md[i].hit_start = start[mp] - hit_offset;
+      md[i].hit_num = num[mp];
+      md[i].z[0] = __ldg(g->module_zs + 2 * mp);
+      md[i].z[1] = __ldg(g->module_zs + 2 * mp + 1);
+      md[i].mp = mp;
     }
   }
 
@@ -485,14 +510,8 @@ namespace velo {
       }
     }
     const HitsSoA h {xs, ys, zs, phis, flags};
-    if (threadIdx.x == 0) {
-      s.ttf_counter = 0;
-      s.n_three = 0;
-      s.local_hits = 0;
-      s.n_tracks = 0;
-      s.track_hits = 0;
-      s.filter_count = 0;
-    }
+    if (threadIdx.x == 0) s.track_hits = 0;
+    Counters cnt {0, 0, 0, 0, 0};
     __syncthreads();
     // bucket tables: bucket[mp][b] = first index of the module pair with phi >= b * 512 - 32768
     for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
@@ -508,33 +527,36 @@ namespace velo {
     }
 
     unsigned first = n_module_pairs - 1;
-    load_module_pairs(s, p.geo, first, start, num, hit_offset);
-    __syncthreads();
+    ModulePair md[3];
+    module_pairs(md, p.geo, first, start, num, hit_offset);
+    __syncthreads(); // bucket tables
 
-    seeding<LPH>(s, k, h, 8);
+    seeding<LPH>(s, cnt, k, h, md, 8);
 
     unsigned last_ttf = 0;
     --first;
     while (first > 1) {
-      load_module_pairs(s, p.geo, first, start, num, hit_offset);
+      module_pairs(md, p.geo, first, start, num, hit_offset);
       const unsigned prev_ttf = last_ttf;
-      last_ttf = s.ttf_counter;
+      last_ttf = cnt.ttf;
       const unsigned diff = last_ttf - prev_ttf;
-      if (threadIdx.x == 0) s.local_hits = 0;
-      __syncthreads();
-      forwarding(s, k, h, prev_ttf, diff, tracks, track_limit, three_hit, p.status);
+      cnt.local_hits = 0;
+      __syncthreads(); // ring entries of the last seeding
+      forwarding(s, cnt, k, h, md[2], prev_ttf, diff, tracks, track_limit, three_hit, p.status);
       // The ring holds 2048 entries; beyond that the reference overwrites entries it has
       // not read yet, an order-dependent outcome this kernel does not reproduce.
-      if (threadIdx.x == 0 && s.ttf_counter - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
-      seeding<LPH>(s, k, h, 4);
-      if (threadIdx.x == 0 && s.ttf_counter - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
+      if (threadIdx.x == 0 && cnt.ttf - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
+      __syncthreads(); // hit_used flags written by forwarding
+      seeding<LPH>(s, cnt, k, h, md, 4);
+      if (threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       --first;
     }
+    __syncthreads(); // ring entries of the last seeding
 
     // Tail: seeds still in flight become three-hit tracks (SearchByTriplet.cu:247-264)
     {
       const unsigned prev_ttf = last_ttf;
-      last_ttf = s.ttf_counter;
+      last_ttf = cnt.ttf;
       const unsigned diff = last_ttf - prev_ttf;
       for (unsigned c0 = 0; c0 < diff; c0 += blockDim.x) {
         const unsigned kk = c0 + threadIdx.x;
@@ -545,9 +567,9 @@ namespace velo {
           seed = (entry & seed_flag) != 0;
         }
         unsigned total;
-        const unsigned excl = block_exclusive_scan(seed ? 1u : 0u, s.warp_sums, &total);
+        const unsigned excl = scan1(s, cnt, seed ? 1u : 0u, total);
         if (seed) {
-          const unsigned slot = s.n_three + excl;
+          const unsigned slot = cnt.n_three + excl;
           if (slot < track_limit) {
             three_hit[slot] = TrackletHits {{static_cast<uint16_t>(entry & 0xFFFFu),
                                              static_cast<uint16_t>((entry >> 16) & 0xFFFFu),
@@ -557,19 +579,17 @@ namespace velo {
             set_error(p.status, err_track_capacity);
           }
         }
-        __syncthreads();
-        if (threadIdx.x == 0) s.n_three += total;
-        __syncthreads();
+        cnt.n_three += total;
       }
     }
 
     if (threadIdx.x == 0) {
       unsigned* atomics = p.atomics_velo + 3 * e;
-      atomics[0] = s.n_three;
-      atomics[1] = s.ttf_counter;
-      atomics[2] = s.local_hits;
-      p.number_of_velo_tracks[e] = s.n_tracks;
-      if (s.n_tracks > to_next - to) set_error(p.status, err_track_capacity);
+      atomics[0] = cnt.n_three;
+      atomics[1] = cnt.ttf;
+      atomics[2] = cnt.local_hits;
+      p.number_of_velo_tracks[e] = cnt.n_tracks;
+      if (cnt.n_tracks > to_next - to) set_error(p.status, err_track_capacity);
     }
     {
       uint8_t* g_used = reinterpret_cast<uint8_t*>(p.hit_used) + hit_offset;
@@ -579,8 +599,9 @@ namespace velo {
     __syncthreads();
 
     // Three-hit filter (ThreeHitTracksFilter.cu:109-130), input order preserved
-    const unsigned n_in = min(s.n_three, track_limit);
+    const unsigned n_in = min(cnt.n_three, track_limit);
     TrackletHits* out = p.three_hit_tracks_output + to;
+    unsigned filter_count = 0;
     for (unsigned c0 = 0; c0 < n_in; c0 += blockDim.x) {
       const unsigned i = c0 + threadIdx.x;
       bool keep = false;
@@ -593,15 +614,13 @@ namespace velo {
         keep = !any_used && chi2 < k.max_chi2;
       }
       unsigned total;
-      const unsigned excl = block_exclusive_scan(keep ? 1u : 0u, s.warp_sums, &total);
-      if (keep) out[s.filter_count + excl] = t;
-      __syncthreads();
-      if (threadIdx.x == 0) s.filter_count += total;
-      __syncthreads();
+      const unsigned excl = scan1(s, cnt, keep ? 1u : 0u, total);
+      if (keep) out[filter_count + excl] = t;
+      filter_count += total;
     }
     if (threadIdx.x == 0) {
-      p.number_of_three_hit_tracks_output[e] = s.filter_count;
-      p.event_track_hits[e] = s.track_hits + 3 * s.filter_count;
+      p.number_of_three_hit_tracks_output[e] = filter_count;
+      p.event_track_hits[e] = s.track_hits + 3 * filter_count;
     }
   }
 
