@@ -44,6 +44,19 @@ def load_generator():
     return _load(GEN_LIB, build.build_generator)
 
 
+TUNED_CONFIG = os.path.join(PKG, "data", "launch_config.json")
+
+
+def tuned_launch_config() -> dict | None:
+    """The launch configuration picked by allen_b200.autotune, if one was saved."""
+    import json
+    try:
+        with open(TUNED_CONFIG) as f:
+            return json.load(f).get("config")
+    except (OSError, ValueError):
+        return None
+
+
 def default_geometry() -> bytes:
     with open(GEOMETRY, "rb") as f:
         return f.read()

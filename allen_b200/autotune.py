@@ -1,0 +1,112 @@
+"""Autotuner of the chain's launch configuration.
+
+Sweeps, on a generated workload of the target occupancy, the search kernel's block size and
+lanes per seed candidate (the compiled pairs) and the shared-memory staging capacities of
+the search and clustering kernels, by coordinate descent: each parameter in turn takes the
+value with the highest events/s (CUDA-event timed graph replays) while the others stay at
+the current best.  The winner is written to allen_b200/data/launch_config.json, which
+VeloChain loads by default.
+
+    python -m allen_b200.autotune [--events 16000] [--pileup-min 1 --pileup-max 15]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+SEARCH_VARIANTS = [(128, 1), (128, 2), (256, 1), (256, 2), (256, 4), (512, 2), (512, 4), (128, 0), (256, 0), (512, 0)]
+SEARCH_CAPACITIES = [2048, 2560, 3072, 3584, 4096, 5120]
+CLUSTER_CAPACITIES = [2048, 2560, 3072, 4096]
+CLUSTER_BLOBS = [12 * 1024, 16 * 1024, 24 * 1024]
+
+
+def measure(chain, dev_slices, repeats=3) -> float:
+    """events/s over `repeats` passes of all slices, graphs captured beforehand."""
+    import torch
+    for d in dev_slices:
+        chain.run(d, use_graph=True)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(repeats):
+        for d in dev_slices:
+            chain.run(d, use_graph=True)
+    end.record()
+    torch.cuda.synchronize()
+    events = repeats * sum(d.n_events for d in dev_slices)
+    return events / (start.elapsed_time(end) / 1e3)
+
+
+def tune(chain, dev_slices, log=print) -> tuple[dict, float, list]:
+    trials = []
+    best = chain.get_config()
+
+    def try_config(**upd):
+        cfg = dict(best)
+        cfg.update(upd)
+        try:
+            chain.configure(**cfg)
+        except Exception as exc:  # configuration the device cannot hold
+            log(f"skip {upd}: {exc}")
+            return None
+        rate = measure(chain, dev_slices)
+        trials.append({"config": cfg, "events_per_s": rate})
+        log(f"{upd} -> {rate:,.0f} events/s")
+        return rate
+
+    best_rate = try_config()
+    for name, values in (
+        ("search", SEARCH_VARIANTS),
+        ("search_hit_capacity", SEARCH_CAPACITIES),
+        ("cluster_stage_capacity", CLUSTER_CAPACITIES),
+        ("cluster_blob_bytes", CLUSTER_BLOBS),
+    ):
+        for v in values:
+            upd = {"search_threads": v[0], "search_lanes_per_seed": v[1]} if name == "search" else {name: v}
+            rate = try_config(**upd)
+            if rate is not None and rate > best_rate:
+                best_rate = rate
+                best.update(upd)
+    chain.configure(**best)
+    return best, best_rate, trials
+
+
+def main():
+    import torch
+    from allen_b200 import _native, generator
+    from allen_b200.chain import VeloChain, upload
+    from allen_b200.rawbanks import super_pixels_per_event
+
+    p = argparse.ArgumentParser()
+    p.add_argument("--events", type=int, default=16000)
+    p.add_argument("--slice", type=int, default=16000)
+    p.add_argument("--pileup", type=float, default=7.6)
+    p.add_argument("--pileup-min", type=float, default=0.0)
+    p.add_argument("--pileup-max", type=float, default=0.0)
+    p.add_argument("--seed", type=int, default=99)
+    p.add_argument("--out", default=_native.TUNED_CONFIG)
+    args = p.parse_args()
+    torch.cuda.set_device(0)
+    slices = []
+    for first in range(0, args.events, args.slice):
+        slices.append(generator.generate(min(args.slice, args.events - first), seed=args.seed, first_event=first,
+                                         mean_pileup=args.pileup, pileup_min=args.pileup_min,
+                                         pileup_max=args.pileup_max).raw)
+    dev = [upload(s) for s in slices]
+    chain = VeloChain(use_tuned=False)
+    chain.reserve(max(s.n_events for s in slices), max(int(super_pixels_per_event(s).sum()) for s in slices) + 64)
+    t0 = time.time()
+    best, rate, trials = tune(chain, dev)
+    result = {"config": best, "events_per_s": rate, "workload": vars(args), "trials": trials,
+              "device": torch.cuda.get_device_name(0), "seconds": round(time.time() - t0, 1)}
+    os.makedirs(os.path.dirname(args.out), exist_ok=True)
+    with open(args.out, "w") as f:
+        json.dump(result, f, indent=1)
+    print(json.dumps({"best": best, "events_per_s": rate}))
+    chain.close()
+
+
+if __name__ == "__main__":
+    main()

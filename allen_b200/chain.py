@@ -71,6 +71,12 @@ class OutputsC(C.Structure):
     _fields_ = [(f, C.c_void_p) for f in OUTPUT_FIELDS]
 
 
+class LaunchConfigC(C.Structure):
+    _fields_ = [(f, C.c_uint) for f in (
+        "search_threads", "search_lanes_per_seed", "search_hit_capacity", "cluster_stage_capacity",
+        "cluster_blob_bytes", "estimate_blob_bytes")]
+
+
 class TotalsC(C.Structure):
     _fields_ = [(f, C.c_uint) for f in (
         "n_events", "host_total_number_of_velo_clusters", "host_number_of_cluster_candidates",
@@ -105,6 +111,10 @@ def _lib():
     lib.velo_copy_to_host.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.velo_copy_to_device.restype = C.c_int
     lib.velo_copy_to_device.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.velo_chain_configure.restype = C.c_int
+    lib.velo_chain_configure.argtypes = [C.c_void_p, C.POINTER(LaunchConfigC)]
+    lib.velo_chain_get_config.restype = C.c_int
+    lib.velo_chain_get_config.argtypes = [C.c_void_p, C.POINTER(LaunchConfigC)]
     lib.velo_chain_set_timing.restype = C.c_int
     lib.velo_chain_set_timing.argtypes = [C.c_void_p, C.c_int]
     lib.velo_chain_kernel_count.restype = C.c_uint
@@ -159,7 +169,7 @@ def upload(s: RawSlice, device="cuda") -> DeviceSlice:
 
 class VeloChain:
     def __init__(self, geometry: bytes | None = None, phi_tolerance=0.045, max_scatter=0.08,
-                 max_skipped_modules=1, max_chi2=20.0):
+                 max_skipped_modules=1, max_chi2=20.0, use_tuned: bool = True):
         self.lib = _lib()
         self.geometry = geometry if geometry is not None else _native.default_geometry()
         props = Properties(phi_tolerance, max_scatter, max_skipped_modules, max_chi2)
@@ -168,6 +178,10 @@ class VeloChain:
         self.handle = h
         self.max_events = 0
         self.max_super_pixels = 0
+        if use_tuned:
+            tuned = _native.tuned_launch_config()
+            if tuned:
+                self.configure(**tuned)
 
     def close(self):
         if getattr(self, "handle", None):
@@ -201,6 +215,19 @@ class VeloChain:
         if check:
             _check(self.lib, status, totals["device_flags"])
         return totals
+
+    def configure(self, **cfg):
+        """Sets launch parameters (search_threads, search_lanes_per_seed, search_hit_capacity,
+        cluster_stage_capacity, cluster_blob_bytes, estimate_blob_bytes); others keep their value."""
+        cur = self.get_config()
+        cur.update(cfg)
+        c = LaunchConfigC(*[cur[f] for f, _ in LaunchConfigC._fields_])
+        _check(self.lib, self.lib.velo_chain_configure(self.handle, C.byref(c)))
+
+    def get_config(self) -> dict:
+        c = LaunchConfigC()
+        _check(self.lib, self.lib.velo_chain_get_config(self.handle, C.byref(c)))
+        return {f: getattr(c, f) for f, _ in LaunchConfigC._fields_}
 
     def set_timing(self, enable: bool):
         _check(self.lib, self.lib.velo_chain_set_timing(self.handle, int(enable)))

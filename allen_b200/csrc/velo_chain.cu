@@ -170,6 +170,25 @@ namespace {
   }
 } // namespace
 
+// search_by_triplet_kernel instantiations (block size, lanes per seed candidate)
+using SearchKernel = void (*)(velo::SearchParams);
+struct SearchVariant {
+  unsigned threads, lanes;
+  SearchKernel fn;
+};
+static const SearchVariant search_variants[] = {
+#define VELO_SEARCH_VARIANT(T, L) {T, L, velo::search_by_triplet_kernel<T, L>},
+  VELO_SEARCH_CONFIGS(VELO_SEARCH_VARIANT)
+#undef VELO_SEARCH_VARIANT
+};
+
+static const SearchVariant* find_search_variant(unsigned threads, unsigned lanes)
+{
+  for (const auto& v : search_variants)
+    if (v.threads == threads && v.lanes == lanes) return &v;
+  return nullptr;
+}
+
 static constexpr unsigned n_timed_kernels = 7;
 static const char* const kernel_names[n_timed_kernels] = {
   "estimate_kernel", "exclusive_scan_kernel(candidates, estimates)", "cluster_sort_kernel",
@@ -187,11 +206,13 @@ struct VeloChain {
   size_t cap_tracks = 0;   // track container entries
   size_t cap_track_hits = 0;
 
-  // launch configuration (autotuned by the Python layer)
+  // launch configuration (autotuned by allen_b200/autotune.py)
   unsigned estimate_blob_bytes = 32 * 1024;
   unsigned cluster_blob_bytes = 16 * 1024;
   unsigned cluster_stage_capacity = 3072;
   unsigned search_hit_capacity = 3072;
+  unsigned search_threads = 256;
+  unsigned search_lanes = 2;
 
   // workspace
   DeviceBuffer<unsigned long long> bank_index_key;
@@ -317,8 +338,12 @@ namespace {
     sp.hit_scratch = c->hit_scratch.p;
     sp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
     const unsigned search_smem = c->search_hit_capacity * search_hit_bytes;
-    search_by_triplet_kernel<<<n, search_threads, search_smem, stream>>>(sp);
-    VELO_CUDA(cudaGetLastError());
+    {
+      const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes);
+      if (!v) return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for this launch configuration");
+      void* args[] = {&sp};
+      VELO_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(v->fn), dim3(n), dim3(v->threads), args, search_smem, stream));
+    }
     VELO_CUDA(mark());
 
     ScanParams sp2 {};
@@ -374,7 +399,8 @@ namespace {
     const int search_smem = int(c->search_hit_capacity * search_hit_bytes);
     VELO_CUDA(cudaFuncSetAttribute(estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c->estimate_blob_bytes)));
     VELO_CUDA(cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cluster_smem));
-    VELO_CUDA(cudaFuncSetAttribute(search_by_triplet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, search_smem));
+    for (const auto& v : search_variants)
+      VELO_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(v.fn), cudaFuncAttributeMaxDynamicSharedMemorySize, search_smem));
     return VELO_OK;
   }
 } // namespace
@@ -399,7 +425,7 @@ VeloStatus velo_device_check(void)
   if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return fail(VELO_ERR_NO_DEVICE, "cannot query the device");
   if (prop.major != 10) return fail(VELO_ERR_NO_DEVICE, std::string("sm_100 required, found ") + prop.name);
   cudaFuncAttributes attr {};
-  if (cudaFuncGetAttributes(&attr, velo::search_by_triplet_kernel) != cudaSuccess)
+  if (cudaFuncGetAttributes(&attr, reinterpret_cast<const void*>(search_variants[0].fn)) != cudaSuccess)
     return fail(VELO_ERR_NO_DEVICE, "kernels not loadable on this device");
   return VELO_OK;
 }
@@ -564,6 +590,43 @@ VeloStatus velo_chain_run(VeloChain* c, const VeloDeviceSlice* s, VeloStream str
   }
   VELO_CUDA(cudaGraphLaunch(entry->exec, stream));
   VELO_CUDA(cudaEventRecord(c->done, stream));
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
+{
+  if (!c || !cfg) return fail(VELO_ERR_ARGUMENT, "null argument");
+  if (!find_search_variant(cfg->search_threads, cfg->search_lanes_per_seed))
+    return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for (" + std::to_string(cfg->search_threads) + ", " +
+                                     std::to_string(cfg->search_lanes_per_seed) + ")");
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  const unsigned search_static = 32 * 1024; // upper bound of the kernel's static shared memory
+  const unsigned cluster_dyn = velo::cluster_sort_blob_offset(cfg->cluster_stage_capacity) + cfg->cluster_blob_bytes;
+  if (cfg->search_hit_capacity * velo::search_hit_bytes + search_static > unsigned(optin) ||
+      cluster_dyn + 16 * 1024 > unsigned(optin) || cfg->estimate_blob_bytes + 16 * 1024 > unsigned(optin) ||
+      cfg->search_hit_capacity > 65536 || cfg->cluster_stage_capacity > 65535 || (cfg->cluster_blob_bytes & 15) ||
+      (cfg->estimate_blob_bytes & 15))
+    return fail(VELO_ERR_ARGUMENT, "launch configuration exceeds the device's shared memory");
+  c->release_graph();
+  c->search_threads = cfg->search_threads;
+  c->search_lanes = cfg->search_lanes_per_seed;
+  c->search_hit_capacity = cfg->search_hit_capacity;
+  c->cluster_stage_capacity = cfg->cluster_stage_capacity;
+  c->cluster_blob_bytes = cfg->cluster_blob_bytes;
+  c->estimate_blob_bytes = cfg->estimate_blob_bytes;
+  return configure_kernels(c);
+}
+
+VeloStatus velo_chain_get_config(const VeloChain* c, VeloLaunchConfig* cfg)
+{
+  if (!c || !cfg) return fail(VELO_ERR_ARGUMENT, "null argument");
+  cfg->search_threads = c->search_threads;
+  cfg->search_lanes_per_seed = c->search_lanes;
+  cfg->search_hit_capacity = c->search_hit_capacity;
+  cfg->cluster_stage_capacity = c->cluster_stage_capacity;
+  cfg->cluster_blob_bytes = c->cluster_blob_bytes;
+  cfg->estimate_blob_bytes = c->estimate_blob_bytes;
   return VELO_OK;
 }
 

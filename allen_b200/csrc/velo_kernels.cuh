@@ -105,15 +105,17 @@ namespace velo {
 
   __global__ void estimate_kernel(EstimateParams p);
   __global__ void cluster_sort_kernel(ClusterSortParams p);
+  template<unsigned THREADS, unsigned LPH>
   __global__ void search_by_triplet_kernel(SearchParams p);
+  // (block size, lanes per seed candidate) pairs compiled for the autotuner
+// lanes 0 = flattened seeding (one thread per h1 candidate)
+#define VELO_SEARCH_CONFIGS(X) X(128, 1) X(128, 2) X(256, 1) X(256, 2) X(256, 4) X(512, 2) X(512, 4) X(128, 0) X(256, 0) X(512, 0)
   __global__ void consolidate_kernel(ConsolidateParams p);
   __global__ void exclusive_scan_kernel(ScanParams p);
 
   constexpr unsigned decode_threads = 256;
   constexpr unsigned scan_threads = 1024;
   constexpr unsigned consolidate_threads = 256;
-  constexpr unsigned search_threads = 256;
-  constexpr unsigned search_lanes_per_seed = 2;
   constexpr unsigned search_hit_bytes = 15; // x, y, z, phi, flags per staged hit
 
 } // namespace velo

@@ -25,6 +25,8 @@
 //    as they grow.
 //  * Leftmost binary searches over a module pair's phi go through a 128-bucket table
 //    per module pair, built once per event, plus a short scan: same index, fewer loads.
+#include <type_traits>
+
 #include "velo_kernels.cuh"
 
 namespace velo {
@@ -36,6 +38,7 @@ namespace velo {
   constexpr unsigned n_buckets = 128;
   constexpr uint8_t flag_used = 1;
   constexpr uint8_t flag_odd_module = 2;
+  constexpr unsigned flat_slots = 1024; // (h1, h0 candidate) slots per chunk of the flat seeding
 
   struct ModulePair {
     unsigned hit_start;
@@ -51,6 +54,13 @@ namespace velo {
     uint32_t tail[max_tail_tracks]; // last two hits of a track (hit[n-2] | hit[n-1] << 16)
     uint8_t tail_n[max_tail_tracks];
     uint16_t bucket[n_module_pairs][n_buckets + 1];
+  };
+
+  // Shared state of the flat seeding variant: one slot per (h1, candidate order).
+  struct SearchSharedFlat : SearchShared {
+    uint16_t cand_h0[flat_slots];
+    uint16_t res_h2[flat_slots];
+    float res_fit[flat_slots];
   };
 
   struct HitsSoA {
@@ -169,8 +179,10 @@ namespace velo {
     const float tx = txn * td;
     const float ty = tyn * td;
     const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[0] - prev.z[0]);
-    for (unsigned j = 0; j < next.hit_num; ++j) {
-      const unsigned h2 = next.hit_start + (static_cast<unsigned>(f.start) + j) % next.hit_num;
+    // circular walk from the candidate: index (start + j) % n without a division per step
+    unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
+    for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
+      const unsigned h2 = next.hit_start + idx;
       if (phi_outside(h.phi[h2], f.phi, tol)) break;
       if (h.flags[h2] & flag_used) continue;
       const float dz = h.z[h2] - h0z;
@@ -190,7 +202,7 @@ namespace velo {
 
   // Seeding over the current module pair (SearchByTriplet.cu:298-446), LPH lanes per h1.
   template<unsigned LPH>
-  __device__ void seeding(
+  __device__ __forceinline__ void seeding(
     SearchShared& s, Counters& cnt, const Constants& k, const HitsSoA& h, const ModulePair* md, unsigned n_candidates)
   {
     const ModulePair prev = md[0], cur = md[1], next = md[2];
@@ -256,8 +268,108 @@ namespace velo {
     }
   }
 
+  // Seeding with the candidates flattened (SearchByTriplet.cu:298-446): phase A, one thread
+  // per h1, walks the pendulum and writes its first n_candidates unused h0 into its own slots;
+  // phase B, one thread per slot, extrapolates and scans the h2 window; phase C, one thread per
+  // h1, keeps the first strictly best candidate in candidate order (the reference's sequential
+  // choice) and queues the seed in h1 order.  Phase B runs the same instruction path on every
+  // lane, unlike a thread walking all of its h1's candidates.
+  __device__ __forceinline__ void seeding_flat(
+    SearchSharedFlat& s, Counters& cnt, const Constants& k, const HitsSoA& h, const ModulePair* md, unsigned n_candidates)
+  {
+    const ModulePair prev = md[0], cur = md[1], next = md[2];
+    const unsigned shift = n_candidates == 8 ? 3u : 2u; // 8 or 4 candidates per h1
+    const unsigned per_chunk = min(blockDim.x, flat_slots >> shift);
+    const int n_prev = static_cast<int>(prev.hit_num);
+    const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
+    for (unsigned c0 = 0; c0 < cur.hit_num; c0 += per_chunk) {
+      const unsigned n_h1 = min(per_chunk, cur.hit_num - c0);
+      // Phase A
+      const unsigned r = c0 + threadIdx.x;
+      const unsigned h1 = cur.hit_start + r;
+      const bool mine = threadIdx.x < n_h1;
+      const bool valid = mine && !(h.flags[h1] & flag_used);
+      if (mine) {
+        unsigned found = 0;
+        if (valid) {
+          const int p0 = leftmost(s.bucket[prev.mp], h.phi + prev.hit_start, prev.hit_num, h.phi[h1]);
+          int pos = p0;
+          for (unsigned i = 0; i < prev.hit_num && found < n_candidates; ++i) {
+            pos += (i & 1u) ? static_cast<int>(i) : -static_cast<int>(i);
+            const int in_bounds = pos < 0 ? pos + n_prev : (pos >= n_prev ? pos - n_prev : pos);
+            const unsigned h0 = prev.hit_start + static_cast<unsigned>(in_bounds);
+            if (!(h.flags[h0] & flag_used)) s.cand_h0[(threadIdx.x << shift) + found++] = static_cast<uint16_t>(h0);
+          }
+        }
+        for (unsigned c = found; c < n_candidates; ++c)
+          s.cand_h0[(threadIdx.x << shift) + c] = 0xFFFFu;
+      }
+      __syncthreads();
+      // Phase B
+      for (unsigned q = threadIdx.x; q < (n_h1 << shift); q += blockDim.x) {
+        const unsigned h0 = s.cand_h0[q];
+        float best_fit = k.max_scatter;
+        unsigned best_h2 = 0xFFFFu;
+        if (h0 != 0xFFFFu) {
+          const unsigned hh1 = cur.hit_start + c0 + (q >> shift);
+          const float h1x = h.x[hh1], h1y = h.y[hh1], h1z = h.z[hh1];
+          const float h0x = h.x[h0], h0y = h.y[h0], h0z = h.z[h0];
+          const float td = __fdiv_rn(1.0f, h1z - h0z);
+          const float txn = h1x - h0x;
+          const float tyn = h1y - h0y;
+          const float tx = txn * td;
+          const float ty = tyn * td;
+          const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[0] - prev.z[0]);
+          unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
+          for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
+            const unsigned h2 = next.hit_start + idx;
+            if (phi_outside(h.phi[h2], f.phi, tol)) break;
+            if (h.flags[h2] & flag_used) continue;
+            const float dz = h.z[h2] - h0z;
+            const float predx = h0x + tx * dz;
+            const float predy = h0y + ty * dz;
+            const float dx = predx - h.x[h2];
+            const float dy = predy - h.y[h2];
+            const float scatter = dx * dx + dy * dy;
+            if (scatter < best_fit) {
+              best_fit = scatter;
+              best_h2 = h2;
+            }
+          }
+        }
+        s.res_fit[q] = best_fit;
+        s.res_h2[q] = static_cast<uint16_t>(best_h2);
+      }
+      __syncthreads();
+      // Phase C
+      bool ok = false;
+      unsigned best_h0 = 0, best_h2 = 0;
+      if (valid) {
+        float best_fit = k.max_scatter;
+        for (unsigned c = 0; c < n_candidates; ++c) {
+          const unsigned q = (threadIdx.x << shift) + c;
+          if (s.res_fit[q] < best_fit) {
+            best_fit = s.res_fit[q];
+            best_h0 = s.cand_h0[q];
+            best_h2 = s.res_h2[q];
+          }
+        }
+        ok = best_fit < k.max_scatter;
+      }
+      unsigned total;
+      const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | ((valid ? 1u : 0u) << 16), total);
+      if (ok) {
+        const unsigned tn = (cnt.ttf + (excl & 0xFFFFu)) % max_tracks_to_follow;
+        s.ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
+                     (uint64_t(best_h2 & 0xFFFFu) << 32);
+      }
+      cnt.ttf += total & 0xFFFFu;
+      cnt.local_hits += total >> 16;
+    }
+  }
+
   // Forwarding of the tracks to follow (SearchByTriplet.cu:451-609), one thread per track.
-  __device__ void forwarding(
+  __device__ __forceinline__ void forwarding(
     SearchShared& s,
     Counters& cnt,
     const Constants& k,
@@ -313,8 +425,9 @@ namespace velo {
         const float ty = tyn * td;
         float best_fit = k.max_scatter;
         const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[odd] - h0z);
-        for (unsigned j = 0; j < next.hit_num; ++j) {
-          const unsigned h2 = next.hit_start + (static_cast<unsigned>(f.start) + j) % next.hit_num;
+        unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
+        for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
+          const unsigned h2 = next.hit_start + idx;
           if (phi_outside(h.phi[h2], f.phi, tol)) break;
           const float dz = h.z[h2] - h0z;
           const float predx = h0x + tx * dz;
@@ -458,8 +571,8 @@ namespace velo {
     }
   }
 
-  template<unsigned LPH>
-  __device__ void search_event(const SearchParams& p, SearchShared& s, unsigned char* dsmem)
+  template<unsigned LPH, bool SMEM, typename Shared>
+  __device__ __forceinline__ void search_event(const SearchParams& p, Shared& s, unsigned char* dsmem)
   {
     const unsigned e = blockIdx.x;
     const unsigned n = p.n_events;
@@ -487,11 +600,10 @@ namespace velo {
     TrackHits* tracks = p.tracks + to;
     TrackletHits* three_hit = p.three_hit_tracks + to;
 
-    // Stage the hits as SoA: shared memory when they fit, else the event's global slice
-    // (16 bytes per estimated hit, so every slice starts 16-byte aligned).
-    const bool in_smem = n_hits <= p.smem_hit_capacity;
-    unsigned char* base = in_smem ? dsmem : reinterpret_cast<unsigned char*>(p.hit_scratch) + size_t(16) * hit_offset;
-    const unsigned cap = in_smem ? p.smem_hit_capacity : n_hits;
+    // Stage the hits as SoA: shared memory when they fit (SMEM), else the event's global
+    // slice (16 bytes per estimated hit, so every slice starts 16-byte aligned).
+    unsigned char* base = SMEM ? dsmem : reinterpret_cast<unsigned char*>(p.hit_scratch) + size_t(16) * hit_offset;
+    const unsigned cap = SMEM ? p.smem_hit_capacity : n_hits;
     float* xs = reinterpret_cast<float*>(base);
     float* ys = xs + cap;
     float* zs = ys + cap;
@@ -531,7 +643,8 @@ namespace velo {
     module_pairs(md, p.geo, first, start, num, hit_offset);
     __syncthreads(); // bucket tables
 
-    seeding<LPH>(s, cnt, k, h, md, 8);
+    if constexpr (LPH == 0) seeding_flat(s, cnt, k, h, md, 8);
+    else seeding<LPH>(s, cnt, k, h, md, 8);
 
     unsigned last_ttf = 0;
     --first;
@@ -547,7 +660,8 @@ namespace velo {
       // not read yet, an order-dependent outcome this kernel does not reproduce.
       if (threadIdx.x == 0 && cnt.ttf - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       __syncthreads(); // hit_used flags written by forwarding
-      seeding<LPH>(s, cnt, k, h, md, 4);
+      if constexpr (LPH == 0) seeding_flat(s, cnt, k, h, md, 4);
+      else seeding<LPH>(s, cnt, k, h, md, 4);
       if (threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       --first;
     }
@@ -624,11 +738,23 @@ namespace velo {
     }
   }
 
-  __global__ void __launch_bounds__(search_threads) search_by_triplet_kernel(SearchParams p)
+  // One instantiation per (block size, lanes per seed); the chain launches the one its
+  // launch configuration names (autotuned).  Events whose hits fit the shared-memory
+  // capacity run the shared-memory body, the others the global-scratch body.
+  template<unsigned THREADS, unsigned LPH>
+  __global__ void __launch_bounds__(THREADS) search_by_triplet_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
-    __shared__ SearchShared s;
-    search_event<search_lanes_per_seed>(p, s, dsmem);
+    __shared__ std::conditional_t<LPH == 0, SearchSharedFlat, SearchShared> s;
+    const unsigned* start = p.offsets_estimated_input_size + blockIdx.x * n_module_pairs;
+    const unsigned n_hits = start[n_module_pairs] - start[0];
+    if (n_hits <= p.smem_hit_capacity) search_event<LPH, true>(p, s, dsmem);
+    else search_event<LPH, false>(p, s, dsmem);
   }
+
+#define VELO_SEARCH_CONFIG(T, L)                                                 \
+  template __global__ void search_by_triplet_kernel<T, L>(SearchParams p);
+  VELO_SEARCH_CONFIGS(VELO_SEARCH_CONFIG)
+#undef VELO_SEARCH_CONFIG
 
 } // namespace velo

@@ -321,11 +321,11 @@ def run_ours(args):
     peak = peaks.get("hbm_gbs", 6650.0)
     ach = per_kernel[dominant]["gbs"] if dominant else None
     traffic = None
-    try:
-        prof = json.load(open(os.path.join(REPO, "profiles", "dram_traffic.json")))
-        per_unit = prof.get(dominant, {}).get("dram_bytes_per_event")
-        if per_unit:
-            traffic = int(per_unit * events_step / len(counts))
+    try:  # ncu DRAM bytes per event of the dominant kernel, scaled to one launch
+        for line in open(os.path.join(REPO, "profiles", "dram_traffic.md")):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) >= 2 and cells[0] == dominant:
+                traffic = int(float(cells[1]) * events_step / len(counts))
     except Exception:
         pass
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": peak, "unit": "GB/s",

@@ -168,6 +168,22 @@ VeloStatus velo_chain_synchronize(VeloChain* chain, VeloChainTotals* totals);
 
 VeloStatus velo_chain_outputs(const VeloChain* chain, VeloChainOutputs* outputs);
 
+/* Launch configuration (no counterpart in the reference, whose block sizes are algorithm
+ * PROPERTYs, e.g. SearchByTriplet.cuh:132): block size and lanes per seed candidate of the
+ * search kernel (a compiled pair: (128,1) (128,2) (256,1) (256,2) (256,4) (512,2) (512,4), and
+ * lanes 0 = flattened seeding, one thread per h1 candidate: (128,0) (256,0) (512,0)),
+ * and the shared-memory staging capacities.  Chosen by allen_b200/autotune.py. */
+typedef struct {
+  unsigned search_threads;
+  unsigned search_lanes_per_seed;
+  unsigned search_hit_capacity;    /* hits of an event staged in shared memory (15 B each) */
+  unsigned cluster_stage_capacity; /* clusters of an event staged in shared memory (22 B each) */
+  unsigned cluster_blob_bytes;     /* raw event bytes staged by the clustering kernel */
+  unsigned estimate_blob_bytes;    /* raw event bytes staged by the estimate kernel */
+} VeloLaunchConfig;
+VeloStatus velo_chain_configure(VeloChain* chain, const VeloLaunchConfig* config);
+VeloStatus velo_chain_get_config(const VeloChain* chain, VeloLaunchConfig* config);
+
 /* Per-kernel CUDA-event timing (no counterpart in the reference; its CI profiles with ncu,
  * scripts/ci/jobs/run_throughput.sh:61-67).  When enabled, every run records an event
  * between consecutive kernels, inside the captured graphs too; velo_chain_kernel_times()
