@@ -196,6 +196,37 @@ VeloStatus velo_chain_kernel_times(VeloChain* chain, float* ms_sum, unsigned* n_
 
 void velo_chain_destroy(VeloChain* chain);
 
+/* Allocation-free decoding (no counterpart in the reference).  For callers that cannot
+ * call cudaMalloc: code running inside a pre-reserved device-memory arena, such as an
+ * Allen algorithm whose buffers all belong to the scheduler's per-stream arena.  Runs the
+ * decoding half of the chain (velo_calculate_number_of_candidates, velo_estimate_input_size,
+ * its prefix sum, velo_masked_clustering and velo_sort_by_phi) with the same kernels as
+ * velo_chain_run() and writes dev_offsets_estimated_input_size [26 N + 1],
+ * dev_module_cluster_num [26 N] and dev_sorted_velo_cluster_container (at least
+ * 18 x 2 x super_pixels bytes) into caller buffers.  Its scratch is a file-scope static
+ * device array of velo_noalloc_scratch_bytes() (8 MiB at most) that every GPU loading the
+ * library holds until exit; slices above velo_noalloc_max_events() events or
+ * 2 x super_pixels > velo_noalloc_max_clusters() are rejected with VELO_ERR_CAPACITY.
+ * The first call on a device makes synchronous set-up calls (scratch address, geometry
+ * upload, kernel attributes): make it before any stream capture.  All calls share the
+ * scratch, which keeps the last call's contents; calls that overlap on the GPU race.
+ * dev_status (optional, device u32) receives the kernels' error flags. */
+VeloStatus velo_decode_noalloc(
+  const void* geometry,
+  size_t geometry_size,
+  const VeloDeviceSlice* slice,
+  unsigned long long super_pixels,
+  VeloStream stream,
+  unsigned* dev_offsets_estimated_input_size,
+  unsigned* dev_module_cluster_num,
+  char* dev_sorted_velo_cluster_container,
+  unsigned long long container_bytes,
+  unsigned* dev_status);
+unsigned velo_noalloc_max_events(void);
+unsigned velo_noalloc_max_clusters(void);
+unsigned long long velo_noalloc_scratch_bytes(void);
+const char* velo_noalloc_last_error_string(void);
+
 /* Utilities (synchronous copies on the current device), for callers without a CUDA runtime binding. */
 VeloStatus velo_copy_to_host(void* host, const void* device, size_t bytes);
 VeloStatus velo_copy_to_device(void* device, const void* host, size_t bytes);
