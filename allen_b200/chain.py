@@ -109,6 +109,8 @@ def _lib():
     lib.velo_chain_destroy.argtypes = [C.c_void_p]
     lib.velo_copy_to_host.restype = C.c_int
     lib.velo_copy_to_host.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.velo_copy_to_host_async.restype = C.c_int
+    lib.velo_copy_to_host_async.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
     lib.velo_copy_to_device.restype = C.c_int
     lib.velo_copy_to_device.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.velo_chain_configure.restype = C.c_int
@@ -302,3 +304,102 @@ class VeloChain:
                "dev_offsets_velo_track_hit_number": off_hn[:reco + 1],
                "dev_velo_track_hits": hits[:ELEMENT_SIZE * TH]}
         return totals, out, up.value, down.value
+
+
+class HostPipeline:
+    """End-to-end processing of slices held in page-locked host memory, through the C ABI.
+
+    Two chains on two CUDA streams alternate: while one chain runs slice i, the other copies
+    slice i + 1 in and the consolidated tracks of slice i - 1 out, so the PCIe transfers
+    overlap the kernels.  Per slice the host receives dev_offsets_all_velo_tracks,
+    dev_offsets_velo_track_hit_number and the id + xyz columns of dev_velo_track_hits
+    (16 bytes per track hit; the phi column is never written by the reference).
+    """
+
+    def __init__(self, geometry: bytes | None = None, n_chains: int = 2, **props):
+        import torch
+        self.torch = torch
+        self.chains = [VeloChain(geometry, **props) for _ in range(n_chains)]
+        self.streams = [torch.cuda.Stream() for _ in range(n_chains)]
+        self.dev_in = [None] * n_chains
+        self.host_out = []
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
+
+    def reserve(self, max_events: int, max_super_pixels: int, max_raw_bytes: int, max_sizes_words: int,
+                max_types_words: int):
+        torch = self.torch
+        for i, c in enumerate(self.chains):
+            c.reserve(max_events, max_super_pixels)
+            self.dev_in[i] = (torch.empty(max_raw_bytes + 16, dtype=torch.uint8, device="cuda"),
+                              torch.empty(max_events + 1, dtype=torch.int32, device="cuda"),
+                              torch.empty(max_sizes_words, dtype=torch.int32, device="cuda"),
+                              torch.empty(max_types_words, dtype=torch.int32, device="cuda"))
+        self.max_super_pixels = max_super_pixels
+        self.max_events = max_events
+
+    def _out_buffers(self, k):
+        torch = self.torch
+        while len(self.host_out) <= k:
+            cap = 2 * self.max_super_pixels + 64
+            self.host_out.append((torch.empty(self.max_events + 1, dtype=torch.int32, pin_memory=True),
+                                  torch.empty(cap + 1, dtype=torch.int32, pin_memory=True),
+                                  torch.empty(16 * cap, dtype=torch.uint8, pin_memory=True)))
+        return self.host_out[k]
+
+    def run(self, host_slices, keep_outputs: int = 0):
+        """host_slices: RawSlice objects whose arrays are page-locked.  Returns the totals per
+        slice; the outputs of the first `keep_outputs` slices are returned as numpy arrays too."""
+        torch = self.torch
+        n_c = len(self.chains)
+        pending = [None] * n_c  # (slice index, out buffers) waiting for their results
+        totals_all, outputs = {}, {}
+
+        def drain(ci):
+            if pending[ci] is None:
+                return
+            k, bufs = pending[ci]
+            chain = self.chains[ci]
+            t = chain.synchronize()
+            p = chain.device_outputs()
+            n = t["n_events"]
+            tracks = t["host_number_of_reconstructed_velo_tracks"]
+            TH = t["host_accumulated_number_of_hits_in_velo_tracks"]
+            stream = C.c_void_p(self.streams[ci].cuda_stream)
+            sizes = ((bufs[0], p["dev_offsets_all_velo_tracks"], 4 * (n + 1)),
+                     (bufs[1], p["dev_offsets_velo_track_hit_number"], 4 * (tracks + 1)),
+                     (bufs[2], p["dev_velo_track_hits"], 16 * TH))
+            for host, dev, nbytes in sizes:
+                _check(chain.lib, chain.lib.velo_copy_to_host_async(host.data_ptr(), dev, nbytes, stream))
+                self.d2h_bytes += nbytes
+            totals_all[k] = t
+            if k < keep_outputs:
+                self.streams[ci].synchronize()
+                outputs[k] = ({"dev_offsets_all_velo_tracks": bufs[0][:n + 1].numpy().view(np.uint32).copy(),
+                                "dev_offsets_velo_track_hit_number":
+                                    bufs[1][:tracks + 1].numpy().view(np.uint32).copy(),
+                                "dev_velo_track_hits_id_xyz": bufs[2][:16 * TH].numpy().copy()})
+            pending[ci] = None
+
+        for k, s in enumerate(host_slices):
+            ci = k % n_c
+            drain(ci)  # the slot's previous slice: its results go out while the other chain runs
+            raw_t, off_t, siz_t, typ_t = self.dev_in[ci]
+            stream = self.streams[ci]
+            with torch.cuda.stream(stream):
+                for dst, src in ((raw_t, s.raw.view(np.uint8)), (off_t, s.offsets.view(np.int32)),
+                                 (siz_t, s.sizes.view(np.int32)), (typ_t, s.types.view(np.int32))):
+                    dst[:src.size].copy_(torch.from_numpy(src), non_blocking=True)
+                    self.h2d_bytes += src.nbytes
+            d = DeviceSlice(raw_t, off_t, siz_t, typ_t, s.n_events, s.bank_version)
+            self.chains[ci].run(d, stream=C.c_void_p(stream.cuda_stream), use_graph=True)
+            pending[ci] = (k, self._out_buffers(k % (2 * n_c)))
+        for ci in range(n_c):
+            drain(ci)
+        for st in self.streams:
+            st.synchronize()
+        return [totals_all[k] for k in sorted(totals_all)], [outputs[k] for k in sorted(outputs)]
+
+    def close(self):
+        for c in self.chains:
+            c.close()

@@ -770,6 +770,12 @@ VeloStatus velo_copy_to_host(void* host, const void* device, size_t bytes)
   return VELO_OK;
 }
 
+VeloStatus velo_copy_to_host_async(void* host, const void* device, size_t bytes, VeloStream stream)
+{
+  VELO_CUDA(cudaMemcpyAsync(host, device, bytes, cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+  return VELO_OK;
+}
+
 VeloStatus velo_copy_to_device(void* device, const void* host, size_t bytes)
 {
   VELO_CUDA(cudaMemcpy(device, host, bytes, cudaMemcpyHostToDevice));

@@ -230,6 +230,8 @@ const char* velo_noalloc_last_error_string(void);
 /* Utilities (synchronous copies on the current device), for callers without a CUDA runtime binding. */
 VeloStatus velo_copy_to_host(void* host, const void* device, size_t bytes);
 VeloStatus velo_copy_to_device(void* device, const void* host, size_t bytes);
+/* Asynchronous device-to-host copy on `stream` (page-locked host memory overlaps with compute). */
+VeloStatus velo_copy_to_host_async(void* host, const void* device, size_t bytes, VeloStream stream);
 
 #ifdef __cplusplus
 }

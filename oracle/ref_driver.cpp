@@ -388,7 +388,7 @@ void velo_ref_free(void* handle) { delete static_cast<Result*>(handle); }
  * CPU baseline timing: the chain over `n_slices` consecutive slices of
  * `slice_size` events starting at in->event_start, distributed round-robin over
  * `n_threads` host threads (one slice per thread at a time, as Allen's -t
- * streams do). Returns wall seconds for all slices.
+ * streams do), cycling over the events available. Returns wall seconds for all slices.
  */
 double velo_ref_time(const VeloCpuInput* in, unsigned slice_size, unsigned n_slices, unsigned n_threads)
 {
@@ -396,9 +396,11 @@ double velo_ref_time(const VeloCpuInput* in, unsigned slice_size, unsigned n_sli
   std::vector<std::thread> workers;
   for (unsigned t = 0; t < n_threads; ++t) {
     workers.emplace_back([=] {
+      // slices cycle over the events available, so a sample may be longer than the input
+      const unsigned available = in->n_events / slice_size ? in->n_events / slice_size : 1;
       for (unsigned s = t; s < n_slices; s += n_threads) {
         VeloCpuInput slice = *in;
-        slice.event_start = in->event_start + s * slice_size;
+        slice.event_start = in->event_start + (s % available) * slice_size;
         slice.n_events = slice_size;
         velo_ref_free(velo_ref_run(&slice));
       }

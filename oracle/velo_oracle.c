@@ -1216,9 +1216,11 @@ typedef struct {
 static void* time_worker(void* arg)
 {
   const TimeArgs* a = arg;
+  /* slices cycle over the events available, so a sample may be longer than the input */
+  const unsigned available = a->in->n_events / a->slice_size ? a->in->n_events / a->slice_size : 1;
   for (unsigned s = a->thread; s < a->n_slices; s += a->n_threads) {
     VeloCpuInput slice = *a->in;
-    slice.event_start = a->in->event_start + s * a->slice_size;
+    slice.event_start = a->in->event_start + (s % available) * a->slice_size;
     slice.n_events = a->slice_size;
     velo_oracle_free(velo_oracle_run(&slice));
   }

@@ -76,3 +76,40 @@ def test_event_slice_offset(chain, oracle, geometry):
     out = chain.outputs_to_host(totals)
     ref = oracle.run(g.raw, geometry, event_start=10, n_events=25)
     assert parity.compare(out, ref, 25) == []
+
+
+def test_host_pipeline_matches_oracle(oracle, geometry):
+    """End-to-end path (page-locked host slices, two overlapping chains) against the oracle."""
+    import torch
+    from allen_b200.chain import HostPipeline
+    from allen_b200.rawbanks import super_pixels_per_event
+    import bench
+    slices = [generator.generate(30, seed=40 + i).raw for i in range(3)]
+    pinned = [bench.pin(s) for s in slices]
+    pipe = HostPipeline()
+    pipe.reserve(30, max(int(super_pixels_per_event(s).sum()) for s in slices) + 64,
+                 max(s.raw.nbytes for s in slices), max(s.sizes.size for s in slices),
+                 max(s.types.size for s in slices))
+    totals, outs = pipe.run(pinned, keep_outputs=3)
+    pipe.close()
+    for s, out in zip(slices, outs):
+        ref = oracle.run(s, geometry)
+        assert np.array_equal(out["dev_offsets_all_velo_tracks"], ref["dev_offsets_all_velo_tracks"])
+        assert np.array_equal(out["dev_offsets_velo_track_hit_number"], ref["dev_offsets_velo_track_hit_number"])
+        TH = int(ref["dev_offsets_velo_track_hit_number"][-1])
+        assert np.array_equal(out["dev_velo_track_hits_id_xyz"], parity._u8(ref["dev_velo_track_hits"])[:16 * TH])
+
+
+@pytest.mark.parametrize("threads,lanes", [(128, 1), (256, 2), (256, 4), (512, 4), (128, 0), (256, 0), (512, 0)])
+def test_search_variants_identical(chain, oracle, geometry, threads, lanes):
+    """Every compiled search configuration gives the same bit-exact result."""
+    g = generator.generate(40, seed=77, pileup_min=1.0, pileup_max=15.0)
+    saved = chain.get_config()
+    try:
+        chain.configure(search_threads=threads, search_lanes_per_seed=lanes, search_hit_capacity=2048,
+                        cluster_stage_capacity=2048)
+        totals, out = run_chain(chain, g.raw)
+        assert totals["device_flags"] == 0
+        assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
+    finally:
+        chain.configure(**saved)
