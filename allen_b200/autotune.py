@@ -2,7 +2,7 @@
 
 Sweeps, on a generated workload of the target occupancy, the search kernel's block size and
 lanes per seed candidate (the compiled pairs) and the shared-memory staging capacities of
-the search and clustering kernels, by coordinate descent: each parameter in turn takes the
+the search, clustering and estimate kernels, by coordinate descent: each parameter in turn takes the
 value with the highest events/s (CUDA-event timed graph replays) while the others stay at
 the current best.  The winner is written to allen_b200/data/launch_config.json, which
 VeloChain loads by default.
@@ -19,7 +19,8 @@ import time
 SEARCH_VARIANTS = [(128, 1), (128, 2), (256, 1), (256, 2), (256, 4), (512, 2), (512, 4), (128, 0), (256, 0), (512, 0)]
 SEARCH_CAPACITIES = [2048, 2560, 3072, 3584, 4096, 5120]
 CLUSTER_CAPACITIES = [2048, 2560, 3072, 4096]
-CLUSTER_BLOBS = [12 * 1024, 16 * 1024, 24 * 1024]
+CLUSTER_BLOBS = [16 * 1024, 24 * 1024, 32 * 1024, 40 * 1024]
+ESTIMATE_BLOBS = [24 * 1024, 32 * 1024, 48 * 1024]
 
 
 def measure(chain, dev_slices, repeats=3) -> float:
@@ -62,6 +63,7 @@ def tune(chain, dev_slices, log=print) -> tuple[dict, float, list]:
         ("search_hit_capacity", SEARCH_CAPACITIES),
         ("cluster_stage_capacity", CLUSTER_CAPACITIES),
         ("cluster_blob_bytes", CLUSTER_BLOBS),
+        ("estimate_blob_bytes", ESTIMATE_BLOBS),
     ):
         for v in values:
             upd = {"search_threads": v[0], "search_lanes_per_seed": v[1]} if name == "search" else {name: v}

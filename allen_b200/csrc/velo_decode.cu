@@ -74,7 +74,8 @@ namespace velo {
     unsigned smem_blob_bytes,
     uint64_t* bar,
     unsigned* status,
-    unsigned& n_words)
+    unsigned& n_words,
+    unsigned& staged_bytes)
   {
     const unsigned begin = in.offsets[ev];
     const unsigned end = in.offsets[ev + 1];
@@ -86,6 +87,7 @@ namespace velo {
     const uintptr_t e_al = e & ~uintptr_t(15);
     const unsigned need = static_cast<unsigned>(((e + 15) & ~uintptr_t(15)) - s_al);
     const bool base_aligned = (reinterpret_cast<uintptr_t>(in.raw) & 15u) == 0;
+    staged_bytes = 0;
     if (!base_aligned || need > smem_blob_bytes) {
       __syncthreads();
       return reinterpret_cast<const uint32_t*>(src);
@@ -115,6 +117,7 @@ namespace velo {
       if (threadIdx.x == 0) set_error(status, err_bulk_copy_timeout);
       return reinterpret_cast<const uint32_t*>(src);
     }
+    staged_bytes = need;
     return reinterpret_cast<const uint32_t*>(smem_blob + (s - s_al));
   }
 
@@ -214,37 +217,109 @@ namespace velo {
   }
 
   // ------------------------------------------------------------------------------------
+  // Sorted bank copies.  The neighbour scans of the reference visit every SP of the bank
+  // for every SP (EstimateInputSize.cu:111-141) and every candidate
+  // (MaskedVeloClustering.cu:361-402).  Each match ORs pattern bits into an accumulator, so
+  // the result depends neither on which non-matching SPs are visited nor on how often a
+  // matching one is.  With a copy of the bank sorted by key (address bits 22:8, plus the
+  // sensor bit 23 for bank version 4), all SPs that can match lie in one key range, found
+  // by binary search.  The readout does not write SPs in column order, so the copy is made
+  // here, in shared memory behind the staged event; events that leave no room for it keep
+  // the full scans.
+  // ------------------------------------------------------------------------------------
+  __device__ __forceinline__ uint32_t sp_key_mask(int version) { return version > 3 ? 0xFFFFu : 0x7FFFu; }
+
+  // sorted[bt.flat[b] + r] = the SP word of VP/Velo bank b with rank r by (key, position).
+  // Banks hold fewer than 2^16 SPs (the event fits the staging buffer).  Ends with a
+  // __syncthreads().
+  __device__ void sort_bank_words(const BankTable& bt, const uint32_t* words, uint32_t* sorted, uint32_t key_mask)
+  {
+    for (unsigned f = threadIdx.x; f < bt.total_sp; f += blockDim.x) {
+      const unsigned b = bank_of(bt, f);
+      const unsigned i = f - bt.flat[b];
+      const uint32_t* w = words + bt.words_off[b];
+      const unsigned n = bt.flat[b + 1] - bt.flat[b];
+      const uint32_t mine = (((w[i] >> 8) & key_mask) << 16) | i;
+      unsigned rank = 0;
+      for (unsigned j = 0; j < n; ++j)
+        rank += ((((w[j] >> 8) & key_mask) << 16) | j) < mine;
+      sorted[bt.flat[b] + rank] = w[i];
+    }
+    __syncthreads();
+  }
+
+  // First index in [0, n) whose key is >= k (keys non-decreasing).
+  __device__ __forceinline__ unsigned first_key_at_least(const uint32_t* w, unsigned n, uint32_t k, uint32_t key_mask)
+  {
+    unsigned lo = 0, len = n;
+    while (len > 0) {
+      const unsigned half = len >> 1;
+      if (((w[lo + half] >> 8) & key_mask) < k) {
+        lo += half + 1;
+        len -= half + 1;
+      }
+      else {
+        len = half;
+      }
+    }
+    return lo;
+  }
+
+  // ------------------------------------------------------------------------------------
   // Candidate search of a non-isolated SP (EstimateInputSize.cu:72-204).  Every SP of
   // the bank is a potential neighbour: the reference reads the current SP's own
   // no-neighbour bit instead of the other's (line 113), which is always 0 here.
   // Returns up to two candidate pixel codes: bit 8 set = present, bits 0..2 = pixel.
   // ------------------------------------------------------------------------------------
-  __device__ __forceinline__ uint32_t sp_candidates(uint32_t sp_word, const uint32_t* bank_words, unsigned n_sp)
+  __device__ __forceinline__ void
+  add_neighbour_pixels(uint32_t& pixels, uint32_t ow, uint32_t sp_row, uint32_t sp_col)
+  {
+    const uint32_t oaddr = (ow & 0x007FFF00u) >> 8;
+    const uint32_t orow = oaddr & 0x3Fu;
+    const uint32_t ocol = oaddr >> 6;
+    const uint32_t osp = ow & 0xFFu;
+    const bool col_same = ocol == sp_col;
+    const bool col_right = ocol == sp_col + 1;
+    if (!(col_same || col_right)) return;
+    if (orow == sp_row + 1) {
+      if (col_same) pixels |= (((osp & 0x01u) | ((osp & 0x10u) << 2)) << 4);
+      else pixels |= ((osp & 0x01u) << 16);
+    }
+    else if (orow == sp_row) {
+      if (col_right) pixels |= ((osp & 0x0Fu) << 12);
+    }
+    else if (orow == sp_row - 1) {
+      if (col_right) pixels |= ((osp & 0x08u) << 8);
+      else pixels |= ((osp & 0x80u) >> 2);
+    }
+  }
+
+  // key_mask != 0: the bank is sorted by (w >> 8) & key_mask.  Neighbours of either
+  // sensor count (the reference compares bits 22:8 only), so version 4 banks, sorted by
+  // (sensor bit, address), are searched in two ranges.
+  __device__ __forceinline__ uint32_t
+  sp_candidates(uint32_t sp_word, const uint32_t* bank_words, unsigned n_sp, uint32_t key_mask = 0)
   {
     const uint32_t sp_addr = (sp_word & 0x007FFF00u) >> 8;
     const uint32_t sp = sp_word & 0xFFu;
     uint32_t pixels = (sp & 0x0Fu) | ((sp & 0xF0u) << 2);
     const uint32_t sp_row = sp_addr & 0x3Fu;
     const uint32_t sp_col = sp_addr >> 6;
-    for (unsigned k = 0; k < n_sp; ++k) {
-      const uint32_t ow = bank_words[k];
-      const uint32_t oaddr = (ow & 0x007FFF00u) >> 8;
-      const uint32_t orow = oaddr & 0x3Fu;
-      const uint32_t ocol = oaddr >> 6;
-      const uint32_t osp = ow & 0xFFu;
-      const bool col_same = ocol == sp_col;
-      const bool col_right = ocol == sp_col + 1;
-      if (!(col_same || col_right)) continue;
-      if (orow == sp_row + 1) {
-        if (col_same) pixels |= (((osp & 0x01u) | ((osp & 0x10u) << 2)) << 4);
-        else pixels |= ((osp & 0x01u) << 16);
-      }
-      else if (orow == sp_row) {
-        if (col_right) pixels |= ((osp & 0x0Fu) << 12);
-      }
-      else if (orow == sp_row - 1) {
-        if (col_right) pixels |= ((osp & 0x08u) << 8);
-        else pixels |= ((osp & 0x80u) >> 2);
+    if (key_mask == 0) {
+      for (unsigned k = 0; k < n_sp; ++k)
+        add_neighbour_pixels(pixels, bank_words[k], sp_row, sp_col);
+    }
+    else {
+      // matches have column sp_col or sp_col + 1 and row sp_row - 1 .. sp_row + 1
+      const uint32_t lo_off = (sp_col << 6) + (sp_row > 0 ? sp_row - 1 : 0u);
+      const uint32_t hi_off = ((sp_col + 1) << 6) + (sp_row < 63 ? sp_row + 1 : 63u);
+      for (uint32_t half = 0; half <= (key_mask >> 15); ++half) {
+        const uint32_t k_hi = (half << 15) + hi_off;
+        for (unsigned k = first_key_at_least(bank_words, n_sp, (half << 15) + lo_off, key_mask); k < n_sp; ++k) {
+          const uint32_t ow = bank_words[k];
+          if (((ow >> 8) & key_mask) > k_hi) break;
+          add_neighbour_pixels(pixels, ow, sp_row, sp_col);
+        }
       }
     }
     const uint32_t inside = pixels & 0x3CFu;
@@ -291,9 +366,11 @@ namespace velo {
     }
     __syncthreads();
 
-    unsigned n_words;
-    const uint32_t* words = stage_event(p.in, ev, dsmem, p.smem_blob_bytes, &bar, p.status, n_words);
+    unsigned n_words, staged;
+    const uint32_t* words = stage_event(p.in, ev, dsmem, p.smem_blob_bytes, &bar, p.status, n_words, staged);
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
+    (void) staged; // the candidate count runs the full scans: only non-isolated SPs (a third)
+                   // search, which costs less than sorting every bank
 
     // velo_calculate_number_of_candidates: block 0 of the reference's launch (grid of
     // ceil(N / 256) blocks, one thread per event) handles events 0, stride, 2 stride, ...
@@ -411,6 +488,7 @@ namespace velo {
     const Constants& k,
     uint32_t candidate,
     const uint32_t* bank_words,
+    const uint32_t* sorted_words,
     unsigned n_sp,
     int version,
     ClusterOut& o)
@@ -429,8 +507,20 @@ namespace velo {
     const int32_t c_lo = sp_col - 3, c_hi = sp_col + 1;
     const int32_t row_lower = r_lo * 4;
     const int32_t col_lower = c_lo * 2;
-    for (unsigned j = 0; j < n_sp; ++j) {
-      const uint32_t ow = bank_words[j];
+    // window SPs lie in one key range of a sorted bank (version 4: of this sensor)
+    const uint32_t key_mask = sp_key_mask(version);
+    const uint32_t* scan = sorted_words ? sorted_words : bank_words;
+    unsigned j = 0;
+    uint32_t k_hi = 0xFFFFFFFFu;
+    if (sorted_words) {
+      const uint32_t half = version > 3 ? (sensor_number & 0x1u) << 15 : 0u;
+      const uint32_t k_lo = half + (static_cast<uint32_t>(max(c_lo, 0)) << 6) + static_cast<uint32_t>(max(r_lo, 0));
+      k_hi = half + (static_cast<uint32_t>(c_hi) << 6) + static_cast<uint32_t>(min(r_hi, 63));
+      j = first_key_at_least(sorted_words, n_sp, k_lo, key_mask);
+    }
+    for (; j < n_sp; ++j) {
+      const uint32_t ow = scan[j];
+      if (((ow >> 8) & key_mask) > k_hi) break;
       if (version > 3) {
         const uint32_t other_bit = (ow & 0x800000u) ? 1u : 0u;
         if (other_bit != (sensor_number & 0x1u)) continue;
@@ -522,6 +612,9 @@ namespace velo {
   // ------------------------------------------------------------------------------------
   // cluster_sort_kernel
   // ------------------------------------------------------------------------------------
+  constexpr unsigned candidate_queue = 1024; // queued candidates per chunk of 512 SPs
+  static_assert((candidate_queue / 2) % decode_threads == 0, "every lane takes the same number of SPs per chunk");
+
   __device__ __forceinline__ unsigned sort_bucket(int16_t phi) { return static_cast<unsigned>(phi + 32768) >> 9; }
 
   // u16 counters packed two per 32-bit word; returns the previous count of counter b.
@@ -539,6 +632,8 @@ namespace velo {
     __shared__ unsigned mp_count[n_module_pairs];
     __shared__ unsigned warp_sums[33];
     __shared__ unsigned sorted_total;
+    __shared__ uint32_t queue[candidate_queue];
+    __shared__ unsigned queue_count[2];
     __shared__ __align__(8) uint64_t bar;
 
     const unsigned e = blockIdx.x;
@@ -563,6 +658,7 @@ namespace velo {
       region[n_module_pairs] = s;
     }
     if (threadIdx.x < n_module_pairs) mp_count[threadIdx.x] = 0;
+    if (threadIdx.x < 2) queue_count[threadIdx.x] = 0;
     __syncthreads();
     if (threadIdx.x < n_module_pairs) {
       p.offsets_estimated_input_size[e * n_module_pairs + threadIdx.x] = base + region[threadIdx.x];
@@ -584,78 +680,106 @@ namespace velo {
     for (unsigned i = threadIdx.x; i < sort_counters / 2; i += blockDim.x)
       reinterpret_cast<uint32_t*>(bucket_start)[i] = 0;
 
-    unsigned n_words;
-    const uint32_t* words = stage_event(p.in, ev, blob, p.smem_blob_bytes, &bar, p.status, n_words);
+    unsigned n_words, staged;
+    const uint32_t* words = stage_event(p.in, ev, blob, p.smem_blob_bytes, &bar, p.status, n_words, staged);
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
+    const uint32_t key_mask = sp_key_mask(version);
+    uint32_t* sorted = nullptr;
+    if (staged > 0 && staged + 4 * bt.total_sp <= p.smem_blob_bytes) {
+      sorted = reinterpret_cast<uint32_t*>(blob + staged);
+      sort_bank_words(bt, words, sorted, key_mask);
+    }
 
     const Geometry* g = p.geo;
-    for (unsigned f = threadIdx.x; f < bt.total_sp; f += blockDim.x) {
-      const unsigned b = bank_of(bt, f);
-      const unsigned mp = bank_module_pair(bt.source_id[b], version);
-      if (mp >= n_module_pairs) continue;
-      const uint32_t* bank_words = words + bt.words_off[b];
-      const unsigned sp_index = f - bt.flat[b];
-      const uint32_t word = bank_words[sp_index];
-      if (word & 0x80000000u) {
-        const unsigned n_clusters = (__ldg(g->sp_patterns + (word & 0xFFu)) & 8u) ? 2u : 1u;
-        for (unsigned which = 0; which < n_clusters; ++which) {
-          ClusterOut o;
-          isolated_cluster(g, p.k, word, bt.source_id[b], version, which, o);
-          const unsigned slot = atomicAdd(&mp_count[mp], 1u);
-          if (region[mp] + slot < region[mp + 1]) {
-            const unsigned i = region[mp] + slot;
-            st.id(i) = o.id;
-            st.x(i) = o.x;
-            st.y(i) = o.y;
-            st.z(i) = o.z;
-            st.phi(i) = o.phi;
-            slot_in_bucket[i] = count_in_bucket(bucket_start, mp * sort_buckets + sort_bucket(o.phi));
-          }
-          else {
-            set_error(p.status, err_cluster_capacity);
-          }
-        }
+    auto stage_cluster = [&](const ClusterOut& o, unsigned mp) {
+      const unsigned slot = atomicAdd(&mp_count[mp], 1u);
+      if (region[mp] + slot < region[mp + 1]) {
+        const unsigned i = region[mp] + slot;
+        st.id(i) = o.id;
+        st.x(i) = o.x;
+        st.y(i) = o.y;
+        st.z(i) = o.z;
+        st.phi(i) = o.phi;
+        slot_in_bucket[i] = count_in_bucket(bucket_start, mp * sort_buckets + sort_bucket(o.phi));
       }
       else {
-        const uint32_t c = sp_candidates(word, bank_words, bt.n_sp[b]);
-        const bool v23 = version == 2 || version == 3;
-        const uint32_t sensor_number =
-          v23 ? (bt.source_id[b] & 0x1FFu) : (((bt.source_id[b] & 0x1FFu) << 1) | ((word >> 23) & 0x1u));
-        for (unsigned which = 0; which < 2; ++which) {
-          const uint32_t code = which ? (c >> 16) : c;
-          if (!(code & 0x100u)) continue;
-          const uint32_t candidate = (sp_index << 11) | (sensor_number << 3) | (code & 0x7u);
-          // MaskedVeloClustering.cu:567-572: the candidate's bank is looked up by sensor
-          const uint32_t cand_sensor = (candidate >> 3) & 0xFFu;
-          if (cand_sensor >= n_sensors) {
-            set_error(p.status, err_bad_sensor);
-            continue;
+        set_error(p.status, err_cluster_capacity);
+      }
+    };
+
+    // Two passes per chunk of SPs, so that the warps do not diverge between the isolated
+    // SPs (about two thirds, one table lookup each) and the flood fills of candidates:
+    // pass 1 makes the clusters of isolated SPs and queues the candidates of the others
+    // (EstimateInputSize.cu:72-204 order of codes), pass 2 runs rest_of_clusters on the
+    // queue.  A chunk has candidate_queue / 2 SPs, so the queue cannot overflow.
+    const unsigned chunk = candidate_queue / 2;
+    for (unsigned chunk_base = 0, parity = 0; chunk_base < bt.total_sp; chunk_base += chunk, parity ^= 1u) {
+      for (unsigned f = chunk_base + threadIdx.x; f < chunk_base + chunk; f += blockDim.x) {
+        uint32_t cand[2] = {0, 0};
+        bool valid[2] = {false, false};
+        if (f < bt.total_sp) {
+          const unsigned b = bank_of(bt, f);
+          const unsigned mp = bank_module_pair(bt.source_id[b], version);
+          const uint32_t* bank_words = words + bt.words_off[b];
+          const unsigned sp_index = f - bt.flat[b];
+          const uint32_t word = bank_words[sp_index];
+          if (mp >= n_module_pairs) {
+            // a source id beyond the 26 module pairs: malformed input, flagged by estimate_kernel
           }
-          const unsigned b2 = static_cast<unsigned>(p.bank_index_key[cand_sensor] & 0xFFFFFFFFull);
-          if (b2 >= bt.n_banks || (candidate >> 11) >= bt.n_sp[b2]) {
-            set_error(p.status, err_input_capacity);
-            continue;
-          }
-          ClusterOut o;
-          if (!rest_of_clusters(g, p.k, candidate, words + bt.words_off[b2], bt.n_sp[b2], version, o)) continue;
-          const unsigned cmp = cand_sensor / 8;
-          const unsigned slot = atomicAdd(&mp_count[cmp], 1u);
-          if (region[cmp] + slot < region[cmp + 1]) {
-            const unsigned i = region[cmp] + slot;
-            st.id(i) = o.id;
-            st.x(i) = o.x;
-            st.y(i) = o.y;
-            st.z(i) = o.z;
-            st.phi(i) = o.phi;
-            slot_in_bucket[i] = count_in_bucket(bucket_start, cmp * sort_buckets + sort_bucket(o.phi));
+          else if (word & 0x80000000u) {
+            const unsigned n_clusters = (__ldg(g->sp_patterns + (word & 0xFFu)) & 8u) ? 2u : 1u;
+            for (unsigned which = 0; which < n_clusters; ++which) {
+              ClusterOut o;
+              isolated_cluster(g, p.k, word, bt.source_id[b], version, which, o);
+              stage_cluster(o, mp);
+            }
           }
           else {
-            set_error(p.status, err_cluster_capacity);
+            const uint32_t c = sorted ? sp_candidates(word, sorted + bt.flat[b], bt.n_sp[b], key_mask)
+                                      : sp_candidates(word, bank_words, bt.n_sp[b]);
+            const bool v23 = version == 2 || version == 3;
+            const uint32_t sensor_number =
+              v23 ? (bt.source_id[b] & 0x1FFu) : (((bt.source_id[b] & 0x1FFu) << 1) | ((word >> 23) & 0x1u));
+            for (unsigned which = 0; which < 2; ++which) {
+              const uint32_t code = which ? (c >> 16) : c;
+              if (!(code & 0x100u)) continue;
+              cand[which] = (sp_index << 11) | (sensor_number << 3) | (code & 0x7u);
+              // MaskedVeloClustering.cu:567-572: the candidate's bank is looked up by sensor
+              if (((cand[which] >> 3) & 0xFFu) >= n_sensors) set_error(p.status, err_bad_sensor);
+              else valid[which] = true;
+            }
           }
         }
+        // warp-aggregated append to the queue (every lane of the warp gets here)
+        const unsigned lane = threadIdx.x & 31u;
+        for (unsigned which = 0; which < 2; ++which) {
+          const unsigned mask = __ballot_sync(0xFFFFFFFFu, valid[which]);
+          if (mask == 0) continue;
+          const unsigned leader = __ffs(mask) - 1;
+          unsigned at = 0;
+          if (lane == leader) at = atomicAdd(&queue_count[parity], __popc(mask));
+          at = __shfl_sync(0xFFFFFFFFu, at, leader);
+          if (valid[which]) queue[at + __popc(mask & ((1u << lane) - 1u))] = cand[which];
+        }
       }
+      __syncthreads();
+      const unsigned queued = min(queue_count[parity], candidate_queue);
+      if (threadIdx.x == 0) queue_count[parity ^ 1u] = 0;
+      for (unsigned q = threadIdx.x; q < queued; q += blockDim.x) {
+        const uint32_t candidate = queue[q];
+        const uint32_t cand_sensor = (candidate >> 3) & 0xFFu;
+        const unsigned b2 = static_cast<unsigned>(p.bank_index_key[cand_sensor] & 0xFFFFFFFFull);
+        if (b2 >= bt.n_banks || (candidate >> 11) >= bt.n_sp[b2]) {
+          set_error(p.status, err_input_capacity);
+          continue;
+        }
+        ClusterOut o;
+        const uint32_t* sorted_b2 = sorted && bt.velo[b2] ? sorted + bt.flat[b2] : nullptr;
+        if (rest_of_clusters(g, p.k, candidate, words + bt.words_off[b2], sorted_b2, bt.n_sp[b2], version, o))
+          stage_cluster(o, cand_sensor / 8);
+      }
+      __syncthreads();
     }
-    __syncthreads();
 
     // Sort by (phi, id) inside each module pair (SortByPhi.cu:104-122).  The reference
     // ranks every pair of clusters; here clusters were counted into 128 phi buckets per

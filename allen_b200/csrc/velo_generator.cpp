@@ -317,6 +317,15 @@ namespace {
         d.push_back(uint32_t(sensor_words[b].size()));
         d.insert(d.end(), sensor_words[b].begin(), sensor_words[b].end());
       }
+      // Readout order: the detector does not write a bank's SPs in column order (the
+      // 2018 minbias sample has about one bank in nine sorted), so sp_order 1 shuffles them.
+      if (cfg.sp_order == 1) {
+        const size_t first = v4 ? 0 : 1;
+        for (size_t k = d.size(); k > first + 1; --k) {
+          const size_t j = first + size_t(rng.next() % (k - first));
+          std::swap(d[k - 1], d[j]);
+        }
+      }
     }
     out.words.clear();
     out.words.push_back(n_banks);
@@ -359,6 +368,7 @@ void velo_gen_default_config(VeloGenConfig* cfg)
   cfg->share_fraction = 0.15;
   cfg->drop_corner_fraction = 0.3;
   cfg->bank_version = 2;
+  cfg->sp_order = 1;
 }
 
 void* velo_gen_create(

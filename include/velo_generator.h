@@ -30,6 +30,7 @@ typedef struct {
   double share_fraction;       /* charge-sharing band at each pixel edge (0.15) */
   double drop_corner_fraction; /* 2x2 clusters that lose their far corner (0.3) */
   int bank_version;            /* 2 (one bank per sensor), 3, or 4 (one per sensor pair) */
+  int sp_order;                /* SP order inside a bank: 0 column order, 1 shuffled as read out (1) */
 } VeloGenConfig;
 
 typedef struct {

@@ -114,3 +114,18 @@ def tracks_as_id_lists(out: dict) -> list[list[tuple]]:
             evt.append(tuple(ids[off_hn[t]:off_hn[t + 1]].tolist()))
         events.append(evt)
     return events
+
+
+def same_clusters_and_tracks(a: dict, b: dict) -> bool:
+    """Two runs over the same events decoded to the same sorted clusters (occupied slots)
+    and the same consolidated tracks; buffers indexed by candidate are not compared."""
+    for k in ("dev_offsets_estimated_input_size", "dev_module_cluster_num", "dev_offsets_all_velo_tracks",
+              "dev_offsets_velo_track_hit_number", "dev_velo_track_hits"):
+        if not np.array_equal(_u8(a[k]), _u8(b[k])):
+            return False
+    off = a["dev_offsets_estimated_input_size"]
+    T = int(off[-1])
+    mask = sorted_container_mask(off, a["dev_module_cluster_num"], T)
+    return all(np.array_equal(_u8(x[mask]), _u8(y[mask]))
+               for x, y in zip(container_fields(a["dev_sorted_velo_cluster_container"], T),
+                               container_fields(b["dev_sorted_velo_cluster_container"], T)))

@@ -113,3 +113,34 @@ def test_search_variants_identical(chain, oracle, geometry, threads, lanes):
         assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
     finally:
         chain.configure(**saved)
+
+
+@pytest.mark.parametrize("blob", [65536, 16384, 4096])
+def test_decode_staging_paths(chain, oracle, geometry, blob):
+    """Raw-event staging sizes that select each decoding path: the event and its sorted
+    bank copies in shared memory (64 KiB), the event alone with the full neighbour scans
+    (16 KiB, events of about 13 KB), and the event read from global memory (4 KiB)."""
+    g = generator.generate(40, seed=31, pileup_min=1.0, pileup_max=15.0)
+    saved = chain.get_config()
+    try:
+        chain.configure(estimate_blob_bytes=blob, cluster_blob_bytes=min(blob, 32768),
+                        cluster_stage_capacity=1024 if blob < 65536 else 2560)
+        totals, out = run_chain(chain, g.raw)
+        assert totals["device_flags"] == 0
+        assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
+    finally:
+        chain.configure(**saved)
+
+
+@pytest.mark.parametrize("version", [2, 4])
+def test_sp_order_does_not_change_results(chain, oracle, geometry, version):
+    """Banks in column order and in shuffled readout order decode to the same sorted
+    clusters and tracks (candidate indices differ, so those buffers are not compared)."""
+    outs = []
+    for order in (0, 1):
+        g = generator.generate(30, seed=12, bank_version=version, sp_order=order)
+        totals, out = run_chain(chain, g.raw)
+        assert totals["device_flags"] == 0
+        assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
+        outs.append(out)
+    assert parity.same_clusters_and_tracks(outs[0], outs[1])

@@ -58,3 +58,12 @@ def test_empty_banks_and_single_event(oracle, geometry):
     out = oracle.run(s, geometry)
     assert out["dev_module_cluster_num"].sum() == 1
     assert out["dev_offsets_all_velo_tracks"][-1] == 0
+
+
+@pytest.mark.parametrize("version", [2, 4])
+def test_sp_order_invariance(oracle, geometry, version):
+    """The reference's decoding does not depend on the order of SPs inside a bank: the
+    generator's column order and its shuffled readout order give the same clusters and tracks."""
+    runs = [oracle.run(generator.generate(8, seed=12, bank_version=version, sp_order=o).raw, geometry)
+            for o in (0, 1)]
+    assert parity.same_clusters_and_tracks(runs[0], runs[1])
