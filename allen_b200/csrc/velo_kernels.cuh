@@ -2,6 +2,7 @@
 #pragma once
 
 #include "velo_common.cuh"
+#include "velo_mlp.cuh"
 
 namespace velo {
 
@@ -57,7 +58,19 @@ namespace velo {
     unsigned smem_hit_capacity;                   // hits staged in shared memory per event
     unsigned cluster_capacity;                    // allocated T of the containers
     char* hit_scratch;                            // [16 T] staging of events above the capacity
+    // learned seed pruning (search_by_triplet_learned_kernel): the network, or null for the
+    // plain search
+    const MlpModelDevice* seed_model;
+    unsigned* seed_stats;                         // [3 N] doublets found, doublets kept, mode
+    // recording of training doublets (search_by_triplet_learned_kernel): null = off
+    DoubletRecord* records;
+    unsigned* record_count;
+    unsigned record_capacity;
+    unsigned record_every;                        // record the doublets of one h1 in record_every
   };
+
+  // seed_stats mode: the search that produced the event's tracks
+  constexpr unsigned seed_mode_plain = 0, seed_mode_learned = 1, seed_mode_fallback = 2;
 
   // ---- copy_track_hit_number + consolidate_tracks, one event per CTA ----
   struct ConsolidateParams {
@@ -107,6 +120,9 @@ namespace velo {
   __global__ void cluster_sort_kernel(ClusterSortParams p);
   template<unsigned THREADS, unsigned LPH>
   __global__ void search_by_triplet_kernel(SearchParams p);
+  // flat seeding with the learned seed pruner and doublet recording, THREADS = 128, 256, 512
+  template<unsigned THREADS>
+  __global__ void search_by_triplet_learned_kernel(SearchParams p);
   // (block size, lanes per seed candidate) pairs compiled for the autotuner
 // lanes 0 = flattened seeding (one thread per h1 candidate)
 #define VELO_SEARCH_CONFIGS(X) X(128, 1) X(128, 2) X(256, 1) X(256, 2) X(256, 4) X(512, 2) X(512, 4) X(128, 0) X(256, 0) X(512, 0)

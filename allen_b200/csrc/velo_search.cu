@@ -58,10 +58,24 @@ namespace velo {
 
   // Shared state of the flat seeding variant: one slot per (h1, candidate order).
   struct SearchSharedFlat : SearchShared {
-    uint16_t cand_h0[flat_slots];
-    uint16_t res_h2[flat_slots];
-    float res_fit[flat_slots];
+    // (h0, h1) doublets of a chunk, packed by pack_doublet(), then overwritten in place
+    // with the best scatter found for the doublet
+    union {
+      uint32_t doublet;
+      float fit;
+    } slot[flat_slots];
+    union {
+      uint16_t res_h2[flat_slots];
+      uint32_t mlp_rows[8][16][8]; // per warp: 16 doublets x 16 bf16 inputs (learned mode)
+    };
   };
+
+  // Packed doublet: h0 | h1 index in the chunk << 16 | rank << 25 | (found - 1) << 28 | keep << 31
+  __device__ __forceinline__ uint32_t pack_doublet(unsigned h0, unsigned h1_local, unsigned rank, unsigned found)
+  {
+    return h0 | (h1_local << 16) | (rank << 25) | ((found - 1u) << 28);
+  }
+  constexpr uint32_t doublet_keep = 1u << 31;
 
   struct HitsSoA {
     const float* x;
@@ -79,6 +93,8 @@ namespace velo {
     unsigned local_hits; // atomics::local_number_of_hits
     unsigned n_tracks;   // dev_number_of_velo_tracks
     unsigned scan_parity;
+    unsigned doublets;   // (h0, h1) doublets formed by the flat seeding
+    unsigned kept;       // doublets whose h2 window was scanned
   };
 
   // Block-wide exclusive scan with a single barrier: warp totals go to one of two
@@ -268,93 +284,190 @@ namespace velo {
     }
   }
 
-  // Seeding with the candidates flattened (SearchByTriplet.cu:298-446): phase A, one thread
-  // per h1, walks the pendulum and writes its first n_candidates unused h0 into its own slots;
-  // phase B, one thread per slot, extrapolates and scans the h2 window; phase C, one thread per
-  // h1, keeps the first strictly best candidate in candidate order (the reference's sequential
-  // choice) and queues the seed in h1 order.  Phase B runs the same instruction path on every
-  // lane, unlike a thread walking all of its h1's candidates.
+  __device__ __forceinline__ unsigned candidate_h0(uint64_t lo, uint64_t hi, unsigned c)
+  {
+    return static_cast<unsigned>((c < 4 ? lo >> (16 * c) : hi >> (16 * (c - 4))) & 0xFFFFu);
+  }
+
+  // Learned mode: scores the n doublets of the list with the network and sets the keep bit
+  // of those above the threshold.  Warps 0..7 take 16-doublet tiles; lanes 0..15 compute one
+  // doublet's inputs each into the warp's staging rows, ldmatrix forms the A fragment.
+  __device__ __forceinline__ void score_doublets(
+    SearchSharedFlat& s, const MlpModelDevice* m, const HitsSoA& h, unsigned h1_base, unsigned n)
+  {
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const unsigned n_warps = min(blockDim.x >> 5, 8u);
+    if (warp >= n_warps) return;
+    uint32_t(*rows)[8] = s.mlp_rows[warp];
+    for (unsigned t = warp; 16 * t < n; t += n_warps) {
+      if (lane < 16) {
+        const unsigned q = 16 * t + lane;
+        uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (q < n) {
+          const uint32_t d = s.slot[q].doublet;
+          const unsigned h0 = d & 0xFFFFu, h1 = h1_base + ((d >> 16) & 0x1FFu);
+          float f[mlp_features];
+          doublet_features(h.x[h0], h.y[h0], h.z[h0], h.phi[h0], h.x[h1], h.y[h1], h.z[h1], h.phi[h1], (d >> 25) & 7u,
+                           ((d >> 28) & 7u) + 1u, f);
+          standardise_pairs(*m, f, w);
+        }
+#pragma unroll
+        for (unsigned i = 0; i < 8; ++i)
+          rows[lane][i] = w[i];
+      }
+      __syncwarp();
+      uint32_t a[4];
+      ldmatrix_x4(a, &rows[lane & 15u][(lane >> 4) * 4]);
+      float lg, lg8;
+      mlp_forward_tile(m, a, lg, lg8);
+      if ((lane & 3u) == 0) {
+        const float thr = __ldg(&m->threshold_logit);
+        const unsigned q0 = 16 * t + (lane >> 2), q1 = q0 + 8;
+        if (q0 < n && lg > thr) s.slot[q0].doublet |= doublet_keep;
+        if (q1 < n && lg8 > thr) s.slot[q1].doublet |= doublet_keep;
+      }
+      __syncwarp();
+    }
+  }
+
+  // Seeding with the candidates flattened (SearchByTriplet.cu:298-446).  Phase A, one
+  // thread per h1, walks the pendulum and keeps its first n_candidates unused h0 in
+  // registers; a block scan packs all (h0, h1) doublets of the chunk into one list.
+  // Phase B, one thread per doublet, extrapolates and scans the h2 window.  Phase C, one
+  // thread per h1, keeps the first strictly best of its doublets in candidate order (the
+  // reference's sequential choice) and queues the seed in h1 order.  Phase B runs the same
+  // path on every lane and has no idle slots for h1 with fewer than n_candidates doublets.
+  // LEARNED kernels can also score the doublets with the seed pruner (only kept doublets
+  // reach phase B) and record training doublets.
+  template<bool LEARNED>
   __device__ __forceinline__ void seeding_flat(
-    SearchSharedFlat& s, Counters& cnt, const Constants& k, const HitsSoA& h, const ModulePair* md, unsigned n_candidates)
+    SearchSharedFlat& s,
+    Counters& cnt,
+    const Constants& k,
+    const HitsSoA& h,
+    const ModulePair* md,
+    unsigned n_candidates,
+    const SearchParams& p,
+    bool learned,
+    unsigned event,
+    unsigned hit_offset)
   {
     const ModulePair prev = md[0], cur = md[1], next = md[2];
-    const unsigned shift = n_candidates == 8 ? 3u : 2u; // 8 or 4 candidates per h1
-    const unsigned per_chunk = min(blockDim.x, flat_slots >> shift);
+    const unsigned per_chunk = min(blockDim.x, flat_slots / n_candidates);
     const int n_prev = static_cast<int>(prev.hit_num);
     const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
     for (unsigned c0 = 0; c0 < cur.hit_num; c0 += per_chunk) {
       const unsigned n_h1 = min(per_chunk, cur.hit_num - c0);
-      // Phase A
-      const unsigned r = c0 + threadIdx.x;
-      const unsigned h1 = cur.hit_start + r;
-      const bool mine = threadIdx.x < n_h1;
-      const bool valid = mine && !(h.flags[h1] & flag_used);
-      if (mine) {
-        unsigned found = 0;
-        if (valid) {
-          const int p0 = leftmost(s.bucket[prev.mp], h.phi + prev.hit_start, prev.hit_num, h.phi[h1]);
-          int pos = p0;
-          for (unsigned i = 0; i < prev.hit_num && found < n_candidates; ++i) {
-            pos += (i & 1u) ? static_cast<int>(i) : -static_cast<int>(i);
-            const int in_bounds = pos < 0 ? pos + n_prev : (pos >= n_prev ? pos - n_prev : pos);
-            const unsigned h0 = prev.hit_start + static_cast<unsigned>(in_bounds);
-            if (!(h.flags[h0] & flag_used)) s.cand_h0[(threadIdx.x << shift) + found++] = static_cast<uint16_t>(h0);
+      // Phase A: candidates c < 4 in the 16-bit fields of cand_lo, 4..7 in cand_hi
+      const unsigned h1 = cur.hit_start + c0 + threadIdx.x;
+      const bool valid = threadIdx.x < n_h1 && !(h.flags[h1] & flag_used);
+      uint64_t cand_lo = 0, cand_hi = 0;
+      unsigned found = 0;
+      if (valid) {
+        const int p0 = leftmost(s.bucket[prev.mp], h.phi + prev.hit_start, prev.hit_num, h.phi[h1]);
+        int pos = p0;
+        for (unsigned i = 0; i < prev.hit_num && found < n_candidates; ++i) {
+          pos += (i & 1u) ? static_cast<int>(i) : -static_cast<int>(i);
+          const int in_bounds = pos < 0 ? pos + n_prev : (pos >= n_prev ? pos - n_prev : pos);
+          const unsigned h0 = prev.hit_start + static_cast<unsigned>(in_bounds);
+          if (!(h.flags[h0] & flag_used)) {
+            if (found < 4) cand_lo |= uint64_t(h0) << (16 * found);
+            else cand_hi |= uint64_t(h0) << (16 * (found - 4));
+            ++found;
           }
         }
-        for (unsigned c = found; c < n_candidates; ++c)
-          s.cand_h0[(threadIdx.x << shift) + c] = 0xFFFFu;
       }
+      unsigned n_doublets;
+      unsigned first = scan1(s, cnt, found, n_doublets);
+      for (unsigned c = 0; c < found; ++c)
+        s.slot[first + c].doublet = pack_doublet(candidate_h0(cand_lo, cand_hi, c), threadIdx.x, c, found);
       __syncthreads();
+      cnt.doublets += n_doublets;
+      // keep_mask bit c: the h2 window of doublet c is scanned (always, in the plain search)
+      unsigned keep_mask = (1u << found) - 1u;
+      if (LEARNED && learned) {
+        score_doublets(s, p.seed_model, h, cur.hit_start + c0, n_doublets);
+        __syncthreads();
+        keep_mask = 0;
+        for (unsigned c = 0; c < found; ++c)
+          keep_mask |= (s.slot[first + c].doublet >> 31) << c;
+        // pack the kept doublets (reads above, writes after the scan's barrier)
+        first = scan1(s, cnt, __popc(keep_mask), n_doublets);
+        unsigned at = first;
+        for (unsigned c = 0; c < found; ++c)
+          if (keep_mask & (1u << c))
+            s.slot[at++].doublet = pack_doublet(candidate_h0(cand_lo, cand_hi, c), threadIdx.x, c, found);
+        __syncthreads();
+      }
+      cnt.kept += n_doublets;
       // Phase B
-      for (unsigned q = threadIdx.x; q < (n_h1 << shift); q += blockDim.x) {
-        const unsigned h0 = s.cand_h0[q];
+      for (unsigned q = threadIdx.x; q < n_doublets; q += blockDim.x) {
+        const uint32_t d = s.slot[q].doublet;
+        const unsigned h0 = d & 0xFFFFu;
+        const unsigned hh1 = cur.hit_start + c0 + ((d >> 16) & 0x1FFu);
         float best_fit = k.max_scatter;
         unsigned best_h2 = 0xFFFFu;
-        if (h0 != 0xFFFFu) {
-          const unsigned hh1 = cur.hit_start + c0 + (q >> shift);
-          const float h1x = h.x[hh1], h1y = h.y[hh1], h1z = h.z[hh1];
-          const float h0x = h.x[h0], h0y = h.y[h0], h0z = h.z[h0];
-          const float td = __fdiv_rn(1.0f, h1z - h0z);
-          const float txn = h1x - h0x;
-          const float tyn = h1y - h0y;
-          const float tx = txn * td;
-          const float ty = tyn * td;
-          const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[0] - prev.z[0]);
-          unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
-          for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
-            const unsigned h2 = next.hit_start + idx;
-            if (phi_outside(h.phi[h2], f.phi, tol)) break;
-            if (h.flags[h2] & flag_used) continue;
-            const float dz = h.z[h2] - h0z;
-            const float predx = h0x + tx * dz;
-            const float predy = h0y + ty * dz;
-            const float dx = predx - h.x[h2];
-            const float dy = predy - h.y[h2];
-            const float scatter = dx * dx + dy * dy;
-            if (scatter < best_fit) {
-              best_fit = scatter;
-              best_h2 = h2;
-            }
+        const float h1x = h.x[hh1], h1y = h.y[hh1], h1z = h.z[hh1];
+        const float h0x = h.x[h0], h0y = h.y[h0], h0z = h.z[h0];
+        const float td = __fdiv_rn(1.0f, h1z - h0z);
+        const float txn = h1x - h0x;
+        const float tyn = h1y - h0y;
+        const float tx = txn * td;
+        const float ty = tyn * td;
+        const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[0] - prev.z[0]);
+        unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
+        for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
+          const unsigned h2 = next.hit_start + idx;
+          if (phi_outside(h.phi[h2], f.phi, tol)) break;
+          if (h.flags[h2] & flag_used) continue;
+          const float dz = h.z[h2] - h0z;
+          const float predx = h0x + tx * dz;
+          const float predy = h0y + ty * dz;
+          const float dx = predx - h.x[h2];
+          const float dy = predy - h.y[h2];
+          const float scatter = dx * dx + dy * dy;
+          if (scatter < best_fit) {
+            best_fit = scatter;
+            best_h2 = h2;
           }
         }
-        s.res_fit[q] = best_fit;
+        s.slot[q].fit = best_fit;
         s.res_h2[q] = static_cast<uint16_t>(best_h2);
       }
       __syncthreads();
       // Phase C
       bool ok = false;
-      unsigned best_h0 = 0, best_h2 = 0;
+      unsigned best_h0 = 0, best_h2 = 0, best_c = 0xFFFFFFFFu;
       if (valid) {
         float best_fit = k.max_scatter;
-        for (unsigned c = 0; c < n_candidates; ++c) {
-          const unsigned q = (threadIdx.x << shift) + c;
-          if (s.res_fit[q] < best_fit) {
-            best_fit = s.res_fit[q];
-            best_h0 = s.cand_h0[q];
-            best_h2 = s.res_h2[q];
+        unsigned at = first;
+        for (unsigned c = 0; c < found; ++c) {
+          if (!(keep_mask & (1u << c))) continue;
+          const float fit = s.slot[at].fit;
+          if (fit < best_fit) {
+            best_fit = fit;
+            best_c = c;
+            best_h0 = candidate_h0(cand_lo, cand_hi, c);
+            best_h2 = s.res_h2[at];
           }
+          ++at;
         }
         ok = best_fit < k.max_scatter;
+        // training doublets: every candidate of one h1 in record_every, labelled by the choice
+        if (LEARNED && p.records != nullptr && found > 0 &&
+            ((event * 0x9E3779B1u) ^ ((hit_offset + h1) * 0x85EBCA77u)) % p.record_every == 0) {
+          const unsigned slot0 = atomicAdd(p.record_count, found);
+          for (unsigned c = 0; c < found && slot0 + found <= p.record_capacity; ++c) {
+            const unsigned h0 = candidate_h0(cand_lo, cand_hi, c);
+            DoubletRecord r;
+            doublet_features(h.x[h0], h.y[h0], h.z[h0], h.phi[h0], h.x[h1], h.y[h1], h.z[h1], h.phi[h1], c, found, r.f);
+            r.label = (ok && c == best_c) ? 1.0f : 0.0f;
+            r.event = event;
+            r.h0 = hit_offset + h0;
+            r.h1 = hit_offset + h1;
+            p.records[slot0 + c] = r;
+          }
+        }
       }
       unsigned total;
       const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | ((valid ? 1u : 0u) << 16), total);
@@ -571,7 +684,90 @@ namespace velo {
     }
   }
 
-  template<unsigned LPH, bool SMEM, typename Shared>
+  // Seeding, forwarding and the tail of one event over staged hits (hit_used clear):
+  // SearchByTriplet.cu:165-264.  Returns the event's counters; the track containers hold
+  // its tracks and three-hit tracks.
+  template<unsigned LPH, bool LEARNED, typename Shared>
+  __device__ __forceinline__ Counters search_pass(
+    const SearchParams& p,
+    Shared& s,
+    const Constants& k,
+    const HitsSoA& h,
+    const unsigned* start,
+    const unsigned* num,
+    unsigned hit_offset,
+    unsigned e,
+    TrackHits* tracks,
+    unsigned track_limit,
+    TrackletHits* three_hit,
+    bool learned)
+  {
+    if (threadIdx.x == 0) s.track_hits = 0;
+    Counters cnt {0, 0, 0, 0, 0, 0, 0};
+    __syncthreads();
+    unsigned first = n_module_pairs - 1;
+    ModulePair md[3];
+    module_pairs(md, p.geo, first, start, num, hit_offset);
+    __syncthreads(); // bucket tables
+
+    if constexpr (LPH == 0) seeding_flat<LEARNED>(s, cnt, k, h, md, 8, p, learned, e, hit_offset);
+    else seeding<LPH>(s, cnt, k, h, md, 8);
+
+    unsigned last_ttf = 0;
+    --first;
+    while (first > 1) {
+      module_pairs(md, p.geo, first, start, num, hit_offset);
+      const unsigned prev_ttf = last_ttf;
+      last_ttf = cnt.ttf;
+      const unsigned diff = last_ttf - prev_ttf;
+      cnt.local_hits = 0;
+      __syncthreads(); // ring entries of the last seeding
+      forwarding(s, cnt, k, h, md[2], prev_ttf, diff, tracks, track_limit, three_hit, p.status);
+      // The ring holds 2048 entries; beyond that the reference overwrites entries it has
+      // not read yet, an order-dependent outcome this kernel does not reproduce.
+      if (threadIdx.x == 0 && cnt.ttf - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
+      __syncthreads(); // hit_used flags written by forwarding
+      if constexpr (LPH == 0) seeding_flat<LEARNED>(s, cnt, k, h, md, 4, p, learned, e, hit_offset);
+      else seeding<LPH>(s, cnt, k, h, md, 4);
+      if (threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
+      --first;
+    }
+    __syncthreads(); // ring entries of the last seeding
+
+    // Tail: seeds still in flight become three-hit tracks (SearchByTriplet.cu:247-264)
+    {
+      const unsigned prev_ttf = last_ttf;
+      last_ttf = cnt.ttf;
+      const unsigned diff = last_ttf - prev_ttf;
+      for (unsigned c0 = 0; c0 < diff; c0 += blockDim.x) {
+        const unsigned kk = c0 + threadIdx.x;
+        uint64_t entry = 0;
+        bool seed = false;
+        if (kk < diff) {
+          entry = s.ring[(prev_ttf + kk) % max_tracks_to_follow];
+          seed = (entry & seed_flag) != 0;
+        }
+        unsigned total;
+        const unsigned excl = scan1(s, cnt, seed ? 1u : 0u, total);
+        if (seed) {
+          const unsigned slot = cnt.n_three + excl;
+          if (slot < track_limit) {
+            three_hit[slot] = TrackletHits {{static_cast<uint16_t>(entry & 0xFFFFu),
+                                             static_cast<uint16_t>((entry >> 16) & 0xFFFFu),
+                                             static_cast<uint16_t>((entry >> 32) & 0xFFFFu)}};
+          }
+          else {
+            set_error(p.status, err_track_capacity);
+          }
+        }
+        cnt.n_three += total;
+      }
+    }
+
+    return cnt;
+  }
+
+  template<unsigned LPH, bool SMEM, bool LEARNED, typename Shared>
   __device__ __forceinline__ void search_event(const SearchParams& p, Shared& s, unsigned char* dsmem)
   {
     const unsigned e = blockIdx.x;
@@ -622,9 +818,6 @@ namespace velo {
       }
     }
     const HitsSoA h {xs, ys, zs, phis, flags};
-    if (threadIdx.x == 0) s.track_hits = 0;
-    Counters cnt {0, 0, 0, 0, 0};
-    __syncthreads();
     // bucket tables: bucket[mp][b] = first index of the module pair with phi >= b * 512 - 32768
     for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
       const unsigned s0 = start[mp] - hit_offset;
@@ -638,63 +831,27 @@ namespace velo {
       }
     }
 
-    unsigned first = n_module_pairs - 1;
-    ModulePair md[3];
-    module_pairs(md, p.geo, first, start, num, hit_offset);
-    __syncthreads(); // bucket tables
-
-    if constexpr (LPH == 0) seeding_flat(s, cnt, k, h, md, 8);
-    else seeding<LPH>(s, cnt, k, h, md, 8);
-
-    unsigned last_ttf = 0;
-    --first;
-    while (first > 1) {
-      module_pairs(md, p.geo, first, start, num, hit_offset);
-      const unsigned prev_ttf = last_ttf;
-      last_ttf = cnt.ttf;
-      const unsigned diff = last_ttf - prev_ttf;
-      cnt.local_hits = 0;
-      __syncthreads(); // ring entries of the last seeding
-      forwarding(s, cnt, k, h, md[2], prev_ttf, diff, tracks, track_limit, three_hit, p.status);
-      // The ring holds 2048 entries; beyond that the reference overwrites entries it has
-      // not read yet, an order-dependent outcome this kernel does not reproduce.
-      if (threadIdx.x == 0 && cnt.ttf - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
-      __syncthreads(); // hit_used flags written by forwarding
-      if constexpr (LPH == 0) seeding_flat(s, cnt, k, h, md, 4);
-      else seeding<LPH>(s, cnt, k, h, md, 4);
-      if (threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
-      --first;
-    }
-    __syncthreads(); // ring entries of the last seeding
-
-    // Tail: seeds still in flight become three-hit tracks (SearchByTriplet.cu:247-264)
-    {
-      const unsigned prev_ttf = last_ttf;
-      last_ttf = cnt.ttf;
-      const unsigned diff = last_ttf - prev_ttf;
-      for (unsigned c0 = 0; c0 < diff; c0 += blockDim.x) {
-        const unsigned kk = c0 + threadIdx.x;
-        uint64_t entry = 0;
-        bool seed = false;
-        if (kk < diff) {
-          entry = s.ring[(prev_ttf + kk) % max_tracks_to_follow];
-          seed = (entry & seed_flag) != 0;
-        }
-        unsigned total;
-        const unsigned excl = scan1(s, cnt, seed ? 1u : 0u, total);
-        if (seed) {
-          const unsigned slot = cnt.n_three + excl;
-          if (slot < track_limit) {
-            three_hit[slot] = TrackletHits {{static_cast<uint16_t>(entry & 0xFFFFu),
-                                             static_cast<uint16_t>((entry >> 16) & 0xFFFFu),
-                                             static_cast<uint16_t>((entry >> 32) & 0xFFFFu)}};
-          }
-          else {
-            set_error(p.status, err_track_capacity);
-          }
-        }
-        cnt.n_three += total;
+    // Learned mode: the pruned search first; an event whose fraction of kept doublets falls
+    // outside the model's bounds is searched again by the plain search, from scratch.
+    const bool learned = LEARNED && p.seed_model != nullptr;
+    Counters cnt =
+      search_pass<LPH, LEARNED>(p, s, k, h, start, num, hit_offset, e, tracks, track_limit, three_hit, learned);
+    unsigned mode = learned ? seed_mode_learned : seed_mode_plain;
+    const unsigned doublets = cnt.doublets, kept = cnt.kept;
+    if (learned && doublets > 0) {
+      const float frac = __fdiv_rn(__uint2float_rn(kept), __uint2float_rn(doublets));
+      if (frac < __ldg(&p.seed_model->kept_lo) || frac > __ldg(&p.seed_model->kept_hi)) {
+        mode = seed_mode_fallback;
+        __syncthreads();
+        for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x)
+          flags[i] &= static_cast<uint8_t>(~flag_used);
+        cnt = search_pass<LPH, LEARNED>(p, s, k, h, start, num, hit_offset, e, tracks, track_limit, three_hit, false);
       }
+    }
+    if (p.seed_stats != nullptr && threadIdx.x == 0) {
+      p.seed_stats[3 * e] = doublets;
+      p.seed_stats[3 * e + 1] = kept;
+      p.seed_stats[3 * e + 2] = mode;
     }
 
     if (threadIdx.x == 0) {
@@ -748,13 +905,30 @@ namespace velo {
     __shared__ std::conditional_t<LPH == 0, SearchSharedFlat, SearchShared> s;
     const unsigned* start = p.offsets_estimated_input_size + blockIdx.x * n_module_pairs;
     const unsigned n_hits = start[n_module_pairs] - start[0];
-    if (n_hits <= p.smem_hit_capacity) search_event<LPH, true>(p, s, dsmem);
-    else search_event<LPH, false>(p, s, dsmem);
+    if (n_hits <= p.smem_hit_capacity) search_event<LPH, true, false>(p, s, dsmem);
+    else search_event<LPH, false, false>(p, s, dsmem);
+  }
+
+  // The learned search (flat seeding with the seed pruner; with seed_model null, the plain
+  // search, recording training doublets when asked) is a kernel of its own, so the plain
+  // kernels keep their register budget.
+  template<unsigned THREADS>
+  __global__ void __launch_bounds__(THREADS, 768 / THREADS) search_by_triplet_learned_kernel(SearchParams p)
+  {
+    extern __shared__ __align__(128) unsigned char dsmem[];
+    __shared__ SearchSharedFlat s;
+    const unsigned* start = p.offsets_estimated_input_size + blockIdx.x * n_module_pairs;
+    const unsigned n_hits = start[n_module_pairs] - start[0];
+    if (n_hits <= p.smem_hit_capacity) search_event<0, true, true>(p, s, dsmem);
+    else search_event<0, false, true>(p, s, dsmem);
   }
 
 #define VELO_SEARCH_CONFIG(T, L)                                                 \
   template __global__ void search_by_triplet_kernel<T, L>(SearchParams p);
   VELO_SEARCH_CONFIGS(VELO_SEARCH_CONFIG)
 #undef VELO_SEARCH_CONFIG
+  template __global__ void search_by_triplet_learned_kernel<128>(SearchParams p);
+  template __global__ void search_by_triplet_learned_kernel<256>(SearchParams p);
+  template __global__ void search_by_triplet_learned_kernel<512>(SearchParams p);
 
 } // namespace velo
