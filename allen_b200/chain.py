@@ -63,12 +63,23 @@ OUTPUT_FIELDS = [
     "dev_offsets_velo_tracks", "dev_three_hit_tracks_output", "dev_number_of_three_hit_tracks_output",
     "dev_offsets_number_of_three_hit_tracks_filtered", "dev_offsets_all_velo_tracks",
     "dev_velo_track_hit_number", "dev_offsets_velo_track_hit_number", "dev_velo_track_hits",
-    "dev_accepted_velo_tracks",
+    "dev_accepted_velo_tracks", "dev_seed_stats",
 ]
 
 
 class OutputsC(C.Structure):
     _fields_ = [(f, C.c_void_p) for f in OUTPUT_FIELDS]
+
+
+class SeedModelC(C.Structure):
+    """VeloSeedModel of velo_b200.h."""
+    _fields_ = [("w1", (C.c_float * 12) * 32), ("b1", C.c_float * 32), ("w2", (C.c_float * 32) * 32),
+                ("b2", C.c_float * 32), ("w3", C.c_float * 32), ("b3", C.c_float), ("mean", C.c_float * 12),
+                ("inv_std", C.c_float * 12), ("threshold_logit", C.c_float), ("kept_lo", C.c_float),
+                ("kept_hi", C.c_float)]
+
+
+SEED_PARAMS = 32 * 12 + 32 + 32 * 32 + 32 + 32 + 1
 
 
 class LaunchConfigC(C.Structure):
@@ -124,6 +135,23 @@ def _lib():
     lib.velo_chain_kernel_name.argtypes = [C.c_uint]
     lib.velo_chain_kernel_times.restype = C.c_int
     lib.velo_chain_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint)]
+    lib.velo_chain_set_seed_model.restype = C.c_int
+    lib.velo_chain_set_seed_model.argtypes = [C.c_void_p, C.POINTER(SeedModelC)]
+    lib.velo_chain_record_doublets.restype = C.c_int
+    lib.velo_chain_record_doublets.argtypes = [C.c_void_p, C.c_void_p, C.c_uint, C.c_uint, C.c_void_p]
+    lib.velo_seed_trainer_create.restype = C.c_int
+    lib.velo_seed_trainer_create.argtypes = [C.POINTER(SeedModelC), C.c_float, C.c_float, C.POINTER(C.c_void_p)]
+    lib.velo_seed_trainer_step.restype = C.c_int
+    lib.velo_seed_trainer_step.argtypes = [C.c_void_p, C.c_void_p, C.c_ulonglong, C.c_uint, C.c_void_p,
+                                           C.POINTER(C.c_float)]
+    lib.velo_seed_trainer_gradients.restype = C.c_int
+    lib.velo_seed_trainer_gradients.argtypes = [C.c_void_p, C.c_void_p, C.c_ulonglong, C.c_uint, C.c_void_p,
+                                                C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    lib.velo_seed_trainer_score.restype = C.c_int
+    lib.velo_seed_trainer_score.argtypes = [C.c_void_p, C.c_void_p, C.c_ulonglong, C.c_void_p, C.c_void_p]
+    lib.velo_seed_trainer_model.restype = C.c_int
+    lib.velo_seed_trainer_model.argtypes = [C.c_void_p, C.POINTER(SeedModelC)]
+    lib.velo_seed_trainer_destroy.argtypes = [C.c_void_p]
     lib._typed = True
     return lib
 
@@ -241,6 +269,25 @@ class VeloChain:
         runs = C.c_uint()
         _check(self.lib, self.lib.velo_chain_kernel_times(self.handle, ms, C.byref(runs)))
         return {self.lib.velo_chain_kernel_name(i).decode(): float(ms[i]) for i in range(n)}, runs.value
+
+    def set_seed_model(self, model):
+        """model: a SeedModelC (learned search) or None (plain search)."""
+        _check(self.lib, self.lib.velo_chain_set_seed_model(self.handle, C.byref(model) if model is not None else None))
+
+    def record_doublets(self, records, count, every: int = 1):
+        """records: device uint8 tensor of 64-byte VeloDoubletRecord entries, count: device
+        int32 tensor of one element (zeroed by the caller); None stops the recording."""
+        if records is None:
+            _check(self.lib, self.lib.velo_chain_record_doublets(self.handle, None, 0, 1, None))
+        else:
+            _check(self.lib, self.lib.velo_chain_record_doublets(self.handle, records.data_ptr(), records.numel() // 64,
+                                                                 every, count.data_ptr()))
+
+    def seed_stats(self, n_events: int) -> np.ndarray:
+        """[n_events, 3]: doublets formed, doublets scanned, search mode (0 plain, 1 learned,
+        2 learned then plain) of the last run."""
+        p = self.device_outputs()["dev_seed_stats"]
+        return self._fetch(p, 12 * n_events, np.uint8).view(np.uint32).reshape(n_events, 3)
 
     def device_outputs(self) -> dict:
         o = OutputsC()

@@ -33,6 +33,13 @@ namespace {
     return s;
   }
 
+} // namespace
+
+namespace velo_host {
+  void set_last_error(const std::string& what) { last_error = what; }
+} // namespace velo_host
+
+namespace {
 #define VELO_CUDA(call)                                                                                 \
   do {                                                                                                  \
     const cudaError_t e_ = (call);                                                                      \
@@ -182,6 +189,16 @@ static const SearchVariant search_variants[] = {
 #undef VELO_SEARCH_VARIANT
 };
 
+static SearchKernel learned_search_kernel(unsigned threads)
+{
+  switch (threads) {
+    case 128: return velo::search_by_triplet_learned_kernel<128>;
+    case 256: return velo::search_by_triplet_learned_kernel<256>;
+    case 512: return velo::search_by_triplet_learned_kernel<512>;
+    default: return nullptr;
+  }
+}
+
 static const SearchVariant* find_search_variant(unsigned threads, unsigned lanes)
 {
   for (const auto& v : search_variants)
@@ -228,6 +245,14 @@ struct VeloChain {
   DeviceTotals* totals_host = nullptr;
   cudaEvent_t done = nullptr;
   cudaStream_t capture_stream = nullptr; // graphs are captured here (the legacy stream cannot be)
+
+  // learned seed pruner and training-doublet recording
+  DeviceBuffer<velo::MlpModelDevice> seed_model;
+  bool learned = false;
+  DeviceBuffer<unsigned> seed_stats;
+  velo::DoubletRecord* records = nullptr;
+  unsigned* record_count = nullptr;
+  unsigned record_capacity = 0, record_every = 1;
 
   // host-buffer path
   DeviceBuffer<char> in_raw;
@@ -337,12 +362,20 @@ namespace {
     sp.smem_hit_capacity = c->search_hit_capacity;
     sp.hit_scratch = c->hit_scratch.p;
     sp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
+    sp.seed_stats = c->seed_stats.p;
+    sp.seed_model = c->learned ? c->seed_model.p : nullptr;
+    sp.records = c->records;
+    sp.record_count = c->record_count;
+    sp.record_capacity = c->record_capacity;
+    sp.record_every = c->record_every;
     const unsigned search_smem = c->search_hit_capacity * search_hit_bytes;
     {
+      const SearchKernel fn = (c->learned || c->records) ? learned_search_kernel(c->search_threads) : nullptr;
       const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes);
-      if (!v) return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for this launch configuration");
+      if (!fn && !v) return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for this launch configuration");
       void* args[] = {&sp};
-      VELO_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(v->fn), dim3(n), dim3(v->threads), args, search_smem, stream));
+      VELO_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(fn ? fn : v->fn), dim3(n), dim3(c->search_threads),
+                                 args, search_smem, stream));
     }
     VELO_CUDA(mark());
 
@@ -401,6 +434,9 @@ namespace {
     VELO_CUDA(cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cluster_smem));
     for (const auto& v : search_variants)
       VELO_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(v.fn), cudaFuncAttributeMaxDynamicSharedMemorySize, search_smem));
+    for (unsigned threads : {128u, 256u, 512u})
+      VELO_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(learned_search_kernel(threads)),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, search_smem));
     return VELO_OK;
   }
 } // namespace
@@ -526,6 +562,7 @@ VeloStatus velo_chain_reserve(
   RES(c->three_out, tracks)
   RES(c->hit_used, T)
   RES(c->accepted, 2 * tracks)
+  RES(c->seed_stats, 3 * n)
   if (max_raw_bytes) {
     RES(c->in_raw, max_raw_bytes + 16)
   }
@@ -714,6 +751,7 @@ VeloStatus velo_chain_outputs(const VeloChain* c, VeloChainOutputs* o)
   o->dev_offsets_velo_track_hit_number = c->offsets_hit_number.p;
   o->dev_velo_track_hits = c->track_hits.p;
   o->dev_accepted_velo_tracks = c->accepted.p;
+  o->dev_seed_stats = c->seed_stats.p;
   return VELO_OK;
 }
 
@@ -782,6 +820,41 @@ VeloStatus velo_copy_to_device(void* device, const void* host, size_t bytes)
   return VELO_OK;
 }
 
+VeloStatus velo_chain_set_seed_model(VeloChain* c, const VeloSeedModel* model)
+{
+  if (!c) return fail(VELO_ERR_ARGUMENT, "null chain");
+  c->release_graph();
+  if (!model) {
+    c->learned = false;
+    return VELO_OK;
+  }
+  if (!learned_search_kernel(c->search_threads))
+    return fail(VELO_ERR_ARGUMENT, "the learned search needs search_threads 128, 256 or 512");
+  std::vector<float> params(VELO_SEED_PARAMS);
+  velo::model_params(*model, params.data());
+  velo::MlpModelDevice d;
+  velo::make_model_device(params.data(), *model, d);
+  if (c->seed_model.reserve(1) != cudaSuccess) return fail(VELO_ERR_CUDA, "seed model allocation failed");
+  VELO_CUDA(cudaMemcpy(c->seed_model.p, &d, sizeof(d), cudaMemcpyHostToDevice));
+  c->learned = true;
+  return configure_kernels(c);
+}
+
+VeloStatus velo_chain_record_doublets(
+  VeloChain* c, VeloDoubletRecord* records, unsigned capacity, unsigned record_every, unsigned* dev_count)
+{
+  if (!c) return fail(VELO_ERR_ARGUMENT, "null chain");
+  if (records && (!dev_count || record_every == 0)) return fail(VELO_ERR_ARGUMENT, "recording needs a counter and record_every > 0");
+  if (records && !learned_search_kernel(c->search_threads))
+    return fail(VELO_ERR_ARGUMENT, "recording needs search_threads 128, 256 or 512");
+  c->release_graph();
+  c->records = reinterpret_cast<velo::DoubletRecord*>(records);
+  c->record_count = records ? dev_count : nullptr;
+  c->record_capacity = records ? capacity : 0;
+  c->record_every = records ? record_every : 1;
+  return configure_kernels(c);
+}
+
 void velo_chain_destroy(VeloChain* c)
 {
   if (!c) return;
@@ -818,6 +891,8 @@ void velo_chain_destroy(VeloChain* c)
   c->three_out.release();
   c->hit_used.release();
   c->accepted.release();
+  c->seed_stats.release();
+  c->seed_model.release();
   c->totals_dev.release();
   c->in_raw.release();
   c->in_offsets.release();

@@ -19,6 +19,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include "velo_b200.h"
+
 namespace velo {
 
   constexpr unsigned mlp_features = 12; // inputs of the network
@@ -42,6 +44,11 @@ namespace velo {
     float threshold_logit;                    // keep a doublet when its logit > threshold
     float kept_lo, kept_hi;                   // per-event bounds of kept / found doublets
   };
+
+  // Host: a model (flat parameters w1, b1, w2, b2, w3, b3 and meta's standardisation,
+  // threshold and bounds) in its device form, with bf16 weights rounded to nearest even.
+  void make_model_device(const float* params, const VeloSeedModel& meta, MlpModelDevice& d);
+  void model_params(const VeloSeedModel& m, float* params);
 
   // One training example, written by the search in recording mode (64 bytes).
   struct DoubletRecord {

@@ -76,3 +76,15 @@ def evaluate(gen, tracks_per_event) -> dict:
         "reconstructible": n_recoble, "reconstructed": n_reco, "efficiency": n_reco / max(n_recoble, 1),
         "clones": n_clone, "clone_rate": n_clone / max(n_reco + n_clone, 1),
     }
+
+
+def tracks_from_outputs(out: dict) -> list:
+    """Per event, the LHCb ids of each consolidated track, from dev_offsets_all_velo_tracks,
+    dev_offsets_velo_track_hit_number and dev_velo_track_hits (ids first in its SoA)."""
+    off_all = np.asarray(out["dev_offsets_all_velo_tracks"]).view(np.uint32)
+    off_hn = np.asarray(out["dev_offsets_velo_track_hit_number"]).view(np.uint32)
+    th = int(off_hn[-1]) if off_hn.size else 0
+    hits = np.asarray(out["dev_velo_track_hits"]).view(np.uint8)
+    ids = hits[:4 * th].view(np.uint32)
+    return [[tuple(ids[off_hn[t]:off_hn[t + 1]]) for t in range(int(off_all[e]), int(off_all[e + 1]))]
+            for e in range(off_all.size - 1)]

@@ -103,6 +103,8 @@ typedef struct {
   unsigned* dev_offsets_velo_track_hit_number;     /* [tracks + 1] */
   char* dev_velo_track_hits;                       /* [18 TH] */
   uint8_t* dev_accepted_velo_tracks;               /* [tracks + three-hit tracks] */
+  unsigned* dev_seed_stats;                        /* [3 N]: doublets formed, doublets scanned, search
+                                                      mode (0 plain, 1 learned, 2 learned then plain) */
 } VeloChainOutputs;
 
 /* Host scalars of the last run, available after velo_chain_synchronize(). */
@@ -226,6 +228,79 @@ unsigned velo_noalloc_max_events(void);
 unsigned velo_noalloc_max_clusters(void);
 unsigned long long velo_noalloc_scratch_bytes(void);
 const char* velo_noalloc_last_error_string(void);
+
+/* Learned seed pruner (no counterpart in the reference).  A 12-32-32-1 network scores each
+ * (h0, h1) doublet of the flat seeding (SearchByTriplet.cu:298-446) before its h2 window is
+ * scanned; doublets whose logit is not above threshold_logit are not scanned.  An event whose
+ * fraction of scanned doublets falls outside [kept_lo, kept_hi] is searched again by the
+ * plain search.  Weights are used as bf16 on the tensor cores (mma.sync, fp32 accumulation);
+ * inputs are standardised with mean / inv_std.  Parameter order of a flat gradient or
+ * parameter vector (VELO_SEED_PARAMS floats): w1, b1, w2, b2, w3, b3. */
+#define VELO_SEED_FEATURES 12
+#define VELO_SEED_HIDDEN 32
+#define VELO_SEED_PARAMS (32 * 12 + 32 + 32 * 32 + 32 + 32 + 1)
+typedef struct {
+  float w1[VELO_SEED_HIDDEN][VELO_SEED_FEATURES];
+  float b1[VELO_SEED_HIDDEN];
+  float w2[VELO_SEED_HIDDEN][VELO_SEED_HIDDEN];
+  float b2[VELO_SEED_HIDDEN];
+  float w3[VELO_SEED_HIDDEN];
+  float b3;
+  float mean[VELO_SEED_FEATURES];
+  float inv_std[VELO_SEED_FEATURES];
+  float threshold_logit;
+  float kept_lo, kept_hi;
+} VeloSeedModel;
+
+/* One training doublet (64 bytes): raw features, label 1 if the plain seeding turned the
+ * doublet into a seed, event index and the two hits' indices in the sorted container.
+ * Features: tx, ty, |t|, signed distance to the beam axis, z of closest approach,
+ * phi(h1) - phi(h0) and phi(h1) (rad / pi), r(h1), dr/dz, |dz|, candidate rank, candidates. */
+typedef struct {
+  float f[VELO_SEED_FEATURES];
+  float label;
+  unsigned event, h0, h1;
+} VeloDoubletRecord;
+
+/* model != NULL: the chain searches in learned mode (flat seeding, search_threads block
+ * size); NULL: the plain search. */
+VeloStatus velo_chain_set_seed_model(VeloChain* chain, const VeloSeedModel* model);
+/* dev_records != NULL: the following runs (plain search) append the doublets of one h1
+ * candidate in record_every to dev_records (capacity entries) and count them in *dev_count
+ * (device u32; entries beyond the capacity are counted, not written). */
+VeloStatus velo_chain_record_doublets(
+  VeloChain* chain, VeloDoubletRecord* dev_records, unsigned capacity, unsigned record_every, unsigned* dev_count);
+
+/* Training on the GPU: binary cross-entropy (positives weighted by pos_weight), mean over the
+ * batch, Adam (beta1 0.9, beta2 0.999, eps 1e-8).  Forward and backward passes are warp-level
+ * tensor-core kernels over 16-doublet tiles. */
+typedef struct VeloSeedTrainer VeloSeedTrainer;
+VeloStatus velo_seed_trainer_create(
+  const VeloSeedModel* init, float learning_rate, float pos_weight, VeloSeedTrainer** trainer);
+/* One Adam step on records [first, first + batch).  loss (optional, host) receives the
+ * batch's mean loss and makes the call synchronous. */
+VeloStatus velo_seed_trainer_step(
+  VeloSeedTrainer* trainer,
+  const VeloDoubletRecord* dev_records,
+  unsigned long long first,
+  unsigned batch,
+  VeloStream stream,
+  float* loss);
+/* Gradients (VELO_SEED_PARAMS floats, host) and mean loss of a batch, without a step. */
+VeloStatus velo_seed_trainer_gradients(
+  VeloSeedTrainer* trainer,
+  const VeloDoubletRecord* dev_records,
+  unsigned long long first,
+  unsigned batch,
+  VeloStream stream,
+  float* grads,
+  float* loss);
+/* Logits of records [0, n) into dev_logits (device floats) with the current weights. */
+VeloStatus velo_seed_trainer_score(
+  VeloSeedTrainer* trainer, const VeloDoubletRecord* dev_records, unsigned long long n, float* dev_logits, VeloStream stream);
+/* The current fp32 weights, with the standardisation, threshold and bounds of the model. */
+VeloStatus velo_seed_trainer_model(VeloSeedTrainer* trainer, VeloSeedModel* model);
+void velo_seed_trainer_destroy(VeloSeedTrainer* trainer);
 
 /* Utilities (synchronous copies on the current device), for callers without a CUDA runtime binding. */
 VeloStatus velo_copy_to_host(void* host, const void* device, size_t bytes);
