@@ -430,13 +430,12 @@ namespace {
     using namespace velo;
     const int cluster_smem = int(cluster_sort_blob_offset(c->cluster_stage_capacity) + c->cluster_blob_bytes);
     const int search_smem = int(c->search_hit_capacity * search_hit_bytes);
-    VELO_CUDA(cudaFuncSetAttribute(estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c->estimate_blob_bytes)));
-    VELO_CUDA(cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cluster_smem));
+    VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(estimate_kernel), int(c->estimate_blob_bytes)));
+    VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(cluster_sort_kernel), cluster_smem));
     for (const auto& v : search_variants)
-      VELO_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(v.fn), cudaFuncAttributeMaxDynamicSharedMemorySize, search_smem));
+      VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(v.fn), search_smem));
     for (unsigned threads : {128u, 256u, 512u})
-      VELO_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(learned_search_kernel(threads)),
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, search_smem));
+      VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(learned_search_kernel(threads)), search_smem));
     return VELO_OK;
   }
 } // namespace

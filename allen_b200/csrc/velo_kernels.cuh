@@ -129,6 +129,17 @@ namespace velo {
   __global__ void consolidate_kernel(ConsolidateParams p);
   __global__ void exclusive_scan_kernel(ScanParams p);
 
+  // Raises a kernel's dynamic shared-memory limit to at least `bytes`, never lowers it: the
+  // limit is per kernel and per device, shared by every chain and entry point in the process.
+  inline cudaError_t raise_dynamic_smem_limit(const void* kernel, int bytes)
+  {
+    cudaFuncAttributes a;
+    const cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+    if (e != cudaSuccess) return e;
+    if (a.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  }
+
   constexpr unsigned decode_threads = 256;
   constexpr unsigned scan_threads = 1024;
   constexpr unsigned consolidate_threads = 256;

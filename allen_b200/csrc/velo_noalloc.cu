@@ -153,9 +153,9 @@ namespace {
       const cudaError_t e = cudaGetSymbolAddress(&ptr, velo_noalloc_scratch);
       if (e != cudaSuccess) return fail(VELO_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
       const int cluster_smem = int(velo::cluster_sort_blob_offset(cluster_stage_capacity) + cluster_blob_bytes);
-      if (cudaFuncSetAttribute(velo::estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(estimate_blob_bytes)) !=
+      if (velo::raise_dynamic_smem_limit(reinterpret_cast<const void*>(velo::estimate_kernel), int(estimate_blob_bytes)) !=
             cudaSuccess ||
-          cudaFuncSetAttribute(velo::cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cluster_smem) !=
+          velo::raise_dynamic_smem_limit(reinterpret_cast<const void*>(velo::cluster_sort_kernel), cluster_smem) !=
             cudaSuccess)
         return fail(VELO_ERR_CUDA, "cannot set the kernels' shared-memory limits");
       scratch_address[device] = static_cast<unsigned char*>(ptr);
