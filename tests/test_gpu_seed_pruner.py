@@ -130,3 +130,35 @@ def test_anomalous_events_fall_back_to_the_plain_search(flat_chain, oracle, geom
     assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
     st = flat_chain.seed_stats(g.raw.n_events)
     assert (st[:, 2] == 2).all() and (st[:, 1] == 0).all()
+
+
+def test_trained_network_prunes_doublets_at_equal_efficiency(flat_chain):
+    """What training buys: an untrained network at the same recall calibration keeps nearly
+    every doublet; after a few hundred Adam steps on plain-search labels the learned search
+    scans far fewer doublets with (almost) the same tracking efficiency."""
+    from allen_b200 import seed_pruner as sp
+    from allen_b200.chain import upload
+    from allen_b200.rawbanks import super_pixels_per_event
+    train, n, _ = sp.collect_generated(flat_chain, 8000, 8000, 901, 4, 8000 * 1200 + 4096)
+    val, n_val, _ = sp.collect_generated(flat_chain, 2000, 2000, 902, 4, 2000 * 1200 + 4096)
+    model = sp.initial_model(train, n, seed=1)
+    tr = sp.Trainer(model, lr=1e-3)
+    try:
+        thr0, before = sp.calibrate_threshold(tr, val, n_val, 0.995)
+        sp.train(tr, train, n, epochs=4, batch=16384, seed=2)
+        thr1, after = sp.calibrate_threshold(tr, val, n_val, 0.995)
+        trained = tr.model()
+    finally:
+        tr.close()
+    assert after["kept_fraction"] < 0.8 * before["kept_fraction"]
+    trained.threshold_logit = thr1
+    trained.kept_lo, trained.kept_hi = 0.0, 1.0
+    g = generator.generate(300, seed=903)
+    flat_chain.reserve_for(g.raw)
+    flat_chain.set_seed_model(None)
+    plain = sp.quality(flat_chain, g)
+    flat_chain.set_seed_model(trained)
+    learned = sp.quality(flat_chain, g)
+    assert learned["doublets_scanned"] < 0.8 * plain["doublets_scanned"]
+    assert learned["efficiency"] >= plain["efficiency"] - 0.005
+    assert learned["ghost_rate"] <= plain["ghost_rate"] + 0.005
