@@ -60,9 +60,20 @@ def train_phase():
     p.add_argument("--pos-weight", type=float, default=1.0)
     p.add_argument("--recall", type=float, default=0.995)
     p.add_argument("--pileup", type=float, default=7.6)
+    p.add_argument("--noise", type=float, default=1e-5, help="noise pixels per pixel of the evaluation events")
+    p.add_argument("--efficiency", type=float, default=0.98, help="hit efficiency of the evaluation events")
+    p.add_argument("--evaluate-only", default="", help="skip training: evaluate this saved model")
     p.add_argument("--out", default=DEFAULT_MODEL)
     p.add_argument("--report", default="")
     args = p.parse_args()
+    if args.evaluate_only:
+        torch.cuda.set_device(0)
+        t0 = time.time()
+        log = lambda m: print(f"[{time.time() - t0:7.1f} s] {m}", flush=True)  # noqa: E731
+        chain = VeloChain()
+        chain.configure(search_lanes_per_seed=0)
+        report = {"args": vars(args), "device": torch.cuda.get_device_name(0), "model": args.evaluate_only}
+        return args, report, chain, sp.load(args.evaluate_only), log
     torch.cuda.set_device(0)
     t0 = time.time()
     log = lambda m: print(f"[{time.time() - t0:7.1f} s] {m}", flush=True)  # noqa: E731
@@ -96,10 +107,12 @@ def train_phase():
     return args, report, chain, model, log
 
 
-def eval_slices(args, seed: int, n_events: int):
+def eval_slices(args, seed: int, n_events: int, training_like: bool = False):
+    """Generated slices of the evaluation configuration (or of the training one)."""
     from . import generator
     from .chain import upload
-    gens = [generator.generate(min(args.slice, n_events - f), seed=seed, first_event=f, mean_pileup=args.pileup)
+    cfg = {} if training_like else {"noise_rate": args.noise, "hit_efficiency": args.efficiency}
+    gens = [generator.generate(min(args.slice, n_events - f), seed=seed, first_event=f, mean_pileup=args.pileup, **cfg)
             for f in range(0, n_events, args.slice)]
     return gens, [upload(g.raw) for g in gens]
 
@@ -108,9 +121,15 @@ def main():
     import torch
     from .rawbanks import super_pixels_per_event
     args, report, chain, model, log = train_phase()
+    if not args.evaluate_only:
+        calibrate_bounds(args, report, chain, model, log)
+    evaluate(args, report, chain, model, log)
 
+
+def calibrate_bounds(args, report, chain, model, log):
+    from .rawbanks import super_pixels_per_event
     # fallback bounds from held-out events (stream 303)
-    gens, dev = eval_slices(args, 303, min(args.val_events, args.slice))
+    gens, dev = eval_slices(args, 303, min(args.val_events, args.slice), training_like=True)
     chain.reserve(max(g.raw.n_events for g in gens), max(int(super_pixels_per_event(g.raw).sum()) for g in gens) + 64)
     lo, hi, fstats = kept_fraction_bounds(chain, model, dev, [g.raw.n_events for g in gens])
     model.kept_lo, model.kept_hi = lo, hi
@@ -118,8 +137,10 @@ def main():
     log(f"fallback bounds [{lo:.4f}, {hi:.4f}] {fstats}")
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     sp.save(model, args.out)
-    del gens, dev
 
+
+def evaluate(args, report, chain, model, log):
+    from .rawbanks import super_pixels_per_event
     # evaluation on held-out events (stream 404): throughput of the whole chain per mode
     gens, dev = eval_slices(args, 404, args.eval_events)
     chain.reserve(max(g.raw.n_events for g in gens), max(int(super_pixels_per_event(g.raw).sum()) for g in gens) + 64)
@@ -159,7 +180,8 @@ def main():
 
 def _generate_quality(args):
     from . import generator
-    return generator.generate(args.quality_events, seed=505, mean_pileup=args.pileup)
+    return generator.generate(args.quality_events, seed=505, mean_pileup=args.pileup, noise_rate=args.noise,
+                              hit_efficiency=args.efficiency)
 
 
 if __name__ == "__main__":

@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-learned", action="store_true", help="skip the learned-mode measurement")
     return p.parse_args()
 
 
@@ -333,6 +334,45 @@ def run_ours(args):
     chain_gbs = sum(chain_bytes(c["n"], c["raw_bytes"], c["H"], c["TH"], c["tracks_all"]) for c in counts) \
         * args.steps / (ms / 1e3) / 1e9
 
+    # the same workload in learned mode (the committed seed pruner), same timing rules
+    learned = None
+    if not args.no_learned:
+        from allen_b200 import seed_pruner
+        model_path = os.path.join(REPO, "allen_b200", "data", "seed_pruner.npz")
+        chain.set_seed_model(seed_pruner.load(model_path))
+        for _ in range(max(3, args.warmup)):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        l_start, l_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l_start.record(stream)
+        for _ in range(args.steps):
+            step()
+        l_end.record(stream)
+        torch.cuda.synchronize()
+        l_ms = l_start.elapsed_time(l_end)
+        if world > 1:
+            t = torch.tensor([l_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            l_ms = float(t.item())
+        doublets = scanned = fallback = 0
+        for s, d in zip(slices, dev):
+            chain.run(d, use_graph=True)
+            chain.synchronize(check=False)
+            st = chain.seed_stats(s.n_events)
+            doublets += int(st[:, 0].sum())
+            scanned += int(st[:, 1].sum())
+            fallback += int((st[:, 2] == 2).sum())
+        chain.set_seed_model(None)
+        l_value = world * events_step * args.steps / (l_ms / 1e3)
+        learned = {"value": round(l_value, 1), "unit": UNIT, "ratio_vs_plain": round(l_value / value, 4),
+                   "doublets_scanned_fraction": round(scanned / max(doublets, 1), 4),
+                   "fallback_event_fraction": round(fallback / max(events_step, 1), 6),
+                   "model": "allen_b200/data/seed_pruner.npz",
+                   "quality": "efficiency and ghost-rate deltas vs plain: "
+                              "profiles/seed_pruner_train300k_eval100k_nu7.6.md"}
+
     # end to end through the public API from page-locked host buffers: HostPipeline copies each
     # slice in, runs the chain and copies the consolidated tracks out, two chains overlapping
     e2e = None
@@ -392,6 +432,7 @@ def run_ours(args):
             "kernels": per_kernel,
             "gpu_launches": len(per_kernel) * len(dev) * args.steps,
             "clocks": clocks.summary(),
+            "learned": learned,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "device_flags": totals_last["device_flags"],

@@ -37,7 +37,6 @@ def flat_chain(chain):
 
 
 def _records(chain, s, every=1, capacity=1 << 20):
-    import torch
     from allen_b200 import seed_pruner as sp
     chain.reserve_for(s)
     rec, n, total = sp.collect(chain, [upload(s)], capacity, every)
@@ -137,8 +136,6 @@ def test_trained_network_prunes_doublets_at_equal_efficiency(flat_chain):
     every doublet; after a few hundred Adam steps on plain-search labels the learned search
     scans far fewer doublets with (almost) the same tracking efficiency."""
     from allen_b200 import seed_pruner as sp
-    from allen_b200.chain import upload
-    from allen_b200.rawbanks import super_pixels_per_event
     train, n, _ = sp.collect_generated(flat_chain, 8000, 8000, 901, 4, 8000 * 1200 + 4096)
     val, n_val, _ = sp.collect_generated(flat_chain, 2000, 2000, 902, 4, 2000 * 1200 + 4096)
     model = sp.initial_model(train, n, seed=1)
