@@ -1,8 +1,9 @@
 """Autotuner of the chain's launch configuration.
 
 Sweeps, on a generated workload of the target occupancy, the search kernel's block size and
-lanes per seed candidate (the compiled pairs) and the shared-memory staging capacities of
-the search, clustering and estimate kernels, by coordinate descent: each parameter in turn takes the
+lanes per seed candidate (the compiled pairs), the shared-memory staging capacities of the
+search, clustering and estimate kernels, and persistent launches with a work queue (events
+claimed per CTA) against one CTA per event, by coordinate descent: each parameter in turn takes the
 value with the highest events/s (CUDA-event timed graph replays) while the others stay at
 the current best.  The winner is written to allen_b200/data/launch_config.json, which
 VeloChain loads by default.
@@ -21,6 +22,8 @@ SEARCH_CAPACITIES = [2048, 2560, 3072, 3584, 4096, 5120]
 CLUSTER_CAPACITIES = [2048, 2560, 3072, 4096]
 CLUSTER_BLOBS = [16 * 1024, 24 * 1024, 32 * 1024, 40 * 1024]
 ESTIMATE_BLOBS = [24 * 1024, 32 * 1024, 48 * 1024]
+# (persistent, events per claim): one CTA per event, or resident CTAs claiming events
+QUEUES = [(0, 1), (1, 1), (1, 2), (1, 4)]
 
 
 def measure(chain, dev_slices, repeats=3) -> float:
@@ -64,9 +67,15 @@ def tune(chain, dev_slices, log=print) -> tuple[dict, float, list]:
         ("cluster_stage_capacity", CLUSTER_CAPACITIES),
         ("cluster_blob_bytes", CLUSTER_BLOBS),
         ("estimate_blob_bytes", ESTIMATE_BLOBS),
+        ("queue", QUEUES),
     ):
         for v in values:
-            upd = {"search_threads": v[0], "search_lanes_per_seed": v[1]} if name == "search" else {name: v}
+            if name == "search":
+                upd = {"search_threads": v[0], "search_lanes_per_seed": v[1]}
+            elif name == "queue":
+                upd = {"persistent": v[0], "events_per_claim": v[1]}
+            else:
+                upd = {name: v}
             rate = try_config(**upd)
             if rate is not None and rate > best_rate:
                 best_rate = rate

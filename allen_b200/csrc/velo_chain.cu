@@ -230,6 +230,9 @@ struct VeloChain {
   unsigned search_hit_capacity = 3072;
   unsigned search_threads = 256;
   unsigned search_lanes = 2;
+  unsigned persistent = 0;
+  unsigned events_per_claim = 1;
+  unsigned resident_estimate = 0, resident_cluster = 0, resident_search = 0; // CTAs that fit the device
 
   // workspace
   DeviceBuffer<unsigned long long> bank_index_key;
@@ -250,6 +253,7 @@ struct VeloChain {
   DeviceBuffer<velo::MlpModelDevice> seed_model;
   bool learned = false;
   DeviceBuffer<unsigned> seed_stats;
+  DeviceBuffer<unsigned> queue_next, event_order; // persistent launches: 3 claim counters, event order
   velo::DoubletRecord* records = nullptr;
   unsigned* record_count = nullptr;
   unsigned record_capacity = 0, record_every = 1;
@@ -299,6 +303,17 @@ namespace {
 
     VELO_CUDA(cudaMemsetAsync(c->bank_index_key.p, 0, n_sensors * sizeof(unsigned long long), stream));
     VELO_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(unsigned), stream));
+    // persistent launches: claim counters at zero, events ordered by raw size (largest first)
+    const bool persistent = c->persistent != 0;
+    auto queue = [&](unsigned k) {
+      return persistent ? WorkQueue {c->queue_next.p + k, c->event_order.p, c->events_per_claim} : WorkQueue {};
+    };
+    auto grid = [&](unsigned resident) { return persistent ? std::min(n, std::max(resident, 1u)) : n; };
+    if (persistent) {
+      VELO_CUDA(cudaMemsetAsync(c->queue_next.p, 0, 3 * sizeof(unsigned), stream));
+      event_order_kernel<<<1, scan_threads, 0, stream>>>(in, c->event_order.p);
+      VELO_CUDA(cudaGetLastError());
+    }
     VELO_CUDA(mark());
 
     EstimateParams ep {};
@@ -311,7 +326,8 @@ namespace {
     ep.designated_stride = (n + 255) / 256;
     ep.status = c->status.p;
     ep.smem_blob_bytes = c->estimate_blob_bytes;
-    estimate_kernel<<<n, decode_threads, c->estimate_blob_bytes, stream>>>(ep);
+    ep.queue = queue(0);
+    estimate_kernel<<<grid(c->resident_estimate), decode_threads, c->estimate_blob_bytes, stream>>>(ep);
     VELO_CUDA(cudaGetLastError());
     VELO_CUDA(mark());
 
@@ -338,7 +354,8 @@ namespace {
     cp.smem_cluster_capacity = c->cluster_stage_capacity;
     cp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
     const unsigned cluster_smem = cluster_sort_blob_offset(c->cluster_stage_capacity) + c->cluster_blob_bytes;
-    cluster_sort_kernel<<<n, decode_threads, cluster_smem, stream>>>(cp);
+    cp.queue = queue(1);
+    cluster_sort_kernel<<<grid(c->resident_cluster), decode_threads, cluster_smem, stream>>>(cp);
     VELO_CUDA(cudaGetLastError());
     VELO_CUDA(mark());
 
@@ -368,14 +385,15 @@ namespace {
     sp.record_count = c->record_count;
     sp.record_capacity = c->record_capacity;
     sp.record_every = c->record_every;
+    sp.queue = queue(2);
     const unsigned search_smem = c->search_hit_capacity * search_hit_bytes;
     {
       const SearchKernel fn = (c->learned || c->records) ? learned_search_kernel(c->search_threads) : nullptr;
       const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes);
       if (!fn && !v) return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for this launch configuration");
       void* args[] = {&sp};
-      VELO_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(fn ? fn : v->fn), dim3(n), dim3(c->search_threads),
-                                 args, search_smem, stream));
+      VELO_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(fn ? fn : v->fn), dim3(grid(c->resident_search)),
+                                 dim3(c->search_threads), args, search_smem, stream));
     }
     VELO_CUDA(mark());
 
@@ -436,6 +454,20 @@ namespace {
       VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(v.fn), search_smem));
     for (unsigned threads : {128u, 256u, 512u})
       VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(learned_search_kernel(threads)), search_smem));
+    // CTAs of each kernel resident on the device at once: the grid of a persistent launch
+    int sms = 0, per_sm = 0;
+    VELO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, estimate_kernel, decode_threads, c->estimate_blob_bytes));
+    c->resident_estimate = unsigned(std::max(per_sm, 1) * sms);
+    VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel, decode_threads, cluster_smem));
+    c->resident_cluster = unsigned(std::max(per_sm, 1) * sms);
+    const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes);
+    const SearchKernel learned = learned_search_kernel(c->search_threads);
+    SearchKernel fn = (c->learned || c->records) && learned ? learned : (v ? v->fn : nullptr);
+    if (fn) {
+      VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, int(c->search_threads), search_smem));
+      c->resident_search = unsigned(std::max(per_sm, 1) * sms);
+    }
     return VELO_OK;
   }
 } // namespace
@@ -562,6 +594,8 @@ VeloStatus velo_chain_reserve(
   RES(c->hit_used, T)
   RES(c->accepted, 2 * tracks)
   RES(c->seed_stats, 3 * n)
+  RES(c->queue_next, 3)
+  RES(c->event_order, n)
   if (max_raw_bytes) {
     RES(c->in_raw, max_raw_bytes + 16)
   }
@@ -642,7 +676,7 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
   if (cfg->search_hit_capacity * velo::search_hit_bytes + search_static > unsigned(optin) ||
       cluster_dyn + 16 * 1024 > unsigned(optin) || cfg->estimate_blob_bytes + 16 * 1024 > unsigned(optin) ||
       cfg->search_hit_capacity > 65536 || cfg->cluster_stage_capacity > 65535 || (cfg->cluster_blob_bytes & 15) ||
-      (cfg->estimate_blob_bytes & 15))
+      (cfg->estimate_blob_bytes & 15) || cfg->persistent > 1 || cfg->events_per_claim < 1 || cfg->events_per_claim > 64)
     return fail(VELO_ERR_ARGUMENT, "launch configuration exceeds the device's shared memory");
   c->release_graph();
   c->search_threads = cfg->search_threads;
@@ -651,6 +685,8 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
   c->cluster_stage_capacity = cfg->cluster_stage_capacity;
   c->cluster_blob_bytes = cfg->cluster_blob_bytes;
   c->estimate_blob_bytes = cfg->estimate_blob_bytes;
+  c->persistent = cfg->persistent;
+  c->events_per_claim = cfg->events_per_claim;
   return configure_kernels(c);
 }
 
@@ -663,6 +699,8 @@ VeloStatus velo_chain_get_config(const VeloChain* c, VeloLaunchConfig* cfg)
   cfg->cluster_stage_capacity = c->cluster_stage_capacity;
   cfg->cluster_blob_bytes = c->cluster_blob_bytes;
   cfg->estimate_blob_bytes = c->estimate_blob_bytes;
+  cfg->persistent = c->persistent;
+  cfg->events_per_claim = c->events_per_claim;
   return VELO_OK;
 }
 
@@ -891,6 +929,8 @@ void velo_chain_destroy(VeloChain* c)
   c->hit_used.release();
   c->accepted.release();
   c->seed_stats.release();
+  c->queue_next.release();
+  c->event_order.release();
   c->seed_model.release();
   c->totals_dev.release();
   c->in_raw.release();

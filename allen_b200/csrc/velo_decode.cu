@@ -66,13 +66,15 @@ namespace velo {
 
   // Stages the event blob into `smem_blob` (16-byte aligned) when it fits; returns the
   // address of the event's first word (shared or global) and its length in words.
-  // Ends with a __syncthreads().  `bar` must have been initialised with count 1.
+  // Ends with a __syncthreads().  `bar` must have been initialised with count 1; bar_phase
+  // (the same in every thread) is the parity of its current phase.
   __device__ const uint32_t* stage_event(
     const RawInput& in,
     unsigned ev,
     unsigned char* smem_blob,
     unsigned smem_blob_bytes,
     uint64_t* bar,
+    unsigned& bar_phase,
     unsigned* status,
     unsigned& n_words,
     unsigned& staged_bytes)
@@ -105,12 +107,13 @@ namespace velo {
     bool ok = true;
     if (bulk > 0) {
       unsigned rounds = 0;
-      while (!mbar_try_wait(bar, 0)) {
+      while (!mbar_try_wait(bar, bar_phase)) {
         if (++rounds > bulk_wait_limit) {
           ok = false;
           break;
         }
       }
+      bar_phase ^= 1u; // each completed copy advances the barrier by one phase
     }
     __syncthreads();
     if (!ok) {
@@ -347,27 +350,22 @@ namespace velo {
   // estimate_kernel: dev_number_of_candidates, dev_velo_bank_index (as a max-reduced
   // key), dev_estimated_input_size and dev_module_candidate_num.
   // ------------------------------------------------------------------------------------
-  __global__ void __launch_bounds__(decode_threads) estimate_kernel(EstimateParams p)
+  __device__ __forceinline__ void estimate_event(const EstimateParams& p, unsigned e, uint64_t* bar, unsigned& bar_phase)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ BankTable bt;
     __shared__ unsigned est_mp[n_module_pairs];
     __shared__ unsigned cand_count;
     __shared__ unsigned warp_sums[33];
-    __shared__ __align__(8) uint64_t bar;
 
-    const unsigned e = blockIdx.x;
     const unsigned ev = e + p.in.event_start;
     const bool v23 = p.in.bank_version == 2 || p.in.bank_version == 3;
     if (threadIdx.x < n_module_pairs) est_mp[threadIdx.x] = 0;
-    if (threadIdx.x == 0) {
-      cand_count = 0;
-      mbar_init(&bar, 1);
-    }
+    if (threadIdx.x == 0) cand_count = 0;
     __syncthreads();
 
     unsigned n_words, staged;
-    const uint32_t* words = stage_event(p.in, ev, dsmem, p.smem_blob_bytes, &bar, p.status, n_words, staged);
+    const uint32_t* words = stage_event(p.in, ev, dsmem, p.smem_blob_bytes, bar, bar_phase, p.status, n_words, staged);
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
     (void) staged; // the candidate count runs the full scans: only non-isolated SPs (a third)
                    // search, which costs less than sorting every bank
@@ -419,6 +417,15 @@ namespace velo {
       p.module_candidate_num[e] = cand_count;
     }
     (void) v23;
+  }
+
+  __global__ void __launch_bounds__(decode_threads) estimate_kernel(EstimateParams p)
+  {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    unsigned bar_phase = 0;
+    for_each_event(p.queue, p.in.n_events, [&](unsigned e, unsigned) { estimate_event(p, e, &bar, bar_phase); });
   }
 
   // ------------------------------------------------------------------------------------
@@ -624,7 +631,8 @@ namespace velo {
     const uint32_t old = atomicAdd(reinterpret_cast<uint32_t*>(counters) + (b >> 1), 1u << shift);
     return static_cast<uint16_t>(old >> shift);
   }
-  __global__ void __launch_bounds__(decode_threads) cluster_sort_kernel(ClusterSortParams p)
+  __device__ __forceinline__ void
+  cluster_sort_event(const ClusterSortParams& p, unsigned e, uint64_t* bar, unsigned& bar_phase)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ BankTable bt;
@@ -634,9 +642,7 @@ namespace velo {
     __shared__ unsigned sorted_total;
     __shared__ uint32_t queue[candidate_queue];
     __shared__ unsigned queue_count[2];
-    __shared__ __align__(8) uint64_t bar;
 
-    const unsigned e = blockIdx.x;
     const unsigned ev = e + p.in.event_start;
     const unsigned n = p.in.n_events;
     const int version = p.in.bank_version;
@@ -649,7 +655,6 @@ namespace velo {
     }
 
     if (threadIdx.x == 0) {
-      mbar_init(&bar, 1);
       unsigned s = 0;
       for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
         region[mp] = s;
@@ -681,7 +686,7 @@ namespace velo {
       reinterpret_cast<uint32_t*>(bucket_start)[i] = 0;
 
     unsigned n_words, staged;
-    const uint32_t* words = stage_event(p.in, ev, blob, p.smem_blob_bytes, &bar, p.status, n_words, staged);
+    const uint32_t* words = stage_event(p.in, ev, blob, p.smem_blob_bytes, bar, bar_phase, p.status, n_words, staged);
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
     const uint32_t key_mask = sp_key_mask(version);
     uint32_t* sorted = nullptr;
@@ -854,6 +859,42 @@ namespace velo {
       const unsigned mp = threadIdx.x;
       p.module_cluster_num[e * n_module_pairs + mp] = min(mp_count[mp], region[mp + 1] - region[mp]);
     }
+  }
+
+  __global__ void __launch_bounds__(decode_threads) cluster_sort_kernel(ClusterSortParams p)
+  {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    unsigned bar_phase = 0;
+    for_each_event(p.queue, p.in.n_events, [&](unsigned e, unsigned) { cluster_sort_event(p, e, &bar, bar_phase); });
+  }
+
+  // Events of the slice by raw size, largest first: a counting sort over 1024 size classes
+  // of 64 bytes (order within a class is arbitrary).  One CTA of scan_threads threads.
+  __global__ void __launch_bounds__(scan_threads) event_order_kernel(RawInput in, unsigned* order)
+  {
+    constexpr unsigned classes = 1024;
+    __shared__ unsigned count[classes];
+    __shared__ unsigned warp_sums[33];
+    for (unsigned c = threadIdx.x; c < classes; c += blockDim.x)
+      count[c] = 0;
+    __syncthreads();
+    auto size_class = [&](unsigned e) {
+      const unsigned bytes = in.offsets[e + in.event_start + 1] - in.offsets[e + in.event_start];
+      return classes - 1 - min(bytes / 64u, classes - 1); // descending size
+    };
+    for (unsigned e = threadIdx.x; e < in.n_events; e += blockDim.x)
+      atomicAdd(&count[size_class(e)], 1u);
+    __syncthreads();
+    unsigned total;
+    const unsigned mine = threadIdx.x < classes ? count[threadIdx.x] : 0u;
+    const unsigned excl = block_exclusive_scan(mine, warp_sums, &total);
+    __syncthreads();
+    if (threadIdx.x < classes) count[threadIdx.x] = excl;
+    __syncthreads();
+    for (unsigned e = threadIdx.x; e < in.n_events; e += blockDim.x)
+      order[atomicAdd(&count[size_class(e)], 1u)] = e;
   }
 
   // ------------------------------------------------------------------------------------

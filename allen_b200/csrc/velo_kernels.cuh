@@ -6,6 +6,43 @@
 
 namespace velo {
 
+  // ---- persistent launches: a CTA claims events from a global counter ----
+  // next == null: one CTA per event (blockIdx.x).  Otherwise the grid holds as many CTAs as
+  // fit on the device at once and each claims `chunk` events at a time, in `order` (largest
+  // events first) when given.  Results do not depend on which CTA processes an event.
+  struct WorkQueue {
+    unsigned* next;
+    const unsigned* order;
+    unsigned chunk;
+  };
+
+  // Calls body(event, call) for the events of this CTA; call counts the CTA's events.  One
+  // call site for the body, so it is inlined once.
+  template<typename Body>
+  __device__ __forceinline__ void for_each_event(const WorkQueue& q, unsigned n, Body&& body)
+  {
+    __shared__ unsigned claimed;
+    const bool queued = q.next != nullptr;
+    unsigned first = blockIdx.x, last = blockIdx.x + 1, call = 0;
+    for (bool once = true;; once = false) {
+      if (queued) {
+        if (threadIdx.x == 0) claimed = atomicAdd(q.next, q.chunk);
+        __syncthreads();
+        first = claimed;
+        __syncthreads(); // read before thread 0 claims again
+        if (first >= n) break;
+        last = min(first + q.chunk, n);
+      }
+      else if (!once) {
+        break;
+      }
+      for (unsigned k = first; k < last; ++k) {
+        body(queued && q.order ? q.order[k] : k, call++);
+        __syncthreads(); // the next event reuses the shared memory
+      }
+    }
+  }
+
   // ---- decoding: velo_calculate_number_of_candidates + velo_estimate_input_size ----
   struct EstimateParams {
     RawInput in;
@@ -17,6 +54,7 @@ namespace velo {
     unsigned designated_stride;           // events e with e % stride == 0 set the bank index
     unsigned* status;
     unsigned smem_blob_bytes;
+    WorkQueue queue;
   };
 
   // ---- masked clustering + phi + sort by phi, one event per CTA ----
@@ -35,6 +73,7 @@ namespace velo {
     unsigned smem_blob_bytes;
     unsigned smem_cluster_capacity;             // clusters staged in shared memory per event
     unsigned cluster_capacity;                  // allocated T of the containers
+    WorkQueue queue;
   };
 
   // ---- search by triplet + three-hit filter, one event per CTA ----
@@ -67,6 +106,7 @@ namespace velo {
     unsigned* record_count;
     unsigned record_capacity;
     unsigned record_every;                        // record the doublets of one h1 in record_every
+    WorkQueue queue;
   };
 
   // seed_stats mode: the search that produced the event's tracks
@@ -127,6 +167,8 @@ namespace velo {
 // lanes 0 = flattened seeding (one thread per h1 candidate)
 #define VELO_SEARCH_CONFIGS(X) X(128, 1) X(128, 2) X(256, 1) X(256, 2) X(256, 4) X(512, 2) X(512, 4) X(128, 0) X(256, 0) X(512, 0)
   __global__ void consolidate_kernel(ConsolidateParams p);
+  // order[0..n) = the slice's events by raw size, largest first (one CTA)
+  __global__ void event_order_kernel(RawInput in, unsigned* order);
   __global__ void exclusive_scan_kernel(ScanParams p);
 
   // Raises a kernel's dynamic shared-memory limit to at least `bytes`, never lowers it: the

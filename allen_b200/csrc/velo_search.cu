@@ -768,9 +768,8 @@ namespace velo {
   }
 
   template<unsigned LPH, bool SMEM, bool LEARNED, typename Shared>
-  __device__ __forceinline__ void search_event(const SearchParams& p, Shared& s, unsigned char* dsmem)
+  __device__ __forceinline__ void search_event(const SearchParams& p, Shared& s, unsigned char* dsmem, unsigned e)
   {
-    const unsigned e = blockIdx.x;
     const unsigned n = p.n_events;
     const unsigned* start = p.offsets_estimated_input_size + e * n_module_pairs;
     const unsigned* num = p.module_cluster_num + e * n_module_pairs;
@@ -903,10 +902,12 @@ namespace velo {
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ std::conditional_t<LPH == 0, SearchSharedFlat, SearchShared> s;
-    const unsigned* start = p.offsets_estimated_input_size + blockIdx.x * n_module_pairs;
-    const unsigned n_hits = start[n_module_pairs] - start[0];
-    if (n_hits <= p.smem_hit_capacity) search_event<LPH, true, false>(p, s, dsmem);
-    else search_event<LPH, false, false>(p, s, dsmem);
+    for_each_event(p.queue, p.n_events, [&](unsigned e, unsigned) {
+      const unsigned* start = p.offsets_estimated_input_size + e * n_module_pairs;
+      const unsigned n_hits = start[n_module_pairs] - start[0];
+      if (n_hits <= p.smem_hit_capacity) search_event<LPH, true, false>(p, s, dsmem, e);
+      else search_event<LPH, false, false>(p, s, dsmem, e);
+    });
   }
 
   // The learned search (flat seeding with the seed pruner; with seed_model null, the plain
@@ -917,10 +918,12 @@ namespace velo {
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ SearchSharedFlat s;
-    const unsigned* start = p.offsets_estimated_input_size + blockIdx.x * n_module_pairs;
-    const unsigned n_hits = start[n_module_pairs] - start[0];
-    if (n_hits <= p.smem_hit_capacity) search_event<0, true, true>(p, s, dsmem);
-    else search_event<0, false, true>(p, s, dsmem);
+    for_each_event(p.queue, p.n_events, [&](unsigned e, unsigned) {
+      const unsigned* start = p.offsets_estimated_input_size + e * n_module_pairs;
+      const unsigned n_hits = start[n_module_pairs] - start[0];
+      if (n_hits <= p.smem_hit_capacity) search_event<0, true, true>(p, s, dsmem, e);
+      else search_event<0, false, true>(p, s, dsmem, e);
+    });
   }
 
 #define VELO_SEARCH_CONFIG(T, L)                                                 \

@@ -182,6 +182,10 @@ typedef struct {
   unsigned cluster_stage_capacity; /* clusters of an event staged in shared memory (22 B each) */
   unsigned cluster_blob_bytes;     /* raw event bytes staged by the clustering kernel */
   unsigned estimate_blob_bytes;    /* raw event bytes staged by the estimate kernel */
+  unsigned persistent;             /* 1: estimate, clustering and search kernels run as many CTAs
+                                      as fit the device, claiming events (largest raw size first)
+                                      from a work queue; 0: one CTA per event */
+  unsigned events_per_claim;       /* events a persistent CTA claims at once (1..64) */
 } VeloLaunchConfig;
 VeloStatus velo_chain_configure(VeloChain* chain, const VeloLaunchConfig* config);
 VeloStatus velo_chain_get_config(const VeloChain* chain, VeloLaunchConfig* config);

@@ -144,3 +144,18 @@ def test_sp_order_does_not_change_results(chain, oracle, geometry, version):
         assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
         outs.append(out)
     assert parity.same_clusters_and_tracks(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("claim", [1, 3])
+def test_persistent_work_queue_identical(chain, oracle, geometry, claim):
+    """Resident CTAs claiming events (largest first) from a work queue give the results of
+    one CTA per event, bit for bit, on an uneven slice (nu uniform in 1..15)."""
+    g = generator.generate(300, seed=78, pileup_min=1.0, pileup_max=15.0)
+    saved = chain.get_config()
+    try:
+        chain.configure(persistent=1, events_per_claim=claim)
+        totals, out = run_chain(chain, g.raw, use_graph=True)
+        assert totals["device_flags"] == 0
+        assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
+    finally:
+        chain.configure(**saved)
