@@ -64,7 +64,7 @@ namespace velo {
       uint32_t doublet;
       float fit;
     } slot[flat_slots];
-    union {
+    union alignas(16) { // ldmatrix reads 16-byte rows of mlp_rows
       uint16_t res_h2[flat_slots];
       uint32_t mlp_rows[8][16][8]; // per warp: 16 doublets x 16 bf16 inputs (learned mode)
     };
