@@ -63,7 +63,8 @@ OUTPUT_FIELDS = [
     "dev_offsets_velo_tracks", "dev_three_hit_tracks_output", "dev_number_of_three_hit_tracks_output",
     "dev_offsets_number_of_three_hit_tracks_filtered", "dev_offsets_all_velo_tracks",
     "dev_velo_track_hit_number", "dev_offsets_velo_track_hit_number", "dev_velo_track_hits",
-    "dev_accepted_velo_tracks", "dev_seed_stats",
+    "dev_accepted_velo_tracks", "dev_seed_stats", "dev_is_backward", "dev_velo_kalman_beamline_states",
+    "dev_velo_kalman_endvelo_states",
 ]
 
 
@@ -135,6 +136,11 @@ def _lib():
     lib.velo_chain_kernel_name.argtypes = [C.c_uint]
     lib.velo_chain_kernel_times.restype = C.c_int
     lib.velo_chain_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint)]
+    lib.velo_chain_set_kalman.restype = C.c_int
+    lib.velo_chain_set_kalman.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float]
+    lib.velo_kalman_filter.restype = C.c_int
+    lib.velo_kalman_filter.argtypes = [C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint, C.c_float, C.c_float,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.velo_chain_set_seed_model.restype = C.c_int
     lib.velo_chain_set_seed_model.argtypes = [C.c_void_p, C.POINTER(SeedModelC)]
     lib.velo_chain_record_doublets.restype = C.c_int
@@ -269,6 +275,19 @@ class VeloChain:
         runs = C.c_uint()
         _check(self.lib, self.lib.velo_chain_kernel_times(self.handle, ms, C.byref(runs)))
         return {self.lib.velo_chain_kernel_name(i).decode(): float(ms[i]) for i in range(n)}, runs.value
+
+    def set_kalman(self, enable: bool = True, beamline=(0.0, 0.0)):
+        """Appends velo_kalman_filter to the chain (states in the outputs)."""
+        _check(self.lib, self.lib.velo_chain_set_kalman(self.handle, int(enable), beamline[0], beamline[1]))
+        self.kalman = enable
+
+    def kalman_outputs(self, totals: dict) -> dict:
+        """dev_is_backward and the two state containers of the last run (host copies)."""
+        p = self.device_outputs()
+        reco = totals["host_number_of_reconstructed_velo_tracks"]
+        return {"dev_is_backward": self._fetch(p["dev_is_backward"], reco, np.uint8),
+                "dev_velo_kalman_beamline_states": self._fetch(p["dev_velo_kalman_beamline_states"], 56 * reco, np.uint8),
+                "dev_velo_kalman_endvelo_states": self._fetch(p["dev_velo_kalman_endvelo_states"], 56 * reco, np.uint8)}
 
     def set_seed_model(self, model):
         """model: a SeedModelC (learned search) or None (plain search)."""

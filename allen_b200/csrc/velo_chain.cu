@@ -206,11 +206,11 @@ static const SearchVariant* find_search_variant(unsigned threads, unsigned lanes
   return nullptr;
 }
 
-static constexpr unsigned n_timed_kernels = 7;
+static constexpr unsigned n_timed_kernels = 8;
 static const char* const kernel_names[n_timed_kernels] = {
   "estimate_kernel", "exclusive_scan_kernel(candidates, estimates)", "cluster_sort_kernel",
   "search_by_triplet_kernel", "exclusive_scan_kernel(tracks, three-hit, track hits)", "consolidate_kernel",
-  "totals_kernel"};
+  "kalman_filter_kernel", "totals_kernel"};
 
 struct VeloChain {
   int device = 0;
@@ -254,6 +254,11 @@ struct VeloChain {
   bool learned = false;
   DeviceBuffer<unsigned> seed_stats;
   DeviceBuffer<unsigned> queue_next, event_order; // persistent launches: 3 claim counters, event order
+  // velo_kalman_filter after consolidation (optional)
+  bool kalman = false;
+  float beamline[2] = {0.f, 0.f};
+  DeviceBuffer<uint8_t> is_backward;
+  DeviceBuffer<float> kalman_beamline_states, kalman_endvelo_states;
   velo::DoubletRecord* records = nullptr;
   unsigned* record_count = nullptr;
   unsigned record_capacity = 0, record_every = 1;
@@ -288,6 +293,26 @@ struct VeloChain {
 };
 
 namespace {
+  VeloStatus launch_kalman(VeloChain* c, unsigned n, cudaStream_t stream)
+  {
+    velo::KalmanParams p {};
+    p.n_events = n;
+    p.offsets_all_velo_tracks = c->offsets_all.p;
+    p.offsets_velo_track_hit_number = c->offsets_hit_number.p;
+    p.velo_track_hits = c->track_hits.p;
+    p.beamline_x = c->beamline[0];
+    p.beamline_y = c->beamline[1];
+    p.track_capacity = static_cast<unsigned>(c->cap_tracks);
+    p.is_backward = c->is_backward.p;
+    p.beamline_states = c->kalman_beamline_states.p;
+    p.endvelo_states = c->kalman_endvelo_states.p;
+    p.status = c->status.p;
+    const unsigned blocks = std::min<unsigned>(unsigned((c->cap_tracks + 255) / 256), 148u * 8u);
+    velo::kalman_filter_kernel<<<std::max(blocks, 1u), velo::kalman_threads, 0, stream>>>(p);
+    VELO_CUDA(cudaGetLastError());
+    return VELO_OK;
+  }
+
   VeloStatus enqueue_chain(VeloChain* c, const VeloDeviceSlice& s, cudaStream_t stream, cudaEvent_t* ev, bool capturing)
   {
     using namespace velo;
@@ -426,6 +451,12 @@ namespace {
     kp.status = c->status.p;
     consolidate_kernel<<<n, consolidate_threads, 0, stream>>>(kp);
     VELO_CUDA(cudaGetLastError());
+    VELO_CUDA(mark());
+
+    if (c->kalman) {
+      const VeloStatus st = launch_kalman(c, n, stream);
+      if (st != VELO_OK) return st;
+    }
     VELO_CUDA(mark());
 
     totals_kernel<<<1, 1, 0, stream>>>(
@@ -595,6 +626,9 @@ VeloStatus velo_chain_reserve(
   RES(c->accepted, 2 * tracks)
   RES(c->seed_stats, 3 * n)
   RES(c->queue_next, 3)
+  RES(c->is_backward, tracks)
+  RES(c->kalman_beamline_states, 14 * tracks)
+  RES(c->kalman_endvelo_states, 14 * tracks)
   RES(c->event_order, n)
   if (max_raw_bytes) {
     RES(c->in_raw, max_raw_bytes + 16)
@@ -789,6 +823,9 @@ VeloStatus velo_chain_outputs(const VeloChain* c, VeloChainOutputs* o)
   o->dev_velo_track_hits = c->track_hits.p;
   o->dev_accepted_velo_tracks = c->accepted.p;
   o->dev_seed_stats = c->seed_stats.p;
+  o->dev_is_backward = c->is_backward.p;
+  o->dev_velo_kalman_beamline_states = reinterpret_cast<char*>(c->kalman_beamline_states.p);
+  o->dev_velo_kalman_endvelo_states = reinterpret_cast<char*>(c->kalman_endvelo_states.p);
   return VELO_OK;
 }
 
@@ -854,6 +891,54 @@ VeloStatus velo_copy_to_host_async(void* host, const void* device, size_t bytes,
 VeloStatus velo_copy_to_device(void* device, const void* host, size_t bytes)
 {
   VELO_CUDA(cudaMemcpy(device, host, bytes, cudaMemcpyHostToDevice));
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_set_kalman(VeloChain* c, int enable, float beamline_x, float beamline_y)
+{
+  if (!c) return fail(VELO_ERR_ARGUMENT, "null chain");
+  c->release_graph();
+  c->kalman = enable != 0;
+  c->beamline[0] = beamline_x;
+  c->beamline[1] = beamline_y;
+  return VELO_OK;
+}
+
+VeloStatus velo_kalman_filter(
+  unsigned n_events,
+  const unsigned* dev_offsets_all_velo_tracks,
+  const unsigned* dev_offsets_velo_track_hit_number,
+  const char* dev_velo_track_hits,
+  unsigned track_capacity,
+  float beamline_x,
+  float beamline_y,
+  uint8_t* dev_is_backward,
+  char* dev_velo_kalman_beamline_states,
+  char* dev_velo_kalman_endvelo_states,
+  unsigned* dev_status,
+  VeloStream stream)
+{
+  if (!dev_offsets_all_velo_tracks || !dev_offsets_velo_track_hit_number || !dev_velo_track_hits || !dev_is_backward ||
+      !dev_velo_kalman_beamline_states || !dev_velo_kalman_endvelo_states)
+    return fail(VELO_ERR_ARGUMENT, "null argument");
+  if ((reinterpret_cast<uintptr_t>(dev_velo_kalman_beamline_states) |
+       reinterpret_cast<uintptr_t>(dev_velo_kalman_endvelo_states)) & 7u)
+    return fail(VELO_ERR_ARGUMENT, "state buffers must be 8-byte aligned");
+  velo::KalmanParams p {};
+  p.n_events = n_events;
+  p.offsets_all_velo_tracks = dev_offsets_all_velo_tracks;
+  p.offsets_velo_track_hit_number = dev_offsets_velo_track_hit_number;
+  p.velo_track_hits = dev_velo_track_hits;
+  p.beamline_x = beamline_x;
+  p.beamline_y = beamline_y;
+  p.track_capacity = track_capacity;
+  p.is_backward = dev_is_backward;
+  p.beamline_states = reinterpret_cast<float*>(dev_velo_kalman_beamline_states);
+  p.endvelo_states = reinterpret_cast<float*>(dev_velo_kalman_endvelo_states);
+  p.status = dev_status;
+  const unsigned blocks = std::min<unsigned>((track_capacity + 255) / 256, 148u * 8u);
+  velo::kalman_filter_kernel<<<std::max(blocks, 1u), velo::kalman_threads, 0, static_cast<cudaStream_t>(stream)>>>(p);
+  VELO_CUDA(cudaGetLastError());
   return VELO_OK;
 }
 
@@ -930,6 +1015,9 @@ void velo_chain_destroy(VeloChain* c)
   c->accepted.release();
   c->seed_stats.release();
   c->queue_next.release();
+  c->is_backward.release();
+  c->kalman_beamline_states.release();
+  c->kalman_endvelo_states.release();
   c->event_order.release();
   c->seed_model.release();
   c->totals_dev.release();

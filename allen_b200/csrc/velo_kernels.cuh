@@ -167,6 +167,21 @@ namespace velo {
 // lanes 0 = flattened seeding (one thread per h1 candidate)
 #define VELO_SEARCH_CONFIGS(X) X(128, 1) X(128, 2) X(256, 1) X(256, 2) X(256, 4) X(512, 2) X(512, 4) X(128, 0) X(256, 0) X(512, 0)
   __global__ void consolidate_kernel(ConsolidateParams p);
+  // ---- velo_kalman_filter: one thread per consolidated track ----
+  struct KalmanParams {
+    unsigned n_events;
+    const unsigned* offsets_all_velo_tracks;       // [N + 1]
+    const unsigned* offsets_velo_track_hit_number; // [tracks + 1]
+    const char* velo_track_hits;                   // consolidated hits (ids, then x y z)
+    float beamline_x, beamline_y;                  // Constants::dev_beamline
+    unsigned track_capacity;                       // entries of the outputs
+    uint8_t* is_backward;                          // [tracks] dev_is_backward
+    float* beamline_states;                        // [14 tracks] dev_velo_kalman_beamline_states
+    float* endvelo_states;                         // [14 tracks] dev_velo_kalman_endvelo_states
+    unsigned* status;
+  };
+  __global__ void kalman_filter_kernel(KalmanParams p);
+
   // order[0..n) = the slice's events by raw size, largest first (one CTA)
   __global__ void event_order_kernel(RawInput in, unsigned* order);
   __global__ void exclusive_scan_kernel(ScanParams p);
@@ -183,6 +198,7 @@ namespace velo {
   }
 
   constexpr unsigned decode_threads = 256;
+  constexpr unsigned kalman_threads = 256;
   constexpr unsigned scan_threads = 1024;
   constexpr unsigned consolidate_threads = 256;
   constexpr unsigned search_hit_bytes = 15; // x, y, z, phi, flags per staged hit

@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-mode measurement")
+    p.add_argument("--no-kalman", action="store_true", help="skip the velo_kalman_filter measurement")
     return p.parse_args()
 
 
@@ -373,6 +374,45 @@ def run_ours(args):
                    "quality": "efficiency and ghost-rate deltas vs plain: "
                               "profiles/seed_pruner_train300k_eval100k_nu7.6.md"}
 
+    # velo_kalman_filter appended to the chain (the next stage of the reference sequence)
+    kalman = None
+    if not args.no_kalman:
+        chain.set_kalman(True)
+        for _ in range(max(3, args.warmup)):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        k_start, k_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k_start.record(stream)
+        for _ in range(args.steps):
+            step()
+        k_end.record(stream)
+        torch.cuda.synchronize()
+        k_ms = k_start.elapsed_time(k_end)
+        if world > 1:
+            t = torch.tensor([k_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            k_ms = float(t.item())
+        try:
+            kt, kruns = chain.kernel_times()
+            kf_ms = kt.get("kalman_filter_kernel", 0.0) / max(kruns, 1)
+        except Exception:
+            kf_ms = None
+        chain.set_kalman(False)
+        # bytes of one launch: track and hit offsets, x y z of every track hit in, is_backward and
+        # two 56-byte states per track out
+        kf_bytes = sum(4 * (c["n"] + 1) + 4 * (c["tracks_all"] + 1) + 12 * c["TH"] + 113 * c["tracks_all"]
+                       for c in counts) / len(counts)
+        kf_gbs = kf_bytes / (kf_ms / 1e3) / 1e9 if kf_ms else None
+        kalman = {"value": round(world * events_step * args.steps / (k_ms / 1e3), 1), "unit": UNIT,
+                  "kernel": "kalman_filter_kernel", "ms_per_launch": round(kf_ms, 4) if kf_ms else None,
+                  "bytes_per_launch": int(kf_bytes),
+                  "roofline": {"bound": "hbm", "achieved": round(kf_gbs, 1) if kf_gbs else None, "peak": peak,
+                               "unit": "GB/s", "frac": round(kf_gbs / peak, 4) if kf_gbs else None,
+                               "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+                  "workload": "chain + velo_kalman_filter (beamline 0, 0) on the same events"}
+
     # end to end through the public API from page-locked host buffers: HostPipeline copies each
     # slice in, runs the chain and copies the consolidated tracks out, two chains overlapping
     e2e = None
@@ -430,9 +470,11 @@ def run_ours(args):
             "roofline": roofline,
             "chain_hbm_gbs": round(chain_gbs, 1),
             "kernels": per_kernel,
-            "gpu_launches": len(per_kernel) * len(dev) * args.steps,
+            "gpu_launches": sum(1 for v in per_kernel.values() if v["ms_per_launch"] > 0) * len(dev) * args.steps
+                            + (len(dev) * args.steps if args.events and chain.get_config().get("persistent") else 0),
             "clocks": clocks.summary(),
             "learned": learned,
+            "kalman": kalman,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "device_flags": totals_last["device_flags"],

@@ -105,6 +105,9 @@ typedef struct {
   uint8_t* dev_accepted_velo_tracks;               /* [tracks + three-hit tracks] */
   unsigned* dev_seed_stats;                        /* [3 N]: doublets formed, doublets scanned, search
                                                       mode (0 plain, 1 learned, 2 learned then plain) */
+  uint8_t* dev_is_backward;                        /* [tracks] velo_kalman_filter (when enabled) */
+  char* dev_velo_kalman_beamline_states;           /* [56 tracks] Velo::Consolidated::States */
+  char* dev_velo_kalman_endvelo_states;            /* [56 tracks] */
 } VeloChainOutputs;
 
 /* Host scalars of the last run, available after velo_chain_synchronize(). */
@@ -232,6 +235,31 @@ unsigned velo_noalloc_max_events(void);
 unsigned velo_noalloc_max_clusters(void);
 unsigned long long velo_noalloc_scratch_bytes(void);
 const char* velo_noalloc_last_error_string(void);
+
+/* velo_kalman_filter (device/velo/simplified_kalman_filter/src/VeloKalmanFilter.cu:153-399,
+ * wired at configuration/python/AllenConf/velo_reconstruction.py:295-322): the simplified
+ * Kalman fit of every consolidated track to the beamline and to the end of the VELO.
+ * velo_chain_set_kalman() appends it to the chain (outputs in VeloChainOutputs; beamline =
+ * Constants::dev_beamline, 0, 0 in beamline.bin).  velo_kalman_filter() runs it alone on
+ * caller buffers, allocating nothing: inputs are the consolidation outputs, outputs
+ * dev_is_backward [tracks] and the two Velo::Consolidated::States containers (56 bytes per
+ * track, 8-byte aligned).  States are bit-identical to the reference CPU build; the fields
+ * the reference leaves unwritten (qop, chi2, ndof) are written as 0.  track_capacity bounds
+ * the reconstructed tracks (more raise err_output_capacity in dev_status, optional). */
+VeloStatus velo_chain_set_kalman(VeloChain* chain, int enable, float beamline_x, float beamline_y);
+VeloStatus velo_kalman_filter(
+  unsigned n_events,
+  const unsigned* dev_offsets_all_velo_tracks,
+  const unsigned* dev_offsets_velo_track_hit_number,
+  const char* dev_velo_track_hits,
+  unsigned track_capacity,
+  float beamline_x,
+  float beamline_y,
+  uint8_t* dev_is_backward,
+  char* dev_velo_kalman_beamline_states,
+  char* dev_velo_kalman_endvelo_states,
+  unsigned* dev_status,
+  VeloStream stream);
 
 /* Learned seed pruner (no counterpart in the reference).  A 12-32-32-1 network scores each
  * (h0, h1) doublet of the flat seeding (SearchByTriplet.cu:298-446) before its h2 window is

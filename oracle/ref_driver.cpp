@@ -29,6 +29,7 @@
 #include "ThreeHitTracksFilter.cuh"
 #include "VeloCopyTrackHitNumber.cuh"
 #include "VeloConsolidateTracks.cuh"
+#include "VeloKalmanFilter.cuh"
 #include "HostPrefixSum.h"
 #include "ClusteringCommon.h"
 
@@ -51,8 +52,19 @@ __global__ void velo_masked_clustering_kernel(
   const float* dev_velo_sp_fx,
   const float* dev_velo_sp_fy);
 
+// VeloConsolidateTracks.cu:11-46 (defined at file scope there)
+__global__ void create_velo_views(velo_consolidate_tracks::Parameters parameters);
+
 namespace {
   using Allen::device::span;
+
+  // Uninitialised storage for n objects of a view type the reference constructs in place.
+  template<typename T>
+  struct ViewStorage {
+    std::vector<std::max_align_t> raw;
+    explicit ViewStorage(size_t n) : raw((n * sizeof(T) + sizeof(std::max_align_t) - 1) / sizeof(std::max_align_t) + 1) {}
+    T* data() { return reinterpret_cast<T*>(raw.data()); }
+  };
 
   struct Buffer {
     void* p = nullptr;
@@ -353,6 +365,56 @@ namespace {
       launch(n, [&] {
         velo_consolidate_tracks::velo_consolidate_tracks(
           p, gsl::span<unsigned> {histo.data(), histo.size()}, gsl::span<unsigned> {counter.data(), 1});
+      });
+
+      // create_velo_views (VeloConsolidateTracks.cu:99): the views velo_kalman_filter reads
+      ViewStorage<Allen::Views::Velo::Consolidated::Hits> hits_view(n);
+      ViewStorage<Allen::Views::Velo::Consolidated::Track> track_view(host_reconstructed);
+      ViewStorage<Allen::Views::Velo::Consolidated::Tracks> tracks_view(n);
+      ViewStorage<Allen::Views::Velo::Consolidated::MultiEventTracks> multi_view(1);
+      ViewStorage<Allen::IMultiEventContainer*> imec(1);
+      p.dev_velo_hits_view = sp(hits_view.data(), n);
+      p.dev_velo_track_view = sp(track_view.data(), host_reconstructed);
+      p.dev_velo_tracks_view = sp(tracks_view.data(), n);
+      p.dev_velo_multi_event_tracks_view = sp(multi_view.data(), 1);
+      p.dev_imec_velo_tracks = sp(imec.data(), 1);
+      launch(n, [&] { create_velo_views(p); });
+
+      // 14. velo_kalman_filter (VeloKalmanFilter.cu:8-18 sizes, :153-268 operator(), :362-399 kernel)
+      const unsigned reco = host_reconstructed;
+      auto* is_backward = r->make<bool>("dev_is_backward", reco);
+      char* beamline_states = r->make<char>("dev_velo_kalman_beamline_states", size_t(reco) * Velo::Consolidated::States::size);
+      char* endvelo_states = r->make<char>("dev_velo_kalman_endvelo_states", size_t(reco) * Velo::Consolidated::States::size);
+      ViewStorage<Allen::Views::Physics::KalmanStates> beam_view(n), end_view(n);
+      float beamline[2] = {in.beamline_x, in.beamline_y};
+      std::vector<unsigned> h_eta(40), h_phi(16), h_nhits(50), f_eta(40), f_phi(16), f_nhits(50), b_eta(40), b_phi(16),
+        b_nhits(50);
+      auto us = [](std::vector<unsigned>& v) { return gsl::span<unsigned> {v.data(), v.size()}; };
+      velo_kalman_filter::Parameters k {};
+      k.host_number_of_reconstructed_velo_tracks = sp<const unsigned>(&reco, 1);
+      k.host_number_of_events = sp<const unsigned>(&host_n, 1);
+      k.dev_event_list = sp<const mask_t>(event_list.data(), n);
+      k.dev_number_of_events = sp<const unsigned>(&dev_n, 1);
+      k.dev_offsets_all_velo_tracks = sp<const unsigned>(offsets_all, n + 1);
+      k.dev_velo_tracks_view = sp<const Allen::Views::Velo::Consolidated::Tracks>(tracks_view.data(), n);
+      k.dev_is_backward = sp<bool>(is_backward, reco);
+      k.dev_velo_kalman_beamline_states = sp<char>(beamline_states, size_t(reco) * Velo::Consolidated::States::size);
+      k.dev_velo_kalman_endvelo_states = sp<char>(endvelo_states, size_t(reco) * Velo::Consolidated::States::size);
+      k.dev_velo_kalman_beamline_states_view = sp(beam_view.data(), n);
+      k.dev_velo_kalman_endvelo_states_view = sp(end_view.data(), n);
+      k.histogram_velo_track_eta_min = -10.f;
+      k.histogram_velo_track_eta_max = 10.f;
+      k.histogram_velo_track_eta_nbins = 40u;
+      k.histogram_velo_track_phi_min = -4.f;
+      k.histogram_velo_track_phi_max = 4.f;
+      k.histogram_velo_track_phi_nbins = 16u;
+      k.histogram_velo_track_nhits_min = 0.f;
+      k.histogram_velo_track_nhits_max = 50.f;
+      k.histogram_velo_track_nhits_nbins = 50u;
+      launch(n, [&] {
+        velo_kalman_filter::velo_kalman_filter(
+          k, beamline, us(h_eta), us(h_phi), us(h_nhits), us(f_eta), us(f_phi), us(f_nhits), us(b_eta), us(b_phi),
+          us(b_nhits));
       });
     }
     return r;

@@ -41,6 +41,9 @@ typedef struct {
   float max_scatter;
   unsigned max_skipped_modules;
   float max_chi2;
+  /* beamline position in x and y (Constants::dev_beamline; beamline.bin holds 0, 0) */
+  float beamline_x;
+  float beamline_y;
 } VeloCpuInput;
 
 #ifdef __cplusplus

@@ -1101,6 +1101,139 @@ static void consolidate_tracks(
  * The chain (velo_reconstruction.py:72-292), buffers sized as each
  * set_arguments_size does.
  * ------------------------------------------------------------------------------ */
+/* --------------------------------------------------------------------------------
+ * velo_kalman_filter (device/velo/simplified_kalman_filter/src/VeloKalmanFilter.cu:271-399,
+ * include/VeloKalmanFilter.cuh:24-158), one track after the other.  Track hits are read from
+ * the consolidated container (VeloConsolidated.cuh:19-88: ids, then x y z interleaved).
+ * States go to Velo::Consolidated::States (VeloConsolidated.cuh:388-598): per track
+ * x y z tx ty qop, then for all tracks c00 c20 c22 c11 c31 c33 chi2 ndof; qop, chi2 and
+ * ndof are not written by the filter.
+ * -------------------------------------------------------------------------------- */
+typedef struct {
+  float x, y, z, tx, ty, c00, c20, c22, c11, c31, c33;
+} KalmanState;
+
+static const float param_w_inverted = 0.00015625f; /* VeloDefinitions.cuh:36 */
+static const float z_end_velo = 770.f;             /* VeloDefinitions.cuh:20 */
+
+/* VeloKalmanFilter.cuh:24-58 */
+static void kalman_step(float z, float zhit, float xhit, float whit, float* x, float* tx, float* cov_xx, float* cov_xtx, float* cov_txtx)
+{
+  const float dz = zhit - z;
+  const float predx = *x + dz * *tx;
+  const float dz_t_covTxTx = dz * *cov_txtx;
+  const float predcovXTx = *cov_xtx + dz_t_covTxTx;
+  const float dx_t_covXTx = dz * *cov_xtx;
+  const float predcovXX = *cov_xx + 2.f * dx_t_covXTx + dz * dz_t_covTxTx;
+  const float predcovTxTx = *cov_txtx;
+  const float R = 1.0f / ((1.0f / whit) + predcovXX);
+  const float Kx = predcovXX * R;
+  const float KTx = predcovXTx * R;
+  const float r = xhit - predx;
+  *x = predx + Kx * r;
+  *tx = *tx + KTx * r;
+  *cov_xx = (1.f - Kx) * predcovXX;
+  *cov_xtx = (1.f - Kx) * predcovXTx;
+  *cov_txtx = predcovTxTx - KTx * predcovXTx;
+}
+
+typedef struct {
+  const float* xyz; /* x y z of the track's first hit, 3 floats per hit */
+  unsigned n;
+} KalmanTrack;
+
+/* VeloKalmanFilter.cuh:63-158 */
+static KalmanState simplified_fit(const KalmanTrack* t, float state_tx, float state_ty, const float beamline[2], int backward, int upstream)
+{
+  const int direction = (backward ? 1 : -1) * (upstream ? 1 : -1);
+  const float noise2PerLayer = 1e-8f + 7e-6f * (state_tx * state_tx + state_ty * state_ty);
+  int firsthit = 0, lasthit = (int) t->n - 1, dhit = 1;
+  if ((t->xyz[3 * lasthit + 2] - t->xyz[3 * firsthit + 2]) * (float) direction < 0) {
+    const int temp = firsthit;
+    firsthit = lasthit;
+    lasthit = temp;
+    dhit = -1;
+  }
+  KalmanState s;
+  s.x = t->xyz[3 * firsthit];
+  s.y = t->xyz[3 * firsthit + 1];
+  s.z = t->xyz[3 * firsthit + 2];
+  s.tx = state_tx;
+  s.ty = state_ty;
+  s.c00 = param_w_inverted;
+  s.c11 = param_w_inverted;
+  s.c20 = 0.f;
+  s.c31 = 0.f;
+  s.c22 = 1.f;
+  s.c33 = 1.f;
+  for (int i = firsthit + dhit; i != lasthit + dhit; i += dhit) {
+    const float hx = t->xyz[3 * i], hy = t->xyz[3 * i + 1], hz = t->xyz[3 * i + 2];
+    s.c22 += noise2PerLayer;
+    s.c33 += noise2PerLayer;
+    kalman_step(s.z, hz, hx, param_w, &s.x, &s.tx, &s.c00, &s.c20, &s.c22);
+    kalman_step(s.z, hz, hy, param_w, &s.y, &s.ty, &s.c11, &s.c31, &s.c33);
+    s.z = hz;
+  }
+  s.c22 += noise2PerLayer;
+  s.c33 += noise2PerLayer;
+  float delta_z;
+  if (upstream)
+    delta_z = (s.tx * (beamline[0] - s.x) + s.ty * (beamline[1] - s.y)) / (s.tx * s.tx + s.ty * s.ty);
+  else
+    delta_z = z_end_velo - s.z;
+  s.x = s.x + s.tx * delta_z;
+  s.y = s.y + s.ty * delta_z;
+  s.z = s.z + delta_z;
+  const float dz2 = delta_z * delta_z;
+  s.c00 += dz2 * s.c22 + 2.f * delta_z * s.c20;
+  s.c11 += dz2 * s.c33 + 2.f * delta_z * s.c31;
+  s.c20 += s.c22 * delta_z;
+  s.c31 += s.c33 * delta_z;
+  return s;
+}
+
+static void store_state(float* base, unsigned total, unsigned i, const KalmanState* s)
+{
+  float* st = base + 6u * i;
+  st[0] = s->x;
+  st[1] = s->y;
+  st[2] = s->z;
+  st[3] = s->tx;
+  st[4] = s->ty;
+  float* cov = base + 6u * total + 8u * i;
+  cov[0] = s->c00;
+  cov[1] = s->c20;
+  cov[2] = s->c22;
+  cov[3] = s->c11;
+  cov[4] = s->c31;
+  cov[5] = s->c33;
+}
+
+/* velo_kalman_filter kernel (VeloKalmanFilter.cu:362-399) with linear_fit (:333-353) */
+static void kalman_filter(
+  unsigned n_events, const unsigned* offsets_all, const unsigned* offsets_hit_number, const char* track_hits,
+  const float beamline[2], uint8_t* is_backward, float* beamline_states, float* endvelo_states)
+{
+  const unsigned total_tracks = offsets_all[n_events];
+  const unsigned total_hits = offsets_hit_number[total_tracks];
+  const float* coords = (const float*) track_hits + total_hits;
+  for (unsigned i = 0; i < total_tracks; ++i) {
+    KalmanTrack t = {coords + 3u * offsets_hit_number[i], offsets_hit_number[i + 1] - offsets_hit_number[i]};
+    const float* first = t.xyz;
+    const float* last = t.xyz + 3u * (t.n - 1);
+    const float tx = (last[0] - first[0]) / (last[2] - first[2]);
+    const float ty = (last[1] - first[1]) / (last[2] - first[2]);
+    const float delta_z = (tx * (beamline[0] - last[0]) + ty * (beamline[1] - last[1])) / (tx * tx + ty * ty);
+    const float lin_z = last[2] + delta_z;
+    const int backward = lin_z > first[2];
+    is_backward[i] = (uint8_t) backward;
+    const KalmanState b = simplified_fit(&t, tx, ty, beamline, backward, 1);
+    const KalmanState e = simplified_fit(&t, b.tx, b.ty, beamline, backward, 0);
+    store_state(beamline_states, total_tracks, i, &b);
+    store_state(endvelo_states, total_tracks, i, &e);
+  }
+}
+
 void* velo_oracle_run(const VeloCpuInput* in)
 {
   Result* r = calloc(1, sizeof(Result));
@@ -1182,6 +1315,14 @@ void* velo_oracle_run(const VeloCpuInput* in)
   char* track_hits = make(r, "dev_velo_track_hits", (size_t) total_track_hits * ELEMENT_SIZE);
   consolidate_tracks(
     n, offsets_est, offsets_all, tracks, offsets_hit_number, sorted, three_out, offsets_three, track_hits);
+
+  /* velo_kalman_filter (VeloKalmanFilter.cu:8-18 sizes) */
+  const unsigned reco = offsets_all[n];
+  const float beamline[2] = {in->beamline_x, in->beamline_y};
+  uint8_t* is_backward = make(r, "dev_is_backward", reco);
+  float* beamline_states = make(r, "dev_velo_kalman_beamline_states", (size_t) reco * 56u);
+  float* endvelo_states = make(r, "dev_velo_kalman_endvelo_states", (size_t) reco * 56u);
+  kalman_filter(n, offsets_all, offsets_hit_number, track_hits, beamline, is_backward, beamline_states, endvelo_states);
   free(g);
   return r;
 }

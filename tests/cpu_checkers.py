@@ -31,6 +31,9 @@ DTYPES = {
     "dev_hit_used": np.uint8,
     "dev_rel_indices": np.uint16,
     "dev_accepted_velo_tracks": np.uint8,
+    "dev_is_backward": np.uint8,
+    "dev_velo_kalman_beamline_states": np.uint8,
+    "dev_velo_kalman_endvelo_states": np.uint8,
 }
 
 
@@ -41,6 +44,7 @@ class VeloCpuInput(C.Structure):
         ("bank_version", C.c_int), ("geometry", C.c_void_p), ("geometry_size", C.c_size_t),
         ("phi_tolerance", C.c_float), ("max_scatter", C.c_float),
         ("max_skipped_modules", C.c_uint), ("max_chi2", C.c_float),
+        ("beamline_x", C.c_float), ("beamline_y", C.c_float),
     ]
 
 
@@ -69,7 +73,7 @@ class Checker:
 
     @staticmethod
     def make_input(s, geometry: bytes, event_start=0, n_events=None, phi_tolerance=0.045,
-                   max_scatter=0.08, max_skipped_modules=1, max_chi2=20.0):
+                   max_scatter=0.08, max_skipped_modules=1, max_chi2=20.0, beamline=(0.0, 0.0)):
         keep = (np.ascontiguousarray(s.raw), np.ascontiguousarray(s.offsets),
                 np.ascontiguousarray(s.sizes), np.ascontiguousarray(s.types),
                 np.frombuffer(geometry, dtype=np.uint8))
@@ -77,7 +81,7 @@ class Checker:
             keep[0].ctypes.data, keep[1].ctypes.data, keep[2].ctypes.data, keep[3].ctypes.data,
             event_start, s.n_events - event_start if n_events is None else n_events,
             s.bank_version, keep[4].ctypes.data, len(geometry),
-            phi_tolerance, max_scatter, max_skipped_modules, max_chi2)
+            phi_tolerance, max_scatter, max_skipped_modules, max_chi2, beamline[0], beamline[1])
         return inp, keep
 
     def run(self, s, geometry: bytes, **kw) -> dict:

@@ -129,3 +129,11 @@ def same_clusters_and_tracks(a: dict, b: dict) -> bool:
     return all(np.array_equal(_u8(x[mask]), _u8(y[mask]))
                for x, y in zip(container_fields(a["dev_sorted_velo_cluster_container"], T),
                                container_fields(b["dev_sorted_velo_cluster_container"], T)))
+
+
+def kalman_written_words(reco: int) -> np.ndarray:
+    """Word indices of Velo::Consolidated::States that velo_kalman_filter writes: x y z tx ty
+    of each track (qop not), and c00 c20 c22 c11 c31 c33 (chi2, ndof not)."""
+    st = np.arange(6 * reco).reshape(reco, 6)[:, :5].ravel()
+    cov = (6 * reco + np.arange(8 * reco).reshape(reco, 8)[:, :6]).ravel()
+    return np.concatenate([st, cov])

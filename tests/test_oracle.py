@@ -67,3 +67,20 @@ def test_sp_order_invariance(oracle, geometry, version):
     runs = [oracle.run(generator.generate(8, seed=12, bank_version=version, sp_order=o).raw, geometry)
             for o in (0, 1)]
     assert parity.same_clusters_and_tracks(runs[0], runs[1])
+
+
+@pytest.mark.parametrize("beamline", [(0.0, 0.0), (0.35, -0.2)])
+def test_kalman_filter_matches_reference_build(oracle, geometry, beamline):
+    """velo_kalman_filter of the C restatement against the reference's own kernel compiled as
+    CPU C++: dev_is_backward and the written fields of both state containers, bit for bit."""
+    if not cpu_checkers.available("ref"):
+        pytest.skip("oracle/_ref not built")
+    ref = cpu_checkers.load("ref")
+    g = generator.generate(25, seed=17, pileup_min=1.0, pileup_max=15.0)
+    a = oracle.run(g.raw, geometry, beamline=beamline)
+    b = ref.run(g.raw, geometry, beamline=beamline)
+    reco = int(a["dev_offsets_all_velo_tracks"][-1])
+    assert np.array_equal(a["dev_is_backward"], b["dev_is_backward"])
+    written = parity.kalman_written_words(reco)
+    for k in ("dev_velo_kalman_beamline_states", "dev_velo_kalman_endvelo_states"):
+        assert np.array_equal(a[k].view(np.uint32)[written], b[k].view(np.uint32)[written]), k
