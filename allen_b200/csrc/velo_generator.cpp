@@ -36,6 +36,7 @@
 #include <cstring>
 #include <memory>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/velo_generator.h"
@@ -302,6 +303,58 @@ namespace {
       }
     }
 
+    // Retina clusters (raw_format 1): the pixels of each sensor grouped by 8-connectivity,
+    // centroid column and row with a 3-bit (version 2) or 2-bit (versions 3, 4) fraction,
+    // in the VPRetinaCluster word layout DecodeRetinaClusters.cu:116-140 reads.
+    if (cfg.raw_format == 1) {
+      const bool v2 = cfg.bank_version == 2;
+      const double q = v2 ? 8.0 : 4.0;
+      for (auto& w : sensor_words)
+        w.clear();
+      size_t i = 0;
+      std::unordered_map<uint32_t, unsigned> where;
+      std::vector<unsigned> stack;
+      while (i < pixels.size()) {
+        const unsigned s = pixels[i].sensor;
+        size_t j = i;
+        where.clear();
+        for (; j < pixels.size() && pixels[j].sensor == s; ++j)
+          where[(pixels[j].col << 8) | pixels[j].row] = unsigned(j);
+        std::vector<char> seen(j - i, 0);
+        for (size_t k = i; k < j; ++k) {
+          if (seen[k - i]) continue;
+          double sc = 0, sr = 0;
+          unsigned n = 0;
+          stack.assign(1, unsigned(k));
+          seen[k - i] = 1;
+          while (!stack.empty()) {
+            const unsigned m = stack.back();
+            stack.pop_back();
+            sc += pixels[m].col;
+            sr += pixels[m].row;
+            ++n;
+            for (int dc = -1; dc <= 1; ++dc)
+              for (int dr = -1; dr <= 1; ++dr) {
+                const int c = int(pixels[m].col) + dc, r = int(pixels[m].row) + dr;
+                if ((!dc && !dr) || c < 0 || r < 0 || c >= int(n_cols) || r >= int(n_rows)) continue;
+                const auto it = where.find((uint32_t(c) << 8) | uint32_t(r));
+                if (it != where.end() && !seen[it->second - i]) {
+                  seen[it->second - i] = 1;
+                  stack.push_back(it->second);
+                }
+              }
+          }
+          const double mc = sc / n, mr = sr / n;
+          const uint32_t cx = uint32_t(mc), cy = uint32_t(mr);
+          const uint32_t fx = std::min(uint32_t((mc - cx) * q), uint32_t(q) - 1);
+          const uint32_t fy = std::min(uint32_t((mr - cy) * q), uint32_t(q) - 1);
+          const uint32_t word = v2 ? ((cx << 14) | (fx << 11) | (cy << 3) | fy) : ((cx << 12) | (fx << 10) | (cy << 2) | fy);
+          sensor_words[s].push_back(word);
+        }
+        i = j;
+      }
+    }
+
     // Allen event blob
     const bool v4 = cfg.bank_version == 4;
     const unsigned n_banks = v4 ? n_sensors / 2 : n_sensors;
@@ -311,7 +364,7 @@ namespace {
       if (v4) {
         for (unsigned half = 0; half < 2; ++half)
           for (uint32_t w : sensor_words[2 * b + half])
-            d.push_back(w | (half ? 0x800000u : 0u));
+            d.push_back(w | (half ? (cfg.raw_format == 1 ? 0x400000u : 0x800000u) : 0u));
       }
       else {
         d.push_back(uint32_t(sensor_words[b].size()));
@@ -337,7 +390,7 @@ namespace {
       out.words.push_back(b); // sourceID: sensor (v2/v3) or sensor pair (v4)
       out.words.insert(out.words.end(), banks[b].begin(), banks[b].end());
       out.bank_sizes.push_back(uint16_t(4 * banks[b].size()));
-      out.bank_types.push_back(63); // LHCb::RawBank::VP
+      out.bank_types.push_back(cfg.raw_format == 1 ? 73 : 63); // LHCb::RawBank::VPRetinaCluster or VP
     }
   }
 
@@ -369,6 +422,7 @@ void velo_gen_default_config(VeloGenConfig* cfg)
   cfg->drop_corner_fraction = 0.3;
   cfg->bank_version = 2;
   cfg->sp_order = 1;
+  cfg->raw_format = 0;
 }
 
 void* velo_gen_create(

@@ -18,6 +18,7 @@ class VeloGenConfig(C.Structure):
         ("hit_efficiency", C.c_double), ("scatter_sigma", C.c_double),
         ("noise_rate", C.c_double), ("share_fraction", C.c_double),
         ("drop_corner_fraction", C.c_double), ("bank_version", C.c_int), ("sp_order", C.c_int),
+        ("raw_format", C.c_int),
     ]
 
 

@@ -21,6 +21,7 @@ import numpy as np
 
 BANK_TYPE_VELO = 8
 BANK_TYPE_VP = 63
+BANK_TYPE_VP_RETINA = 73  # LHCb::RawBank::VPRetinaCluster
 
 
 @dataclass
@@ -34,6 +35,15 @@ class RawSlice:
     @property
     def n_events(self) -> int:
         return int(self.offsets.shape[0] - 1)
+
+    @property
+    def retina(self) -> bool:
+        """The slice carries retina-cluster banks (type 73) rather than super-pixel banks."""
+        if self.n_events == 0:
+            return False
+        t8 = self.types.view(np.uint8)
+        first, last = int(self.types[0]), int(self.types[1]) if self.n_events > 1 else t8.size
+        return bool(np.any(t8[first:first + max(last - first, 0)] == BANK_TYPE_VP_RETINA))
 
     def n_super_pixels(self) -> int:
         """Total super pixels of the slice, from the bank sizes alone (no payload read)."""
@@ -97,8 +107,9 @@ def banks_of_event(s: RawSlice, event: int):
 
 
 def super_pixels_per_event(s: RawSlice) -> np.ndarray:
-    """Super pixels per event from the bank sizes: (size - 4) / 4 for v2/v3 (count word
-    first), size / 4 for v4.  Upper bound used to size device buffers before launch."""
+    """Super pixels (or retina clusters) per event from the bank sizes: (size - 4) / 4 for
+    v2/v3 (count word first), size / 4 for v4.  Upper bound used to size device buffers
+    before launch."""
     n = s.n_events
     s16 = s.sizes.view(np.uint16)
     t8 = s.types.view(np.uint8)
@@ -108,7 +119,7 @@ def super_pixels_per_event(s: RawSlice) -> np.ndarray:
     for e in range(n):
         sz = s16[starts[e]:starts[e + 1]].astype(np.int64)
         ty = t8[tstarts[e]:tstarts[e] + sz.size]
-        sel = (ty == BANK_TYPE_VP) | (ty == BANK_TYPE_VELO)
+        sel = (ty == BANK_TYPE_VP) | (ty == BANK_TYPE_VELO) | (ty == BANK_TYPE_VP_RETINA)
         words = sz[sel] // 4
         if s.bank_version in (2, 3):
             words = np.maximum(words - 1, 0)

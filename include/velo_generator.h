@@ -31,6 +31,7 @@ typedef struct {
   double drop_corner_fraction; /* 2x2 clusters that lose their far corner (0.3) */
   int bank_version;            /* 2 (one bank per sensor), 3, or 4 (one per sensor pair) */
   int sp_order;                /* SP order inside a bank: 0 column order, 1 shuffled as read out (1) */
+  int raw_format;              /* 0 super-pixel banks (type 63), 1 retina-cluster banks (type 73) (0) */
 } VeloGenConfig;
 
 typedef struct {

@@ -30,6 +30,8 @@
 #include "VeloCopyTrackHitNumber.cuh"
 #include "VeloConsolidateTracks.cuh"
 #include "VeloKalmanFilter.cuh"
+#include "CalculateNumberOfRetinaClustersPerSensor.cuh"
+#include "DecodeRetinaClusters.cuh"
 #include "HostPrefixSum.h"
 #include "ClusteringCommon.h"
 
@@ -51,6 +53,30 @@ __global__ void velo_masked_clustering_kernel(
   const uint8_t* dev_velo_sp_patterns,
   const float* dev_velo_sp_fx,
   const float* dev_velo_sp_fy);
+
+template<int decoding_version, bool mep_layout>
+__global__ void calculate_number_of_retinaclusters_each_sensor_pair_kernel(
+  calculate_number_of_retinaclusters_each_sensor_pair::Parameters parameters,
+  const unsigned event_start);
+template<int decoding_version>
+__global__ void populate_module_pair_offsets_and_sizes(
+  decode_retinaclusters::Parameters parameters,
+  const unsigned module_pair_cluster_num_size);
+template<int decoding_version, bool mep_layout>
+__global__ void velo_calculate_sorting_key(
+  decode_retinaclusters::Parameters parameters,
+  const unsigned event_start,
+  const VeloGeometry* dev_velo_geometry,
+  unsigned* dev_module_pair_zero_cluster_num);
+template<bool mep_layout>
+__global__ void velo_calculate_permutations(
+  decode_retinaclusters::Parameters parameters,
+  unsigned* dev_module_pair_zero_cluster_num);
+template<int decoding_version, bool mep_layout>
+__global__ void decode_retinaclusters_sorted(
+  decode_retinaclusters::Parameters parameters,
+  const unsigned event_start,
+  const VeloGeometry* dev_velo_geometry);
 
 // VeloConsolidateTracks.cu:11-46 (defined at file scope there)
 __global__ void create_velo_views(velo_consolidate_tracks::Parameters parameters);
@@ -142,103 +168,165 @@ namespace {
     cache_sp_patterns(sp_patterns, sp_sizes, sp_fx, sp_fy);
     const VeloGeometry geometry {std::vector<char>(in.geometry, in.geometry + in.geometry_size)};
 
-    // 1. velo_calculate_number_of_candidates (VeloCalculateNumberOfCandidates.cu:50-86)
-    unsigned* n_candidates = r->make<unsigned>("dev_number_of_candidates", n);
-    unsigned* bank_index = r->make<unsigned>("dev_velo_bank_index", Velo::Constants::n_modules * 4);
-    {
-      velo_calculate_number_of_candidates::Parameters p {};
-      p.host_number_of_events = sp<const unsigned>(&host_n, 1);
-      p.host_raw_bank_version = sp<const int>(&bank_version, 1);
-      p.dev_event_list = sp<const mask_t>(event_list.data(), n);
-      p.dev_velo_raw_input = sp<const char>(in.raw, big);
-      p.dev_velo_raw_input_offsets = sp<const unsigned>(in.raw_offsets, big);
-      p.dev_velo_raw_input_sizes = sp<const unsigned>(in.raw_sizes, big);
-      p.dev_velo_raw_input_types = sp<const unsigned>(in.raw_types, big);
-      p.dev_number_of_candidates = sp<unsigned>(n_candidates, n);
-      p.dev_velo_bank_index = sp<unsigned>(bank_index, Velo::Constants::n_modules * 4);
-      if (bank_version >= 0) {
-        launch((n + 255) / 256, [&] { velo_calculate_number_of_candidates_kernel<V, false>(p, n, start); });
-      }
-    }
-
-    // 2. prefix_sum_offsets_velo_candidates
-    const unsigned total_candidates = prefix_sum(*r, "dev_candidates_offsets", n_candidates, n);
-    const unsigned* candidates_offsets = static_cast<unsigned*>(r->buffers["dev_candidates_offsets"].p);
-
-    // 3. velo_estimate_input_size (EstimateInputSize.cu:241-281)
-    unsigned* estimated = r->make<unsigned>("dev_estimated_input_size", size_t(n) * 26);
-    unsigned* candidate_num = r->make<unsigned>("dev_module_candidate_num", n);
-    unsigned* candidates = r->make<unsigned>("dev_cluster_candidates", total_candidates);
-    {
-      velo_estimate_input_size::Parameters p {};
-      p.host_number_of_events = sp<const unsigned>(&host_n, 1);
-      p.host_number_of_cluster_candidates = sp<const unsigned>(&total_candidates, 1);
-      p.host_raw_bank_version = sp<const int>(&bank_version, 1);
-      p.dev_event_list = sp<const mask_t>(event_list.data(), n);
-      p.dev_candidates_offsets = sp<const unsigned>(candidates_offsets, n + 1);
-      p.dev_velo_raw_input = sp<const char>(in.raw, big);
-      p.dev_velo_raw_input_offsets = sp<const unsigned>(in.raw_offsets, big);
-      p.dev_velo_raw_input_sizes = sp<const unsigned>(in.raw_sizes, big);
-      p.dev_velo_raw_input_types = sp<const unsigned>(in.raw_types, big);
-      p.dev_estimated_input_size = sp<unsigned>(estimated, size_t(n) * 26);
-      p.dev_module_candidate_num = sp<unsigned>(candidate_num, n);
-      p.dev_cluster_candidates = sp<unsigned>(candidates, total_candidates);
-      if (bank_version >= 0) {
-        launch(n, [&] { velo_estimate_input_size_kernel<V, false>(p, start); });
-      }
-    }
-
-    // 4. prefix_sum_offsets_estimated_input_size
-    const unsigned total_clusters = prefix_sum(*r, "dev_offsets_estimated_input_size", estimated, size_t(n) * 26);
-    const unsigned* offsets_est = static_cast<unsigned*>(r->buffers["dev_offsets_estimated_input_size"].p);
-
-    // 5. velo_masked_clustering (MaskedVeloClustering.cu:578-619)
-    unsigned* cluster_num = r->make<unsigned>("dev_module_cluster_num", size_t(n) * 26);
-    char* container = r->make<char>("dev_velo_cluster_container", size_t(total_clusters) * Velo::Clusters::element_size);
+    unsigned total_clusters = 0;
+    const unsigned* offsets_est = nullptr;
+    unsigned* cluster_num = nullptr;
+    char* sorted = nullptr;
     std::vector<Velo::Clusters> clusters_views(n);
-    {
-      velo_masked_clustering::Parameters p {};
+    // VPRetinaCluster banks (velo_reconstruction.py:18-71): each_sensor_pair_size, its prefix
+    // sum and decode_retinaclusters (DecodeRetinaClusters.cu:433-504) give the same three
+    // inputs of the search: offsets per module pair, cluster counts, sorted container.
+    if (in.retina_decoding) {
+      const unsigned per_event = (V == 2 || V == 3) ? Velo::Constants::n_modules * 4 : Velo::Constants::n_modules * 2;
+      unsigned* pair_size = r->make<unsigned>("dev_each_sensor_pair_size", size_t(n) * per_event);
+      unsigned* retina_bank_index = r->make<unsigned>("dev_retina_bank_index", per_event);
+      {
+        calculate_number_of_retinaclusters_each_sensor_pair::Parameters p {};
+        p.host_number_of_events = sp<const unsigned>(&host_n, 1);
+        p.host_raw_bank_version = sp<const int>(&bank_version, 1);
+        p.dev_event_list = sp<const mask_t>(event_list.data(), n);
+        p.dev_velo_retina_raw_input = sp<const char>(in.raw, big);
+        p.dev_velo_retina_raw_input_offsets = sp<const unsigned>(in.raw_offsets, big);
+        p.dev_velo_retina_raw_input_sizes = sp<const unsigned>(in.raw_sizes, big);
+        p.dev_velo_retina_raw_input_types = sp<const unsigned>(in.raw_types, big);
+        p.dev_retina_bank_index = sp<unsigned>(retina_bank_index, per_event);
+        p.dev_each_sensor_pair_size = sp<unsigned>(pair_size, size_t(n) * per_event);
+        if (bank_version >= 0) launch(n, [&] { calculate_number_of_retinaclusters_each_sensor_pair_kernel<V, false>(p, start); });
+      }
+      total_clusters = prefix_sum(*r, "dev_offsets_each_sensor_pair_size", pair_size, size_t(n) * per_event);
+      const unsigned* pair_offsets = static_cast<unsigned*>(r->buffers["dev_offsets_each_sensor_pair_size"].p);
+      cluster_num = r->make<unsigned>("dev_module_cluster_num", size_t(n) * 26);
+      unsigned* offsets_mp = r->make<unsigned>("dev_offsets_estimated_input_size", size_t(n) * 26 + 1);
+      sorted = r->make<char>("dev_sorted_velo_cluster_container", size_t(total_clusters) * Velo::Clusters::element_size);
+      unsigned* permutations = r->make<unsigned>("dev_hit_permutations", total_clusters);
+      int64_t* keys = r->make<int64_t>("dev_hit_sorting_key", total_clusters);
+      std::vector<unsigned> zero_num(size_t(n) * 26, 0);
+      decode_retinaclusters::Parameters p {};
       p.host_total_number_of_velo_clusters = sp<const unsigned>(&total_clusters, 1);
-      p.host_number_of_events = sp<const unsigned>(&host_n, 1);
       p.host_raw_bank_version = sp<const int>(&bank_version, 1);
-      p.dev_velo_raw_input = sp<const char>(in.raw, big);
-      p.dev_velo_raw_input_offsets = sp<const unsigned>(in.raw_offsets, big);
-      p.dev_velo_raw_input_sizes = sp<const unsigned>(in.raw_sizes, big);
-      p.dev_velo_raw_input_types = sp<const unsigned>(in.raw_types, big);
-      p.dev_offsets_estimated_input_size = sp<const unsigned>(offsets_est, size_t(n) * 26 + 1);
-      p.dev_module_pair_candidate_num = sp<const unsigned>(candidate_num, n);
-      p.dev_cluster_candidates = sp<const unsigned>(candidates, total_candidates);
+      p.host_number_of_events = sp<const unsigned>(&host_n, 1);
+      p.dev_velo_retina_raw_input = sp<const char>(in.raw, big);
+      p.dev_velo_retina_raw_input_offsets = sp<const unsigned>(in.raw_offsets, big);
+      p.dev_velo_retina_raw_input_sizes = sp<const unsigned>(in.raw_sizes, big);
+      p.dev_velo_retina_raw_input_types = sp<const unsigned>(in.raw_types, big);
+      p.dev_offsets_each_sensor_pair_size = sp<const unsigned>(pair_offsets, size_t(n) * per_event + 1);
+      p.dev_retina_bank_index = sp<const unsigned>(retina_bank_index, per_event);
       p.dev_event_list = sp<const mask_t>(event_list.data(), n);
-      p.dev_candidates_offsets = sp<const unsigned>(candidates_offsets, n + 1);
       p.dev_number_of_events = sp<const unsigned>(&dev_n, 1);
-      p.dev_velo_bank_index = sp<const unsigned>(bank_index, Velo::Constants::n_modules * 4);
       p.dev_module_pair_cluster_num = sp<unsigned>(cluster_num, size_t(n) * 26);
-      p.dev_velo_cluster_container = sp<char>(container, size_t(total_clusters) * Velo::Clusters::element_size);
+      p.dev_offsets_module_pair_cluster = sp<unsigned>(offsets_mp, size_t(n) * 26 + 1);
+      p.dev_velo_cluster_container = sp<char>(sorted, size_t(total_clusters) * Velo::Clusters::element_size);
+      p.dev_hit_permutations = sp<unsigned>(permutations, total_clusters);
+      p.dev_hit_sorting_key = sp<int64_t>(keys, total_clusters);
       p.dev_velo_clusters = sp<Velo::Clusters>(clusters_views.data(), n);
       if (bank_version >= 0) {
-        launch(n, [&] {
-          velo_masked_clustering_kernel<V, false>(
-            p, start, &geometry, sp_patterns.data(), sp_fx.data(), sp_fy.data());
-        });
+        const unsigned size = n * 26;
+        const unsigned block = Velo::Tracking::block_dim_x_populate_module_pair_offsets_and_sizes;
+        launch((size + block - 1) / block, [&] { populate_module_pair_offsets_and_sizes<V>(p, size); });
+        launch(n, [&] { velo_calculate_sorting_key<V, false>(p, start, &geometry, zero_num.data()); });
+        launch(n, [&] { velo_calculate_permutations<false>(p, zero_num.data()); });
+        launch(n, [&] { decode_retinaclusters_sorted<V, false>(p, start, &geometry); });
       }
+      offsets_est = offsets_mp;
     }
+    else {
+      // 1. velo_calculate_number_of_candidates (VeloCalculateNumberOfCandidates.cu:50-86)
+      unsigned* n_candidates = r->make<unsigned>("dev_number_of_candidates", n);
+      unsigned* bank_index = r->make<unsigned>("dev_velo_bank_index", Velo::Constants::n_modules * 4);
+      {
+        velo_calculate_number_of_candidates::Parameters p {};
+        p.host_number_of_events = sp<const unsigned>(&host_n, 1);
+        p.host_raw_bank_version = sp<const int>(&bank_version, 1);
+        p.dev_event_list = sp<const mask_t>(event_list.data(), n);
+        p.dev_velo_raw_input = sp<const char>(in.raw, big);
+        p.dev_velo_raw_input_offsets = sp<const unsigned>(in.raw_offsets, big);
+        p.dev_velo_raw_input_sizes = sp<const unsigned>(in.raw_sizes, big);
+        p.dev_velo_raw_input_types = sp<const unsigned>(in.raw_types, big);
+        p.dev_number_of_candidates = sp<unsigned>(n_candidates, n);
+        p.dev_velo_bank_index = sp<unsigned>(bank_index, Velo::Constants::n_modules * 4);
+        if (bank_version >= 0) {
+          launch((n + 255) / 256, [&] { velo_calculate_number_of_candidates_kernel<V, false>(p, n, start); });
+        }
+      }
 
-    // 6. velo_sort_by_phi (SortByPhi.cu:15-44)
-    char* sorted = r->make<char>("dev_sorted_velo_cluster_container", size_t(total_clusters) * Velo::Clusters::element_size);
-    unsigned* permutation = r->make<unsigned>("dev_hit_permutation", total_clusters);
-    {
-      velo_sort_by_phi::Parameters p {};
-      p.host_number_of_events = sp<const unsigned>(&host_n, 1);
-      p.host_total_number_of_velo_clusters = sp<const unsigned>(&total_clusters, 1);
-      p.dev_event_list = sp<const mask_t>(event_list.data(), n);
-      p.dev_offsets_estimated_input_size = sp<const unsigned>(offsets_est, size_t(n) * 26 + 1);
-      p.dev_module_cluster_num = sp<const unsigned>(cluster_num, size_t(n) * 26);
-      p.dev_velo_cluster_container = sp<const char>(container, size_t(total_clusters) * Velo::Clusters::element_size);
-      p.dev_number_of_events = sp<const unsigned>(&dev_n, 1);
-      p.dev_sorted_velo_cluster_container = sp<char>(sorted, size_t(total_clusters) * Velo::Clusters::element_size);
-      p.dev_hit_permutation = sp<unsigned>(permutation, total_clusters);
-      p.dev_velo_clusters = sp<const Velo::Clusters>(clusters_views.data(), n);
-      launch(n, [&] { velo_sort_by_phi::velo_sort_by_phi(p); });
+      // 2. prefix_sum_offsets_velo_candidates
+      const unsigned total_candidates = prefix_sum(*r, "dev_candidates_offsets", n_candidates, n);
+      const unsigned* candidates_offsets = static_cast<unsigned*>(r->buffers["dev_candidates_offsets"].p);
+
+      // 3. velo_estimate_input_size (EstimateInputSize.cu:241-281)
+      unsigned* estimated = r->make<unsigned>("dev_estimated_input_size", size_t(n) * 26);
+      unsigned* candidate_num = r->make<unsigned>("dev_module_candidate_num", n);
+      unsigned* candidates = r->make<unsigned>("dev_cluster_candidates", total_candidates);
+      {
+        velo_estimate_input_size::Parameters p {};
+        p.host_number_of_events = sp<const unsigned>(&host_n, 1);
+        p.host_number_of_cluster_candidates = sp<const unsigned>(&total_candidates, 1);
+        p.host_raw_bank_version = sp<const int>(&bank_version, 1);
+        p.dev_event_list = sp<const mask_t>(event_list.data(), n);
+        p.dev_candidates_offsets = sp<const unsigned>(candidates_offsets, n + 1);
+        p.dev_velo_raw_input = sp<const char>(in.raw, big);
+        p.dev_velo_raw_input_offsets = sp<const unsigned>(in.raw_offsets, big);
+        p.dev_velo_raw_input_sizes = sp<const unsigned>(in.raw_sizes, big);
+        p.dev_velo_raw_input_types = sp<const unsigned>(in.raw_types, big);
+        p.dev_estimated_input_size = sp<unsigned>(estimated, size_t(n) * 26);
+        p.dev_module_candidate_num = sp<unsigned>(candidate_num, n);
+        p.dev_cluster_candidates = sp<unsigned>(candidates, total_candidates);
+        if (bank_version >= 0) {
+          launch(n, [&] { velo_estimate_input_size_kernel<V, false>(p, start); });
+        }
+      }
+
+      // 4. prefix_sum_offsets_estimated_input_size
+      total_clusters = prefix_sum(*r, "dev_offsets_estimated_input_size", estimated, size_t(n) * 26);
+      offsets_est = static_cast<unsigned*>(r->buffers["dev_offsets_estimated_input_size"].p);
+
+      // 5. velo_masked_clustering (MaskedVeloClustering.cu:578-619)
+      cluster_num = r->make<unsigned>("dev_module_cluster_num", size_t(n) * 26);
+      char* container = r->make<char>("dev_velo_cluster_container", size_t(total_clusters) * Velo::Clusters::element_size);
+      {
+        velo_masked_clustering::Parameters p {};
+        p.host_total_number_of_velo_clusters = sp<const unsigned>(&total_clusters, 1);
+        p.host_number_of_events = sp<const unsigned>(&host_n, 1);
+        p.host_raw_bank_version = sp<const int>(&bank_version, 1);
+        p.dev_velo_raw_input = sp<const char>(in.raw, big);
+        p.dev_velo_raw_input_offsets = sp<const unsigned>(in.raw_offsets, big);
+        p.dev_velo_raw_input_sizes = sp<const unsigned>(in.raw_sizes, big);
+        p.dev_velo_raw_input_types = sp<const unsigned>(in.raw_types, big);
+        p.dev_offsets_estimated_input_size = sp<const unsigned>(offsets_est, size_t(n) * 26 + 1);
+        p.dev_module_pair_candidate_num = sp<const unsigned>(candidate_num, n);
+        p.dev_cluster_candidates = sp<const unsigned>(candidates, total_candidates);
+        p.dev_event_list = sp<const mask_t>(event_list.data(), n);
+        p.dev_candidates_offsets = sp<const unsigned>(candidates_offsets, n + 1);
+        p.dev_number_of_events = sp<const unsigned>(&dev_n, 1);
+        p.dev_velo_bank_index = sp<const unsigned>(bank_index, Velo::Constants::n_modules * 4);
+        p.dev_module_pair_cluster_num = sp<unsigned>(cluster_num, size_t(n) * 26);
+        p.dev_velo_cluster_container = sp<char>(container, size_t(total_clusters) * Velo::Clusters::element_size);
+        p.dev_velo_clusters = sp<Velo::Clusters>(clusters_views.data(), n);
+        if (bank_version >= 0) {
+          launch(n, [&] {
+            velo_masked_clustering_kernel<V, false>(
+              p, start, &geometry, sp_patterns.data(), sp_fx.data(), sp_fy.data());
+          });
+        }
+      }
+
+      // 6. velo_sort_by_phi (SortByPhi.cu:15-44)
+      sorted = r->make<char>("dev_sorted_velo_cluster_container", size_t(total_clusters) * Velo::Clusters::element_size);
+      unsigned* permutation = r->make<unsigned>("dev_hit_permutation", total_clusters);
+      {
+        velo_sort_by_phi::Parameters p {};
+        p.host_number_of_events = sp<const unsigned>(&host_n, 1);
+        p.host_total_number_of_velo_clusters = sp<const unsigned>(&total_clusters, 1);
+        p.dev_event_list = sp<const mask_t>(event_list.data(), n);
+        p.dev_offsets_estimated_input_size = sp<const unsigned>(offsets_est, size_t(n) * 26 + 1);
+        p.dev_module_cluster_num = sp<const unsigned>(cluster_num, size_t(n) * 26);
+        p.dev_velo_cluster_container = sp<const char>(container, size_t(total_clusters) * Velo::Clusters::element_size);
+        p.dev_number_of_events = sp<const unsigned>(&dev_n, 1);
+        p.dev_sorted_velo_cluster_container = sp<char>(sorted, size_t(total_clusters) * Velo::Clusters::element_size);
+        p.dev_hit_permutation = sp<unsigned>(permutation, total_clusters);
+        p.dev_velo_clusters = sp<const Velo::Clusters>(clusters_views.data(), n);
+        launch(n, [&] { velo_sort_by_phi::velo_sort_by_phi(p); });
+      }
     }
 
     // 7. velo_search_by_triplet (SearchByTriplet.cu:18-63)

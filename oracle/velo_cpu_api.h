@@ -44,6 +44,9 @@ typedef struct {
   /* beamline position in x and y (Constants::dev_beamline; beamline.bin holds 0, 0) */
   float beamline_x;
   float beamline_y;
+  /* 0: super-pixel banks (VP, type 63) through velo_masked_clustering; 1: retina-cluster
+   * banks (VPRetinaCluster, type 73) through decode_retinaclusters (velo_reconstruction.py:18-71) */
+  int retina_decoding;
 } VeloCpuInput;
 
 #ifdef __cplusplus

@@ -1102,6 +1102,152 @@ static void consolidate_tracks(
  * set_arguments_size does.
  * ------------------------------------------------------------------------------ */
 /* --------------------------------------------------------------------------------
+ * Retina-cluster decoding (VPRetinaCluster banks, type 73):
+ * calculate_number_of_retinaclusters_each_sensor_pair (CalculateNumberOfRetinaClustersPerSensor.cu:12-48),
+ * its prefix sum, and decode_retinaclusters (DecodeRetinaClusters.cu:11-383).
+ * -------------------------------------------------------------------------------- */
+static unsigned retina_sensors_per_event(int version) { return (version == 2 || version == 3) ? N_SENSORS : N_SENSORS / 2; }
+
+/* CalculateNumberOfRetinaClustersPerSensor.cu:12-48; bank index written by the slice's first event */
+static void retina_count(const VeloCpuInput* in, unsigned* pair_size, unsigned* bank_index)
+{
+  const int v = in->bank_version;
+  const unsigned per_event = retina_sensors_per_event(v);
+  for (unsigned e = 0; e < in->n_events; ++e) {
+    const RawEvent ev = raw_event(in, in->event_start + e);
+    unsigned* size = pair_size + (size_t) e * per_event;
+    for (unsigned b = 0; b < ev.n_banks; ++b) {
+      const RawBank bank = raw_bank(&ev, b, v);
+      if (bank.type == 73) {
+        if (v == 2 || v == 3) size[bank.source_id] = bank.count;
+        else size[sensor_pair(&bank)] = bank.size / 4u;
+      }
+      if (e == 0) bank_index[sensor_pair(&bank)] = b;
+    }
+  }
+}
+
+/* BinarySearch.cuh:33-47 */
+static int binary_search_rightmost(const unsigned* a, unsigned n, unsigned value)
+{
+  int l = 0, r = (int) n;
+  while (l < r) {
+    const int m = (l + r) / 2;
+    if (a[m] > value) r = m;
+    else l = m + 1;
+  }
+  return r - 1;
+}
+
+typedef struct {
+  uint32_t id;
+  float x, y, z;
+  int16_t phi;
+  unsigned sensor;
+} RetinaCluster;
+
+/* populate_retinacluster / populate_sorting_key (DecodeRetinaClusters.cu:80-160, 246-303) */
+static RetinaCluster retina_cluster(const Geometry* g, int v, const RawBank* bank, uint32_t w)
+{
+  RetinaCluster c;
+  unsigned sensor;
+  if (v == 2 || v == 3) sensor = bank->source_id;
+  else sensor = ((w >> 22) & 0x1u) ? sensor_index1(bank) : sensor_index0(bank);
+  uint32_t cx, cy, or_fx, or_fy;
+  float fx, fy;
+  if (v == 2) {
+    cx = (w >> 14) & 0x3FFu;
+    fx = ((w >> 11) & 0x7u) / 8.f;
+    cy = (w >> 3) & 0xFFu;
+    fy = (w & 0x7FFu) / 8.f;
+    or_fx = 0;
+    or_fy = 0;
+  }
+  else {
+    cx = (w >> 12) & 0x3FFu;
+    fx = ((w >> 10) & 0x3u) / 4.f;
+    cy = (w >> 2) & 0xFFu;
+    fy = (w & 0x3FFu) / 4.f;
+    or_fx = ((w >> 11) & 0x1u) | ((w >> 10) & 0x1u);
+    or_fy = ((w >> 1) & 0x1u) | (w & 0x1u);
+  }
+  const float* ltg = g->ltg + 12u * sensor;
+  const float local_x = g->local_x[cx] + fx * g->x_pitch[cx];
+  const float local_y = (0.5f + fy) * pixel_size;
+  c.x = ltg[0] * local_x + ltg[1] * local_y + ltg[9];
+  c.y = ltg[3] * local_x + ltg[4] * local_y + ltg[10];
+  c.z = ltg[6] * local_x + ltg[7] * local_y + ltg[11];
+  c.id = lhcb_id((or_fx << 27) | (or_fy << 26) | channel_id(sensor, cx >> 8, cx & 0xFFu, cy));
+  c.phi = hit_phi_16(c.x, c.y);
+  c.sensor = sensor;
+  return c;
+}
+
+static void decode_retinaclusters(
+  const VeloCpuInput* in, const Geometry* g, const unsigned* pair_offsets, const unsigned* bank_index,
+  unsigned* cluster_num, unsigned* offsets_mp, char* container, unsigned* permutations, int64_t* keys)
+{
+  const int v = in->bank_version;
+  const unsigned n = in->n_events;
+  const unsigned per_event = retina_sensors_per_event(v);
+  const unsigned step = per_event / N_MODULE_PAIRS;
+  const unsigned total = pair_offsets[(size_t) n * per_event];
+  /* populate_module_pair_offsets_and_sizes (:11-35); offsets_mp[0] stays 0 */
+  for (unsigned el = 0; el < n * N_MODULE_PAIRS; ++el)
+    offsets_mp[el + 1] = pair_offsets[(el + 1) * step];
+  unsigned* zero_num = calloc((size_t) n * N_MODULE_PAIRS + 1, sizeof(unsigned));
+  /* velo_calculate_sorting_key (:162-244) */
+  for (unsigned e = 0; e < n; ++e) {
+    const RawEvent ev = raw_event(in, in->event_start + e);
+    const unsigned* so = pair_offsets + (size_t) e * per_event;
+    const unsigned first = so[0], count = so[per_event] - first;
+    for (unsigned k = 0; k < count; ++k) {
+      const unsigned sp = (unsigned) binary_search_rightmost(so, per_event, first + k);
+      const RawBank bank = raw_bank(&ev, bank_index[sp], v);
+      if (bank.type != 73) continue;
+      const uint32_t w = bank.word[k - (so[sp] - first)];
+      const RetinaCluster c = retina_cluster(g, v, &bank, w);
+      if (w != 0) ++cluster_num[e * N_MODULE_PAIRS + c.sensor / 8];
+      else ++zero_num[e * N_MODULE_PAIRS + c.sensor / 8];
+      keys[first + k] = w != 0 ? (int64_t) (((uint64_t) (uint16_t) c.phi << 48) | c.id) : INT64_MAX;
+    }
+  }
+  /* velo_calculate_permutations (:37-78): rank by key among the module pair's entries */
+  for (unsigned e = 0; e < n; ++e)
+    for (unsigned mp = 0; mp < N_MODULE_PAIRS; ++mp) {
+      const unsigned start = offsets_mp[e * N_MODULE_PAIRS + mp];
+      const unsigned num = cluster_num[e * N_MODULE_PAIRS + mp] + zero_num[e * N_MODULE_PAIRS + mp];
+      for (unsigned i = 0; i < num; ++i) {
+        unsigned position = 0;
+        for (unsigned j = 0; j < num; ++j)
+          if (j != i) position += keys[start + i] > keys[start + j];
+        permutations[start + i] = start + position;
+      }
+    }
+  free(zero_num);
+  /* decode_retinaclusters_sorted (:305-383) */
+  Clusters out = {container, total, 0};
+  for (unsigned e = 0; e < n; ++e) {
+    const RawEvent ev = raw_event(in, in->event_start + e);
+    const unsigned* so = pair_offsets + (size_t) e * per_event;
+    const unsigned first = so[0], count = so[per_event] - first;
+    for (unsigned k = 0; k < count; ++k) {
+      const unsigned cn = first + k;
+      const unsigned sp = (unsigned) binary_search_rightmost(so, per_event, cn);
+      const RawBank bank = raw_bank(&ev, bank_index[sp], v);
+      if (bank.type != 73) continue;
+      const RetinaCluster c = retina_cluster(g, v, &bank, bank.word[cn - so[sp]]);
+      const unsigned dst = permutations[cn];
+      set_id(&out, dst, c.id);
+      set_x(&out, dst, c.x);
+      set_y(&out, dst, c.y);
+      set_z(&out, dst, c.z);
+      set_phi(&out, dst, c.phi);
+    }
+  }
+}
+
+/* --------------------------------------------------------------------------------
  * velo_kalman_filter (device/velo/simplified_kalman_filter/src/VeloKalmanFilter.cu:271-399,
  * include/VeloKalmanFilter.cuh:24-158), one track after the other.  Track hits are read from
  * the consolidated container (VeloConsolidated.cuh:19-88: ids, then x y z interleaved).
@@ -1244,32 +1390,52 @@ void* velo_oracle_run(const VeloCpuInput* in)
   float sp_fx[512], sp_fy[512];
   sp_tables(patterns, sp_fx, sp_fy);
 
-  unsigned* n_cand = make(r, "dev_number_of_candidates", n * sizeof(unsigned));
-  unsigned* bank_index = make(r, "dev_velo_bank_index", N_SENSORS * sizeof(unsigned));
-  if (in->bank_version >= 0) calculate_number_of_candidates(in, n_cand, bank_index);
+  unsigned total_clusters = 0;
+  unsigned* offsets_est = NULL;
+  unsigned* cluster_num = NULL;
+  char* sorted = NULL;
+  if (in->retina_decoding) {
+    const unsigned per_event = retina_sensors_per_event(in->bank_version);
+    unsigned* pair_size = make(r, "dev_each_sensor_pair_size", (size_t) n * per_event * sizeof(unsigned));
+    unsigned* retina_bank_index = make(r, "dev_retina_bank_index", per_event * sizeof(unsigned));
+    if (in->bank_version >= 0) retina_count(in, pair_size, retina_bank_index);
+    unsigned* pair_offsets;
+    total_clusters = prefix_sum(r, "dev_offsets_each_sensor_pair_size", pair_size, (size_t) n * per_event, &pair_offsets);
+    cluster_num = make(r, "dev_module_cluster_num", (size_t) n * N_MODULE_PAIRS * sizeof(unsigned));
+    offsets_est = make(r, "dev_offsets_estimated_input_size", ((size_t) n * N_MODULE_PAIRS + 1) * sizeof(unsigned));
+    sorted = make(r, "dev_sorted_velo_cluster_container", (size_t) total_clusters * ELEMENT_SIZE);
+    unsigned* permutations = make(r, "dev_hit_permutations", (size_t) total_clusters * sizeof(unsigned));
+    int64_t* keys = make(r, "dev_hit_sorting_key", (size_t) total_clusters * sizeof(int64_t));
+    if (in->bank_version >= 0)
+      decode_retinaclusters(in, g, pair_offsets, retina_bank_index, cluster_num, offsets_est, sorted, permutations, keys);
+  }
+  else {
+    unsigned* n_cand = make(r, "dev_number_of_candidates", n * sizeof(unsigned));
+    unsigned* bank_index = make(r, "dev_velo_bank_index", N_SENSORS * sizeof(unsigned));
+    if (in->bank_version >= 0) calculate_number_of_candidates(in, n_cand, bank_index);
 
-  unsigned* cand_offsets;
-  const unsigned total_cand = prefix_sum(r, "dev_candidates_offsets", n_cand, n, &cand_offsets);
+    unsigned* cand_offsets;
+    const unsigned total_cand = prefix_sum(r, "dev_candidates_offsets", n_cand, n, &cand_offsets);
 
-  unsigned* estimated = make(r, "dev_estimated_input_size", (size_t) n * N_MODULE_PAIRS * sizeof(unsigned));
-  unsigned* cand_num = make(r, "dev_module_candidate_num", n * sizeof(unsigned));
-  uint32_t* candidates = make(r, "dev_cluster_candidates", (size_t) total_cand * sizeof(uint32_t));
-  if (in->bank_version >= 0) estimate_input_size(in, cand_offsets, estimated, cand_num, candidates);
+    unsigned* estimated = make(r, "dev_estimated_input_size", (size_t) n * N_MODULE_PAIRS * sizeof(unsigned));
+    unsigned* cand_num = make(r, "dev_module_candidate_num", n * sizeof(unsigned));
+    uint32_t* candidates = make(r, "dev_cluster_candidates", (size_t) total_cand * sizeof(uint32_t));
+    if (in->bank_version >= 0) estimate_input_size(in, cand_offsets, estimated, cand_num, candidates);
 
-  unsigned* offsets_est;
-  const unsigned total_clusters =
-    prefix_sum(r, "dev_offsets_estimated_input_size", estimated, (size_t) n * N_MODULE_PAIRS, &offsets_est);
+    total_clusters =
+      prefix_sum(r, "dev_offsets_estimated_input_size", estimated, (size_t) n * N_MODULE_PAIRS, &offsets_est);
 
-  unsigned* cluster_num = make(r, "dev_module_cluster_num", (size_t) n * N_MODULE_PAIRS * sizeof(unsigned));
-  char* container = make(r, "dev_velo_cluster_container", (size_t) total_clusters * ELEMENT_SIZE);
-  if (in->bank_version >= 0)
-    masked_clustering(
-      in, g, patterns, sp_fx, sp_fy, offsets_est, cand_num, candidates, cand_offsets, bank_index, cluster_num,
-      container);
+    cluster_num = make(r, "dev_module_cluster_num", (size_t) n * N_MODULE_PAIRS * sizeof(unsigned));
+    char* container = make(r, "dev_velo_cluster_container", (size_t) total_clusters * ELEMENT_SIZE);
+    if (in->bank_version >= 0)
+      masked_clustering(
+        in, g, patterns, sp_fx, sp_fy, offsets_est, cand_num, candidates, cand_offsets, bank_index, cluster_num,
+        container);
 
-  char* sorted = make(r, "dev_sorted_velo_cluster_container", (size_t) total_clusters * ELEMENT_SIZE);
-  unsigned* perm = make(r, "dev_hit_permutation", (size_t) total_clusters * sizeof(unsigned));
-  sort_by_phi(n, offsets_est, cluster_num, container, sorted, perm);
+    sorted = make(r, "dev_sorted_velo_cluster_container", (size_t) total_clusters * ELEMENT_SIZE);
+    unsigned* perm = make(r, "dev_hit_permutation", (size_t) total_clusters * sizeof(unsigned));
+    sort_by_phi(n, offsets_est, cluster_num, container, sorted, perm);
+  }
 
   const unsigned by_clusters = (unsigned) ((float) total_clusters * tracks_per_cluster);
   const unsigned track_container_size =

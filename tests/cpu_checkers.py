@@ -44,7 +44,7 @@ class VeloCpuInput(C.Structure):
         ("bank_version", C.c_int), ("geometry", C.c_void_p), ("geometry_size", C.c_size_t),
         ("phi_tolerance", C.c_float), ("max_scatter", C.c_float),
         ("max_skipped_modules", C.c_uint), ("max_chi2", C.c_float),
-        ("beamline_x", C.c_float), ("beamline_y", C.c_float),
+        ("beamline_x", C.c_float), ("beamline_y", C.c_float), ("retina_decoding", C.c_int),
     ]
 
 
@@ -73,7 +73,7 @@ class Checker:
 
     @staticmethod
     def make_input(s, geometry: bytes, event_start=0, n_events=None, phi_tolerance=0.045,
-                   max_scatter=0.08, max_skipped_modules=1, max_chi2=20.0, beamline=(0.0, 0.0)):
+                   max_scatter=0.08, max_skipped_modules=1, max_chi2=20.0, beamline=(0.0, 0.0), retina=None):
         keep = (np.ascontiguousarray(s.raw), np.ascontiguousarray(s.offsets),
                 np.ascontiguousarray(s.sizes), np.ascontiguousarray(s.types),
                 np.frombuffer(geometry, dtype=np.uint8))
@@ -81,7 +81,8 @@ class Checker:
             keep[0].ctypes.data, keep[1].ctypes.data, keep[2].ctypes.data, keep[3].ctypes.data,
             event_start, s.n_events - event_start if n_events is None else n_events,
             s.bank_version, keep[4].ctypes.data, len(geometry),
-            phi_tolerance, max_scatter, max_skipped_modules, max_chi2, beamline[0], beamline[1])
+            phi_tolerance, max_scatter, max_skipped_modules, max_chi2, beamline[0], beamline[1],
+            int(retina if retina is not None else getattr(s, "retina", False)))
         return inp, keep
 
     def run(self, s, geometry: bytes, **kw) -> dict:
@@ -109,6 +110,8 @@ class Checker:
 
 
 U32_BUFFERS = [
+    "dev_each_sensor_pair_size", "dev_retina_bank_index", "dev_offsets_each_sensor_pair_size",
+    "dev_hit_permutations",
     "dev_number_of_candidates", "dev_velo_bank_index", "dev_candidates_offsets",
     "dev_estimated_input_size", "dev_module_candidate_num", "dev_cluster_candidates",
     "dev_offsets_estimated_input_size", "dev_module_cluster_num", "dev_hit_permutation",

@@ -10,11 +10,15 @@ Outputs:
       input/minbias/mdf/MiniBrunel_2018_MinBias_FTv4_DIGI_retinacluster_v1.mdf, in
       Allen's raw-bank layout, plus the reference's own outputs for them;
   tests/golden/synthetic_seed7_20ev.npz
-      20 generated events (nu = 7.6, seed 7) plus the reference's outputs for them.
+      20 generated events (nu = 7.6, seed 7, super pixels in column order) plus the
+      reference's outputs for them;
+  tests/golden/minbias_retina_10ev.npz
+      the VPRetinaCluster banks (type 73, version 3) of the same 10 events, plus the
+      reference's outputs through its retina-cluster decoding and the VELO Kalman filter.
 
 The reference outputs come from oracle/_ref/libvelo_ref.so, the reference's VELO
 kernels compiled as CPU C++ (oracle/Makefile).  Usage:
-    python tests/golden/make_fixtures.py [/path/to/reference]
+    python tests/golden/make_fixtures.py [/path/to/reference] [fixture names...]
 """
 from __future__ import annotations
 
@@ -43,7 +47,17 @@ GOLDEN_BUFFERS = [
 ]
 
 
-def read_mdf_vp_events(path):
+RETINA_BUFFERS = [
+    "dev_each_sensor_pair_size", "dev_offsets_each_sensor_pair_size", "dev_offsets_estimated_input_size",
+    "dev_module_cluster_num", "dev_sorted_velo_cluster_container", "dev_number_of_velo_tracks",
+    "dev_offsets_velo_tracks", "dev_number_of_three_hit_tracks_output",
+    "dev_offsets_number_of_three_hit_tracks_filtered", "dev_offsets_all_velo_tracks", "dev_velo_track_hit_number",
+    "dev_offsets_velo_track_hit_number", "dev_velo_track_hits", "dev_three_hit_tracks_output", "dev_hit_used",
+    "dev_atomics_velo", "dev_is_backward", "dev_velo_kalman_beamline_states", "dev_velo_kalman_endvelo_states",
+]
+
+
+def read_mdf_vp_events(path, bank_type=rawbanks.BANK_TYPE_VP, version=2):
     data = open(path, "rb").read()
     p, events = 0, []
     while p + 20 <= len(data):
@@ -53,10 +67,10 @@ def read_mdf_vp_events(path):
         q, end = p + 20 + sub, p + size0
         banks = []
         while q < end:
-            magic, size, btype, version, src = struct.unpack_from("<HHBBH", data, q)
+            magic, size, btype, bank_version, src = struct.unpack_from("<HHBBH", data, q)
             assert magic == 0xCBCB
-            if btype == rawbanks.BANK_TYPE_VP:
-                assert version == 2
+            if btype == bank_type:
+                assert bank_version == version
                 banks.append((btype, src, data[q + 8:q + size]))
             q += (size + 3) // 4 * 4
         events.append(banks)
@@ -64,7 +78,7 @@ def read_mdf_vp_events(path):
     return events
 
 
-def main(ref_root):
+def main(ref_root, only=()):
     geo_src = os.path.join(ref_root, "input/detector_configuration/velo_geometry.bin")
     geometry = open(geo_src, "rb").read()
     os.makedirs(os.path.join(REPO, "allen_b200/data"), exist_ok=True)
@@ -78,13 +92,16 @@ def main(ref_root):
     real = rawbanks.build_slice(read_mdf_vp_events(mdf), bank_version=2)
 
     from allen_b200 import generator  # noqa: E402
-    synth = generator.generate(20, seed=7, geometry=geometry).raw
+    synth = generator.generate(20, seed=7, geometry=geometry, sp_order=0).raw
+    retina = rawbanks.build_slice(read_mdf_vp_events(mdf, rawbanks.BANK_TYPE_VP_RETINA, 3), bank_version=3)
 
-    for name, s in (("minbias_vp_10ev", real), ("synthetic_seed7_20ev", synth)):
+    for name, s in (("minbias_vp_10ev", real), ("synthetic_seed7_20ev", synth), ("minbias_retina_10ev", retina)):
+        if only and name not in only:
+            continue
         out = ref.run(s, geometry)
         arrays = {"raw": s.raw, "offsets": s.offsets, "sizes": s.sizes, "types": s.types,
                   "bank_version": np.array([s.bank_version])}
-        for b in GOLDEN_BUFFERS:
+        for b in (RETINA_BUFFERS if s.retina else GOLDEN_BUFFERS):
             arrays["ref__" + b] = out[b]
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
         print(name, s.n_events, "events;",
@@ -93,4 +110,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", tuple(sys.argv[2:]))
