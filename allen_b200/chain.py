@@ -64,7 +64,8 @@ OUTPUT_FIELDS = [
     "dev_offsets_number_of_three_hit_tracks_filtered", "dev_offsets_all_velo_tracks",
     "dev_velo_track_hit_number", "dev_offsets_velo_track_hit_number", "dev_velo_track_hits",
     "dev_accepted_velo_tracks", "dev_seed_stats", "dev_is_backward", "dev_velo_kalman_beamline_states",
-    "dev_velo_kalman_endvelo_states",
+    "dev_velo_kalman_endvelo_states", "dev_each_sensor_pair_size", "dev_offsets_each_sensor_pair_size",
+    "dev_retina_bank_index",
 ]
 
 
@@ -136,6 +137,8 @@ def _lib():
     lib.velo_chain_kernel_name.argtypes = [C.c_uint]
     lib.velo_chain_kernel_times.restype = C.c_int
     lib.velo_chain_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint)]
+    lib.velo_chain_set_front_end.restype = C.c_int
+    lib.velo_chain_set_front_end.argtypes = [C.c_void_p, C.c_int]
     lib.velo_chain_set_kalman.restype = C.c_int
     lib.velo_chain_set_kalman.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float]
     lib.velo_kalman_filter.restype = C.c_int
@@ -182,6 +185,7 @@ class DeviceSlice:
     n_events: int
     bank_version: int
     event_start: int = 0
+    retina: bool = False  # retina-cluster banks (type 73)
 
     def c_struct(self) -> DeviceSliceC:
         return DeviceSliceC(self.raw.data_ptr(), self.offsets.data_ptr(), self.sizes.data_ptr(),
@@ -189,7 +193,7 @@ class DeviceSlice:
 
     def sub(self, event_start: int, n_events: int) -> "DeviceSlice":
         return DeviceSlice(self.raw, self.offsets, self.sizes, self.types, n_events, self.bank_version,
-                           event_start)
+                           event_start, self.retina)
 
 
 def upload(s: RawSlice, device="cuda") -> DeviceSlice:
@@ -200,7 +204,7 @@ def upload(s: RawSlice, device="cuda") -> DeviceSlice:
         raw = np.concatenate([raw, np.zeros(pad, np.uint8)])
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
     return DeviceSlice(t(raw), t(s.offsets.view(np.int32)), t(s.sizes.view(np.int32)),
-                       t(s.types.view(np.int32)), s.n_events, s.bank_version)
+                       t(s.types.view(np.int32)), s.n_events, s.bank_version, 0, s.retina)
 
 
 class VeloChain:
@@ -238,8 +242,16 @@ class VeloChain:
         n_sp = int(super_pixels_per_event(s).sum())
         self.reserve(s.n_events, int(n_sp * margin) + 64, s.raw.nbytes + 64)
 
+    def set_front_end(self, retina: bool):
+        """Decoding front end: super-pixel banks (False) or retina-cluster banks (True)."""
+        _check(self.lib, self.lib.velo_chain_set_front_end(self.handle, int(retina)))
+        self.retina = bool(retina)
+
     def run(self, d: DeviceSlice, stream=None, use_graph: bool = False):
+        if bool(getattr(d, "retina", False)) != getattr(self, "retina", False):
+            self.set_front_end(d.retina)
         st = d.c_struct()
+        self.last_bank_version = d.bank_version
         _check(self.lib, self.lib.velo_chain_run(self.handle, C.byref(st),
                                                  stream if stream is not None else _current_stream(),
                                                  int(use_graph)))
@@ -345,6 +357,13 @@ class VeloChain:
             "dev_velo_track_hits": (ELEMENT_SIZE * TH, np.uint8),
             "dev_accepted_velo_tracks": (reco + three, np.uint8),
         }
+        if getattr(self, "retina", False):
+            for k in ("dev_number_of_candidates", "dev_estimated_input_size", "dev_module_candidate_num"):
+                del sizes[k]
+            per_event = 208 if self.last_bank_version in (2, 3) else 104
+            sizes.update({"dev_each_sensor_pair_size": (4 * per_event * n, u4),
+                          "dev_offsets_each_sensor_pair_size": (4 * (per_event * n + 1), u4),
+                          "dev_retina_bank_index": (4 * per_event, u4)})
         return {k: self._fetch(p[k], nb, dt) for k, (nb, dt) in sizes.items()}
 
     def run_host(self, s: RawSlice, stream=None) -> tuple[dict, dict, int, int]:

@@ -189,6 +189,9 @@ static const SearchVariant search_variants[] = {
 #undef VELO_SEARCH_VARIANT
 };
 
+static constexpr unsigned retina_key_capacity = 4096; // clusters of an event keyed in shared memory (32 KiB)
+static constexpr size_t n_sensors_total = velo::n_sensors;
+
 static SearchKernel learned_search_kernel(unsigned threads)
 {
   switch (threads) {
@@ -258,6 +261,10 @@ struct VeloChain {
   bool kalman = false;
   float beamline[2] = {0.f, 0.f};
   DeviceBuffer<uint8_t> is_backward;
+  // retina-cluster front end (VPRetinaCluster banks) instead of super pixels
+  bool retina = false;
+  DeviceBuffer<unsigned> retina_sizes, retina_offsets, retina_bank_index;
+  DeviceBuffer<long long> retina_keys;
   DeviceBuffer<float> kalman_beamline_states, kalman_endvelo_states;
   velo::DoubletRecord* records = nullptr;
   unsigned* record_count = nullptr;
@@ -341,48 +348,82 @@ namespace {
     }
     VELO_CUDA(mark());
 
-    EstimateParams ep {};
-    ep.in = in;
-    ep.estimated_input_size = c->estimated.p;
-    ep.number_of_candidates = c->number_of_candidates.p;
-    ep.module_candidate_num = c->candidate_num.p;
-    ep.event_estimate = c->event_estimate.p;
-    ep.bank_index_key = c->bank_index_key.p;
-    ep.designated_stride = (n + 255) / 256;
-    ep.status = c->status.p;
-    ep.smem_blob_bytes = c->estimate_blob_bytes;
-    ep.queue = queue(0);
-    estimate_kernel<<<grid(c->resident_estimate), decode_threads, c->estimate_blob_bytes, stream>>>(ep);
-    VELO_CUDA(cudaGetLastError());
-    VELO_CUDA(mark());
+    if (c->retina) {
+      // retina-cluster front end (velo_reconstruction.py:18-71): count, scan, decode + sort
+      RetinaParams rp {};
+      rp.in = in;
+      rp.geo = c->geo.p;
+      rp.k = c->k;
+      rp.each_sensor_pair_size = c->retina_sizes.p;
+      rp.bank_index = c->retina_bank_index.p;
+      rp.event_total = c->event_estimate.p;
+      rp.event_base = c->event_base.p;
+      rp.offsets_each_sensor_pair_size = c->retina_offsets.p;
+      rp.offsets_module_pair_cluster = c->offsets_est.p;
+      rp.module_cluster_num = c->cluster_num.p;
+      rp.container = c->sorted.p;
+      rp.key_scratch = c->retina_keys.p;
+      rp.status = c->status.p;
+      rp.smem_key_capacity = retina_key_capacity;
+      rp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
+      VELO_CUDA(cudaMemsetAsync(c->retina_bank_index.p, 0, n_sensors * sizeof(unsigned), stream));
+      VELO_CUDA(cudaMemsetAsync(c->candidates_offsets.p, 0, (n + 1) * sizeof(unsigned), stream));
+      retina_count_kernel<<<n, decode_threads, 0, stream>>>(rp);
+      VELO_CUDA(cudaGetLastError());
+      VELO_CUDA(mark());
+      ScanParams rs {};
+      rs.jobs[0] = {c->event_estimate.p, c->event_base.p, n};
+      exclusive_scan_kernel<<<1, scan_threads, 0, stream>>>(rs);
+      VELO_CUDA(cudaGetLastError());
+      VELO_CUDA(mark());
+      retina_decode_kernel<<<n, decode_threads, retina_key_capacity * sizeof(long long), stream>>>(rp);
+      VELO_CUDA(cudaGetLastError());
+      VELO_CUDA(mark());
+    }
+    else {
+      EstimateParams ep {};
+      ep.in = in;
+      ep.estimated_input_size = c->estimated.p;
+      ep.number_of_candidates = c->number_of_candidates.p;
+      ep.module_candidate_num = c->candidate_num.p;
+      ep.event_estimate = c->event_estimate.p;
+      ep.bank_index_key = c->bank_index_key.p;
+      ep.designated_stride = (n + 255) / 256;
+      ep.status = c->status.p;
+      ep.smem_blob_bytes = c->estimate_blob_bytes;
+      ep.queue = queue(0);
+      estimate_kernel<<<grid(c->resident_estimate), decode_threads, c->estimate_blob_bytes, stream>>>(ep);
+      VELO_CUDA(cudaGetLastError());
+      VELO_CUDA(mark());
 
-    ScanParams sp1 {};
-    sp1.jobs[0] = {c->event_estimate.p, c->event_base.p, n};
-    sp1.jobs[1] = {c->number_of_candidates.p, c->candidates_offsets.p, n};
-    exclusive_scan_kernel<<<2, scan_threads, 0, stream>>>(sp1);
-    VELO_CUDA(cudaGetLastError());
-    VELO_CUDA(mark());
+      ScanParams sp1 {};
+      sp1.jobs[0] = {c->event_estimate.p, c->event_base.p, n};
+      sp1.jobs[1] = {c->number_of_candidates.p, c->candidates_offsets.p, n};
+      exclusive_scan_kernel<<<2, scan_threads, 0, stream>>>(sp1);
+      VELO_CUDA(cudaGetLastError());
+      VELO_CUDA(mark());
 
-    ClusterSortParams cp {};
-    cp.in = in;
-    cp.geo = c->geo.p;
-    cp.k = c->k;
-    cp.estimated_input_size = c->estimated.p;
-    cp.event_base = c->event_base.p;
-    cp.bank_index_key = c->bank_index_key.p;
-    cp.offsets_estimated_input_size = c->offsets_est.p;
-    cp.module_cluster_num = c->cluster_num.p;
-    cp.sorted_container = c->sorted.p;
-    cp.staging = c->staging.p;
-    cp.status = c->status.p;
-    cp.smem_blob_bytes = c->cluster_blob_bytes;
-    cp.smem_cluster_capacity = c->cluster_stage_capacity;
-    cp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
-    const unsigned cluster_smem = cluster_sort_blob_offset(c->cluster_stage_capacity) + c->cluster_blob_bytes;
-    cp.queue = queue(1);
-    cluster_sort_kernel<<<grid(c->resident_cluster), decode_threads, cluster_smem, stream>>>(cp);
-    VELO_CUDA(cudaGetLastError());
-    VELO_CUDA(mark());
+      ClusterSortParams cp {};
+      cp.in = in;
+      cp.geo = c->geo.p;
+      cp.k = c->k;
+      cp.estimated_input_size = c->estimated.p;
+      cp.event_base = c->event_base.p;
+      cp.bank_index_key = c->bank_index_key.p;
+      cp.offsets_estimated_input_size = c->offsets_est.p;
+      cp.module_cluster_num = c->cluster_num.p;
+      cp.sorted_container = c->sorted.p;
+      cp.staging = c->staging.p;
+      cp.status = c->status.p;
+      cp.smem_blob_bytes = c->cluster_blob_bytes;
+      cp.smem_cluster_capacity = c->cluster_stage_capacity;
+      cp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
+      const unsigned cluster_smem = cluster_sort_blob_offset(c->cluster_stage_capacity) + c->cluster_blob_bytes;
+      cp.queue = queue(1);
+      cluster_sort_kernel<<<grid(c->resident_cluster), decode_threads, cluster_smem, stream>>>(cp);
+      VELO_CUDA(cudaGetLastError());
+      VELO_CUDA(mark());
+    }
 
     SearchParams sp {};
     sp.geo = c->geo.p;
@@ -627,6 +668,10 @@ VeloStatus velo_chain_reserve(
   RES(c->seed_stats, 3 * n)
   RES(c->queue_next, 3)
   RES(c->is_backward, tracks)
+  RES(c->retina_sizes, n * n_sensors_total)
+  RES(c->retina_offsets, n * n_sensors_total + 1)
+  RES(c->retina_bank_index, n_sensors_total)
+  RES(c->retina_keys, T)
   RES(c->kalman_beamline_states, 14 * tracks)
   RES(c->kalman_endvelo_states, 14 * tracks)
   RES(c->event_order, n)
@@ -824,6 +869,9 @@ VeloStatus velo_chain_outputs(const VeloChain* c, VeloChainOutputs* o)
   o->dev_accepted_velo_tracks = c->accepted.p;
   o->dev_seed_stats = c->seed_stats.p;
   o->dev_is_backward = c->is_backward.p;
+  o->dev_each_sensor_pair_size = c->retina ? c->retina_sizes.p : nullptr;
+  o->dev_offsets_each_sensor_pair_size = c->retina ? c->retina_offsets.p : nullptr;
+  o->dev_retina_bank_index = c->retina ? c->retina_bank_index.p : nullptr;
   o->dev_velo_kalman_beamline_states = reinterpret_cast<char*>(c->kalman_beamline_states.p);
   o->dev_velo_kalman_endvelo_states = reinterpret_cast<char*>(c->kalman_endvelo_states.p);
   return VELO_OK;
@@ -891,6 +939,14 @@ VeloStatus velo_copy_to_host_async(void* host, const void* device, size_t bytes,
 VeloStatus velo_copy_to_device(void* device, const void* host, size_t bytes)
 {
   VELO_CUDA(cudaMemcpy(device, host, bytes, cudaMemcpyHostToDevice));
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_set_front_end(VeloChain* c, int retina_clusters)
+{
+  if (!c) return fail(VELO_ERR_ARGUMENT, "null chain");
+  if (bool(retina_clusters) != c->retina) c->release_graph();
+  c->retina = retina_clusters != 0;
   return VELO_OK;
 }
 
@@ -1016,6 +1072,10 @@ void velo_chain_destroy(VeloChain* c)
   c->seed_stats.release();
   c->queue_next.release();
   c->is_backward.release();
+  c->retina_sizes.release();
+  c->retina_offsets.release();
+  c->retina_bank_index.release();
+  c->retina_keys.release();
   c->kalman_beamline_states.release();
   c->kalman_endvelo_states.release();
   c->event_order.release();

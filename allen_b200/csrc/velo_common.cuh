@@ -27,6 +27,7 @@ namespace velo {
   constexpr unsigned element_size = 18;
   constexpr unsigned bank_type_velo = 8;
   constexpr unsigned bank_type_vp = 63;
+  constexpr unsigned bank_type_vp_retina = 73; // LHCb::RawBank::VPRetinaCluster
 
   // Error flags (bit set in the chain's device status word; read by the host after a run).
   enum ErrorBits : unsigned {

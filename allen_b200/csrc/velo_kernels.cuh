@@ -167,6 +167,27 @@ namespace velo {
 // lanes 0 = flattened seeding (one thread per h1 candidate)
 #define VELO_SEARCH_CONFIGS(X) X(128, 1) X(128, 2) X(256, 1) X(256, 2) X(256, 4) X(512, 2) X(512, 4) X(128, 0) X(256, 0) X(512, 0)
   __global__ void consolidate_kernel(ConsolidateParams p);
+  // ---- retina-cluster decoding (VPRetinaCluster banks) ----
+  struct RetinaParams {
+    RawInput in;
+    const Geometry* geo;
+    Constants k;
+    unsigned* each_sensor_pair_size;         // [S N] dev_each_sensor_pair_size (S = 208 v2/v3, 104 v4)
+    unsigned* bank_index;                    // [S]   dev_retina_bank_index (zeroed before the count)
+    unsigned* event_total;                   // [N]   clusters per event
+    const unsigned* event_base;              // [N + 1] exclusive scan of event_total
+    unsigned* offsets_each_sensor_pair_size; // [S N + 1]
+    unsigned* offsets_module_pair_cluster;   // [26 N + 1] the search's dev_offsets_estimated_input_size
+    unsigned* module_cluster_num;            // [26 N]
+    char* container;                         // [18 T] dev_velo_cluster_container (sorted)
+    long long* key_scratch;                  // [T] keys of events above the shared-memory capacity
+    unsigned* status;
+    unsigned smem_key_capacity;              // clusters of an event keyed in shared memory
+    unsigned cluster_capacity;               // allocated T
+  };
+  __global__ void retina_count_kernel(RetinaParams p);
+  __global__ void retina_decode_kernel(RetinaParams p);
+
   // ---- velo_kalman_filter: one thread per consolidated track ----
   struct KalmanParams {
     unsigned n_events;

@@ -108,6 +108,9 @@ typedef struct {
   uint8_t* dev_is_backward;                        /* [tracks] velo_kalman_filter (when enabled) */
   char* dev_velo_kalman_beamline_states;           /* [56 tracks] Velo::Consolidated::States */
   char* dev_velo_kalman_endvelo_states;            /* [56 tracks] */
+  unsigned* dev_each_sensor_pair_size;             /* retina front end: [S N], S = 208 (v2/v3) or 104 (v4) */
+  unsigned* dev_offsets_each_sensor_pair_size;     /* [S N + 1] */
+  unsigned* dev_retina_bank_index;                 /* [S] */
 } VeloChainOutputs;
 
 /* Host scalars of the last run, available after velo_chain_synchronize(). */
@@ -235,6 +238,17 @@ unsigned velo_noalloc_max_events(void);
 unsigned velo_noalloc_max_clusters(void);
 unsigned long long velo_noalloc_scratch_bytes(void);
 const char* velo_noalloc_last_error_string(void);
+
+/* Decoding front end.  0 (default): super-pixel banks (VP, type 63) through
+ * velo_calculate_number_of_candidates, velo_estimate_input_size, velo_masked_clustering and
+ * velo_sort_by_phi.  1: retina-cluster banks (VPRetinaCluster, type 73) through
+ * calculate_number_of_retinaclusters_each_sensor_pair, its prefix sum and decode_retinaclusters
+ * (configuration/python/AllenConf/velo_reconstruction.py:18-71, Allen's default); the search
+ * then reads dev_offsets_module_pair_cluster as dev_offsets_estimated_input_size.  In retina
+ * mode the kernel timings of stages 0 and 2 are retina_count_kernel and retina_decode_kernel,
+ * and dev_number_of_candidates, dev_estimated_input_size and dev_module_candidate_num are not
+ * produced. */
+VeloStatus velo_chain_set_front_end(VeloChain* chain, int retina_clusters);
 
 /* velo_kalman_filter (device/velo/simplified_kalman_filter/src/VeloKalmanFilter.cu:153-399,
  * wired at configuration/python/AllenConf/velo_reconstruction.py:295-322): the simplified

@@ -159,3 +159,21 @@ def test_persistent_work_queue_identical(chain, oracle, geometry, claim):
         assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
     finally:
         chain.configure(**saved)
+
+
+@pytest.mark.parametrize("version", [2, 3, 4])
+def test_retina_front_end(chain, oracle, geometry, version):
+    """Retina-cluster banks: decoding, search and consolidation against the oracle."""
+    g = generator.generate(120, seed=90 + version, raw_format=1, bank_version=version, pileup_min=1.0,
+                           pileup_max=15.0)
+    assert g.raw.retina
+    totals, out = run_chain(chain, g.raw, use_graph=True)
+    assert totals["device_flags"] == 0
+    ref = oracle.run(g.raw, geometry)
+    assert parity.compare(out, ref, g.raw.n_events) == []
+    for k in ("dev_each_sensor_pair_size", "dev_offsets_each_sensor_pair_size"):
+        assert np.array_equal(out[k], ref[k]), k
+    # back to super pixels on the same chain
+    s = generator.generate(30, seed=3).raw
+    totals, out = run_chain(chain, s)
+    assert parity.compare(out, oracle.run(s, geometry), s.n_events) == []
