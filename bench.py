@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-mode measurement")
     p.add_argument("--no-kalman", action="store_true", help="skip the velo_kalman_filter measurement")
+    p.add_argument("--no-retina", action="store_true", help="skip the retina-cluster front-end measurement")
     return p.parse_args()
 
 
@@ -110,12 +111,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def generate_slices(n_events, slice_size, seed, pinned=False):
+def generate_slices(n_events, slice_size, seed, pinned=False, **gen):
     from allen_b200 import generator
     out = []
     for first in range(0, n_events, slice_size):
         n = min(slice_size, n_events - first)
-        out.append(generator.generate(n, seed=seed, first_event=first).raw)
+        out.append(generator.generate(n, seed=seed, first_event=first, **gen).raw)
     return out
 
 
@@ -413,6 +414,50 @@ def run_ours(args):
                                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
                   "workload": "chain + velo_kalman_filter (beamline 0, 0) on the same events"}
 
+    # the retina-cluster front end (Allen's default decoding) on the same generated events,
+    # written as VPRetinaCluster banks (version 3, as the 2018 sample)
+    retina = None
+    if not args.no_retina:
+        r_slices = generate_slices(args.events, args.slice, seed, raw_format=1, bank_version=3)
+        r_dev = [upload(x) for x in r_slices]
+        chain.reserve(max(x.n_events for x in r_slices), max(int(super_pixels_per_event(x).sum()) for x in r_slices) + 64,
+                      max(x.raw.nbytes for x in r_slices) + 64)
+
+        def r_step():
+            for d in r_dev:
+                chain.run(d, use_graph=True)
+
+        for _ in range(max(3, args.warmup)):
+            r_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        r_start, r_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r_start.record(stream)
+        for _ in range(args.steps):
+            r_step()
+        r_end.record(stream)
+        torch.cuda.synchronize()
+        r_ms = r_start.elapsed_time(r_end)
+        if world > 1:
+            t = torch.tensor([r_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            r_ms = float(t.item())
+        try:
+            rt, rruns = chain.kernel_times()
+            r_kernels = {"retina_count_kernel": round(rt["estimate_kernel"] / max(rruns, 1), 4),
+                         "retina_decode_kernel": round(rt["cluster_sort_kernel"] / max(rruns, 1), 4),
+                         "search_by_triplet_kernel": round(rt["search_by_triplet_kernel"] / max(rruns, 1), 4)}
+        except Exception:
+            r_kernels = None
+        r_events = sum(x.n_events for x in r_slices)
+        retina = {"value": round(world * r_events * args.steps / (r_ms / 1e3), 1), "unit": UNIT,
+                  "ms_per_launch": r_kernels,
+                  "workload": f"the same {args.events} events per GPU as VPRetinaCluster banks (version 3) "
+                              f"through the retina-cluster front end, slices of {args.slice}"}
+        chain.set_front_end(False)
+        del r_dev, r_slices
+
     # end to end through the public API from page-locked host buffers: HostPipeline copies each
     # slice in, runs the chain and copies the consolidated tracks out, two chains overlapping
     e2e = None
@@ -475,6 +520,7 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "learned": learned,
             "kalman": kalman,
+            "retina": retina,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "device_flags": totals_last["device_flags"],
