@@ -47,7 +47,8 @@ class Properties(C.Structure):
 
 class DeviceSliceC(C.Structure):
     _fields_ = [("raw", C.c_void_p), ("offsets", C.c_void_p), ("sizes", C.c_void_p), ("types", C.c_void_p),
-                ("event_start", C.c_uint), ("n_events", C.c_uint), ("bank_version", C.c_int)]
+                ("event_start", C.c_uint), ("n_events", C.c_uint), ("bank_version", C.c_int),
+                ("mep_layout", C.c_int)]
 
 
 class HostSliceC(C.Structure):
@@ -186,14 +187,15 @@ class DeviceSlice:
     bank_version: int
     event_start: int = 0
     retina: bool = False  # retina-cluster banks (type 73)
+    mep: bool = False     # MEP layout
 
     def c_struct(self) -> DeviceSliceC:
         return DeviceSliceC(self.raw.data_ptr(), self.offsets.data_ptr(), self.sizes.data_ptr(),
-                            self.types.data_ptr(), self.event_start, self.n_events, self.bank_version)
+                            self.types.data_ptr(), self.event_start, self.n_events, self.bank_version, int(self.mep))
 
     def sub(self, event_start: int, n_events: int) -> "DeviceSlice":
         return DeviceSlice(self.raw, self.offsets, self.sizes, self.types, n_events, self.bank_version,
-                           event_start, self.retina)
+                           event_start, self.retina, self.mep)
 
 
 def upload(s: RawSlice, device="cuda") -> DeviceSlice:
@@ -204,7 +206,7 @@ def upload(s: RawSlice, device="cuda") -> DeviceSlice:
         raw = np.concatenate([raw, np.zeros(pad, np.uint8)])
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
     return DeviceSlice(t(raw), t(s.offsets.view(np.int32)), t(s.sizes.view(np.int32)),
-                       t(s.types.view(np.int32)), s.n_events, s.bank_version, 0, s.retina)
+                       t(s.types.view(np.int32)), s.n_events, s.bank_version, 0, s.retina, s.mep)
 
 
 class VeloChain:

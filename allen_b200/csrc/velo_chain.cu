@@ -324,7 +324,7 @@ namespace {
   {
     using namespace velo;
     const unsigned n = s.n_events;
-    RawInput in {s.raw, s.offsets, s.sizes, s.types, s.event_start, s.n_events, s.bank_version};
+    RawInput in {s.raw, s.offsets, s.sizes, s.types, s.event_start, s.n_events, s.bank_version, s.mep_layout};
     unsigned stage = 0;
     // inside a capture the records must become graph nodes of their own (external events)
     auto mark = [&]() -> cudaError_t {
@@ -705,7 +705,8 @@ VeloStatus velo_chain_run(VeloChain* c, const VeloDeviceSlice* s, VeloStream str
   for (auto& g : c->graphs) {
     const VeloDeviceSlice& k = g.key;
     if (k.raw == s->raw && k.offsets == s->offsets && k.sizes == s->sizes && k.types == s->types &&
-        k.event_start == s->event_start && k.n_events == s->n_events && k.bank_version == s->bank_version) {
+        k.event_start == s->event_start && k.n_events == s->n_events && k.bank_version == s->bank_version &&
+        k.mep_layout == s->mep_layout) {
       entry = &g;
       break;
     }

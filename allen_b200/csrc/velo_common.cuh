@@ -153,7 +153,26 @@ namespace velo {
     unsigned event_start;
     unsigned n_events;
     int bank_version;
+    int mep_layout; // 1: MEP layout (MEPTools.h:55-205), banks of one source together
   };
+
+  // MEP layout accessors (MEPTools.h:55-205): offsets = [n_banks, n_events, source ids,
+  // per event the byte offset of every bank's fragment]; sizes and types: one u32 offset per
+  // bank, then the bank's per-event values.  A fragment has no sourceID word.
+  __device__ __forceinline__ unsigned mep_n_banks(const RawInput& in) { return in.offsets[0]; }
+  __device__ __forceinline__ unsigned mep_source_id(const RawInput& in, unsigned b) { return in.offsets[2 + b]; }
+  __device__ __forceinline__ unsigned mep_fragment_offset(const RawInput& in, unsigned ev, unsigned b)
+  {
+    return in.offsets[2 + in.offsets[0] * (1 + ev) + b];
+  }
+  __device__ __forceinline__ unsigned mep_bank_size(const RawInput& in, unsigned ev, unsigned b)
+  {
+    return (reinterpret_cast<const uint16_t*>(in.sizes) + in.sizes[b])[ev];
+  }
+  __device__ __forceinline__ unsigned mep_bank_type(const RawInput& in, unsigned ev, unsigned b)
+  {
+    return (reinterpret_cast<const uint8_t*>(in.types) + in.types[b])[ev];
+  }
 
   __device__ __forceinline__ const uint16_t* bank_sizes(const RawInput& in, unsigned event)
   {

@@ -79,6 +79,13 @@ namespace velo {
     unsigned& n_words,
     unsigned& staged_bytes)
   {
+    staged_bytes = 0;
+    if (in.mep_layout) {
+      // the event's banks are scattered over the MEP: read in place
+      n_words = 0xFFFFFFFFu;
+      __syncthreads();
+      return reinterpret_cast<const uint32_t*>(in.raw);
+    }
     const unsigned begin = in.offsets[ev];
     const unsigned end = in.offsets[ev + 1];
     n_words = (end - begin) / 4;
@@ -89,7 +96,6 @@ namespace velo {
     const uintptr_t e_al = e & ~uintptr_t(15);
     const unsigned need = static_cast<unsigned>(((e + 15) & ~uintptr_t(15)) - s_al);
     const bool base_aligned = (reinterpret_cast<uintptr_t>(in.raw) & 15u) == 0;
-    staged_bytes = 0;
     if (!base_aligned || need > smem_blob_bytes) {
       __syncthreads();
       return reinterpret_cast<const uint32_t*>(src);
@@ -143,6 +149,65 @@ namespace velo {
     return (version == 2 || version == 3) ? (source_id & 0x1FFu) / 8 : ((source_id & 0x1FFu) << 1) / 8;
   }
 
+  // MEP layout: the same table, with word offsets relative to the start of `raw` (the words
+  // pointer stage_event returns).  A fragment must start on a 4-byte boundary; its word count
+  // is clamped to the bank size.  Ends with a __syncthreads().
+  __device__ void parse_banks_mep(const RawInput& in, unsigned ev, BankTable& bt, unsigned* warp_sums, unsigned* status)
+  {
+    const bool v23 = in.bank_version == 2 || in.bank_version == 3;
+    const unsigned n_banks_raw = mep_n_banks(in);
+    const unsigned n_banks = n_banks_raw < max_banks ? n_banks_raw : max_banks;
+    if (n_banks_raw > max_banks && threadIdx.x == 0) set_error(status, err_input_capacity);
+    const uint32_t* raw32 = reinterpret_cast<const uint32_t*>(in.raw);
+    unsigned carry = 0, count = 0;
+    for (unsigned base = 0; base < n_banks; base += blockDim.x) {
+      const unsigned b = base + threadIdx.x;
+      unsigned nsp_flat = 0;
+      if (b < n_banks) {
+        const unsigned frag = mep_fragment_offset(in, ev, b);
+        const unsigned size = mep_bank_size(in, ev, b);
+        const unsigned type = mep_bank_type(in, ev, b);
+        const bool velo_bank = type == bank_type_vp || type == bank_type_velo;
+        unsigned nsp = 0, first = 0;
+        if (frag & 3u) {
+          set_error(status, err_input_capacity);
+        }
+        else if (v23) {
+          nsp = size >= 4 ? raw32[frag / 4] : 0u;
+          first = frag / 4 + 1;
+          if (velo_bank) count += nsp;
+          if (nsp > (size >= 4 ? size / 4 - 1 : 0u)) {
+            set_error(status, err_input_capacity);
+            nsp = size >= 4 ? size / 4 - 1 : 0u;
+          }
+        }
+        else {
+          nsp = size / 4u;
+          first = frag / 4;
+          if (velo_bank) count += nsp;
+        }
+        bt.words_off[b] = first;
+        bt.n_sp[b] = nsp;
+        bt.source_id[b] = mep_source_id(in, b);
+        bt.velo[b] = velo_bank;
+        nsp_flat = velo_bank ? nsp : 0u;
+      }
+      unsigned total;
+      const unsigned excl = block_exclusive_scan(nsp_flat, warp_sums, &total);
+      if (b < n_banks) bt.flat[b] = carry + excl;
+      carry += total;
+    }
+    unsigned total_count;
+    block_exclusive_scan(count, warp_sums, &total_count);
+    if (threadIdx.x == 0) {
+      bt.n_banks = n_banks;
+      bt.total_sp = carry;
+      bt.flat[n_banks] = carry;
+      bt.count_total = total_count;
+    }
+    __syncthreads();
+  }
+
   // Fills the table; ends with a __syncthreads().
   __device__ void parse_banks(
     const RawInput& in,
@@ -154,6 +219,10 @@ namespace velo {
     unsigned* status)
   {
     const bool v23 = in.bank_version == 2 || in.bank_version == 3;
+    if (in.mep_layout) {
+      parse_banks_mep(in, ev, bt, warp_sums, status);
+      return;
+    }
     const unsigned n_banks_raw = n_words > 0 ? words[0] : 0u;
     const unsigned n_banks = n_banks_raw < max_banks ? n_banks_raw : max_banks;
     if (n_banks_raw > max_banks && threadIdx.x == 0) set_error(status, err_input_capacity);
@@ -690,8 +759,8 @@ namespace velo {
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
     const uint32_t key_mask = sp_key_mask(version);
     uint32_t* sorted = nullptr;
-    if (staged > 0 && staged + 4 * bt.total_sp <= p.smem_blob_bytes) {
-      sorted = reinterpret_cast<uint32_t*>(blob + staged);
+    if (staged + 4 * bt.total_sp <= p.smem_blob_bytes) {
+      sorted = reinterpret_cast<uint32_t*>(blob + staged); // behind the staged event, or at the start
       sort_bank_words(bt, words, sorted, key_mask);
     }
 
@@ -884,6 +953,12 @@ namespace velo {
       const unsigned bytes = in.offsets[e + in.event_start + 1] - in.offsets[e + in.event_start];
       return classes - 1 - min(bytes / 64u, classes - 1); // descending size
     };
+    if (in.mep_layout) {
+      // no per-event blob sizes in a MEP: keep the events in order
+      for (unsigned e = threadIdx.x; e < in.n_events; e += blockDim.x)
+        order[e] = e;
+      return;
+    }
     for (unsigned e = threadIdx.x; e < in.n_events; e += blockDim.x)
       atomicAdd(&count[size_class(e)], 1u);
     __syncthreads();

@@ -220,7 +220,7 @@ VeloStatus velo_decode_noalloc(
 
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   const unsigned n = s->n_events;
-  RawInput in {s->raw, s->offsets, s->sizes, s->types, s->event_start, s->n_events, s->bank_version};
+  RawInput in {s->raw, s->offsets, s->sizes, s->types, s->event_start, s->n_events, s->bank_version, s->mep_layout};
   auto* bank_index = reinterpret_cast<unsigned long long*>(scratch + off_bank_index);
   auto* status = reinterpret_cast<unsigned*>(scratch + off_status);
   auto* estimated = reinterpret_cast<unsigned*>(scratch + off_estimated);

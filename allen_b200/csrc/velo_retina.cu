@@ -29,8 +29,25 @@ namespace velo {
     const uint32_t* word;
   };
 
+  __device__ __forceinline__ unsigned retina_n_banks(const RawInput& in, unsigned ev)
+  {
+    return in.mep_layout ? mep_n_banks(in) : reinterpret_cast<const uint32_t*>(in.raw + in.offsets[ev])[0];
+  }
+
   __device__ __forceinline__ RetinaBank retina_bank(const RawInput& in, unsigned ev, unsigned b)
   {
+    const bool v23 = in.bank_version == 2 || in.bank_version == 3;
+    if (in.mep_layout) {
+      // MEPTools.h:55-205: the fragment starts with the bank data (no sourceID word)
+      RetinaBank r;
+      const uint32_t* frag = reinterpret_cast<const uint32_t*>(in.raw + mep_fragment_offset(in, ev, b));
+      r.source_id = mep_source_id(in, b);
+      r.count = v23 ? frag[0] : 0u;
+      r.word = frag + (v23 ? 1 : 0);
+      r.size = mep_bank_size(in, ev, b);
+      r.type = mep_bank_type(in, ev, b);
+      return r;
+    }
     const char* blob = in.raw + in.offsets[ev];
     const uint32_t* w = reinterpret_cast<const uint32_t*>(blob);
     const unsigned n_banks = w[0];
@@ -38,7 +55,6 @@ namespace velo {
     const uint32_t* bank = reinterpret_cast<const uint32_t*>(payload + w[1 + b]);
     RetinaBank r;
     r.source_id = bank[0];
-    const bool v23 = in.bank_version == 2 || in.bank_version == 3;
     r.count = v23 ? bank[1] : 0u;
     r.word = bank + (v23 ? 2 : 1);
     r.size = bank_sizes(in, ev)[b];
@@ -56,7 +72,7 @@ namespace velo {
     for (unsigned s = threadIdx.x; s < per_event; s += blockDim.x)
       size[s] = 0;
     __syncthreads();
-    const unsigned n_banks = reinterpret_cast<const uint32_t*>(p.in.raw + p.in.offsets[ev])[0];
+    const unsigned n_banks = retina_n_banks(p.in, ev);
     for (unsigned b = threadIdx.x; b < n_banks; b += blockDim.x) {
       const RetinaBank bank = retina_bank(p.in, ev, b);
       if (bank.type == bank_type_vp_retina) {
@@ -128,7 +144,7 @@ namespace velo {
   __device__ __forceinline__ bool
   cluster_word(const RetinaParams& p, unsigned ev, unsigned s, unsigned index, RetinaBank& bank, uint32_t& w)
   {
-    const unsigned n_banks = reinterpret_cast<const uint32_t*>(p.in.raw + p.in.offsets[ev])[0];
+    const unsigned n_banks = retina_n_banks(p.in, ev);
     const unsigned b = p.bank_index[s];
     if (b >= n_banks) {
       set_error(p.status, err_input_capacity);

@@ -12,6 +12,13 @@ main/include/MEPTools.h:26-53):
                the u16 payload size of every bank;
 * ``types``    u32[N + 1] offsets in u8 units from the array start, followed by
                the u8 bank type of every bank (VP = 63, Velo = 8).
+
+The MEP layout (``mep = True``; readers in main/include/MEPTools.h:55-205) keeps the
+banks of one source together: ``offsets`` = [n_banks, n_events, source_id[n_banks],
+then for each event the byte offset in ``raw`` of its fragment of every bank];
+``sizes`` and ``types`` start with one u32 offset per bank (u16 and u8 units)
+followed by that bank's per-event sizes and types.  A fragment is the bank data
+without the sourceID word.
 """
 from __future__ import annotations
 
@@ -31,9 +38,12 @@ class RawSlice:
     sizes: np.ndarray    # uint32
     types: np.ndarray    # uint32
     bank_version: int
+    mep: bool = False    # MEP layout (banks of one source together)
 
     @property
     def n_events(self) -> int:
+        if self.mep:
+            return int(self.offsets[1])
         return int(self.offsets.shape[0] - 1)
 
     @property
@@ -42,6 +52,10 @@ class RawSlice:
         if self.n_events == 0:
             return False
         t8 = self.types.view(np.uint8)
+        if self.mep:
+            n_banks = int(self.offsets[0])
+            return bool(any(np.any(t8[int(self.types[b]):int(self.types[b]) + self.n_events] == BANK_TYPE_VP_RETINA)
+                            for b in range(n_banks)))
         first, last = int(self.types[0]), int(self.types[1]) if self.n_events > 1 else t8.size
         return bool(np.any(t8[first:first + max(last - first, 0)] == BANK_TYPE_VP_RETINA))
 
@@ -114,6 +128,15 @@ def super_pixels_per_event(s: RawSlice) -> np.ndarray:
     s16 = s.sizes.view(np.uint16)
     t8 = s.types.view(np.uint8)
     out = np.zeros(n, dtype=np.int64)
+    if s.mep:
+        for b in range(int(s.offsets[0])):
+            sz = s16[int(s.sizes[b]):int(s.sizes[b]) + n].astype(np.int64)
+            ty = t8[int(s.types[b]):int(s.types[b]) + n]
+            words = np.where((ty == BANK_TYPE_VP) | (ty == BANK_TYPE_VELO) | (ty == BANK_TYPE_VP_RETINA), sz // 4, 0)
+            if s.bank_version in (2, 3):
+                words = np.maximum(words - 1, 0)
+            out += words
+        return out
     starts = s.sizes[:n + 1].astype(np.int64)
     tstarts = s.types[:n + 1].astype(np.int64)
     for e in range(n):
@@ -125,3 +148,36 @@ def super_pixels_per_event(s: RawSlice) -> np.ndarray:
             words = np.maximum(words - 1, 0)
         out[e] = words.sum()
     return out
+
+
+def to_mep(s: RawSlice) -> RawSlice:
+    """The same events in the MEP layout.  Every event must have the same banks (sources) in
+    the same order, as a MEP's events do."""
+    assert not s.mep
+    n = s.n_events
+    per_event = [banks_of_event(s, e) for e in range(n)]
+    n_banks = len(per_event[0]) if n else 0
+    assert all(len(b) == n_banks and [x[1] for x in b] == [x[1] for x in per_event[0]] for b in per_event)
+    offsets = np.zeros(2 + n_banks * (n + 1), dtype=np.uint32)
+    offsets[0], offsets[1] = n_banks, n
+    chunks, pos = [], 0
+    for b in range(n_banks):
+        offsets[2 + b] = per_event[0][b][1]
+        for e in range(n):
+            payload = per_event[e][b][2]
+            offsets[2 + n_banks * (1 + e) + b] = pos
+            data = payload + b"\0" * ((-len(payload)) % 4)
+            chunks.append(data)
+            pos += len(data)
+    raw = np.frombuffer(b"".join(chunks), dtype=np.uint8).copy() if chunks else np.zeros(0, np.uint8)
+    s16 = np.zeros(2 * n_banks + n_banks * n + 2, dtype=np.uint16)
+    t8 = np.zeros(4 * n_banks + n_banks * n + 4, dtype=np.uint8)
+    for b in range(n_banks):
+        so, to = 2 * n_banks + b * n, 4 * n_banks + b * n
+        s16.view(np.uint32)[b] = so
+        t8.view(np.uint32)[b] = to
+        s16[so:so + n] = [len(per_event[e][b][2]) for e in range(n)]
+        t8[to:to + n] = [per_event[e][b][0] for e in range(n)]
+    sizes = np.frombuffer(s16.tobytes() + b"\0" * ((-s16.nbytes) % 4), dtype=np.uint32).copy()
+    types = np.frombuffer(t8.tobytes() + b"\0" * ((-t8.nbytes) % 4), dtype=np.uint32).copy()
+    return RawSlice(raw, offsets, sizes, types, s.bank_version, mep=True)

@@ -66,6 +66,9 @@ typedef struct {
   unsigned event_start;     /* first event of the slice (RuntimeOptions::event_interval) */
   unsigned n_events;
   int bank_version;         /* host_raw_bank_version: 2, 3 or 4 */
+  int mep_layout;           /* RuntimeOptions::mep_layout: 1 = MEP layout (main/include/MEPTools.h:55-205):
+                               offsets = [n_banks, n_events, source ids, per event the fragment offset
+                               of every bank]; sizes and types indexed by bank, then event */
 } VeloDeviceSlice;
 
 /* The same slice on the host (page-locked memory gives asynchronous copies). */

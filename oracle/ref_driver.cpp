@@ -146,7 +146,7 @@ namespace {
     }
   }
 
-  template<int V>
+  template<int V, bool MEP>
   Result* run_chain(const VeloCpuInput& in)
   {
     auto* r = new Result;
@@ -191,7 +191,7 @@ namespace {
         p.dev_velo_retina_raw_input_types = sp<const unsigned>(in.raw_types, big);
         p.dev_retina_bank_index = sp<unsigned>(retina_bank_index, per_event);
         p.dev_each_sensor_pair_size = sp<unsigned>(pair_size, size_t(n) * per_event);
-        if (bank_version >= 0) launch(n, [&] { calculate_number_of_retinaclusters_each_sensor_pair_kernel<V, false>(p, start); });
+        if (bank_version >= 0) launch(n, [&] { calculate_number_of_retinaclusters_each_sensor_pair_kernel<V, MEP>(p, start); });
       }
       total_clusters = prefix_sum(*r, "dev_offsets_each_sensor_pair_size", pair_size, size_t(n) * per_event);
       const unsigned* pair_offsets = static_cast<unsigned*>(r->buffers["dev_offsets_each_sensor_pair_size"].p);
@@ -223,9 +223,9 @@ namespace {
         const unsigned size = n * 26;
         const unsigned block = Velo::Tracking::block_dim_x_populate_module_pair_offsets_and_sizes;
         launch((size + block - 1) / block, [&] { populate_module_pair_offsets_and_sizes<V>(p, size); });
-        launch(n, [&] { velo_calculate_sorting_key<V, false>(p, start, &geometry, zero_num.data()); });
-        launch(n, [&] { velo_calculate_permutations<false>(p, zero_num.data()); });
-        launch(n, [&] { decode_retinaclusters_sorted<V, false>(p, start, &geometry); });
+        launch(n, [&] { velo_calculate_sorting_key<V, MEP>(p, start, &geometry, zero_num.data()); });
+        launch(n, [&] { velo_calculate_permutations<MEP>(p, zero_num.data()); });
+        launch(n, [&] { decode_retinaclusters_sorted<V, MEP>(p, start, &geometry); });
       }
       offsets_est = offsets_mp;
     }
@@ -245,7 +245,7 @@ namespace {
         p.dev_number_of_candidates = sp<unsigned>(n_candidates, n);
         p.dev_velo_bank_index = sp<unsigned>(bank_index, Velo::Constants::n_modules * 4);
         if (bank_version >= 0) {
-          launch((n + 255) / 256, [&] { velo_calculate_number_of_candidates_kernel<V, false>(p, n, start); });
+          launch((n + 255) / 256, [&] { velo_calculate_number_of_candidates_kernel<V, MEP>(p, n, start); });
         }
       }
 
@@ -272,7 +272,7 @@ namespace {
         p.dev_module_candidate_num = sp<unsigned>(candidate_num, n);
         p.dev_cluster_candidates = sp<unsigned>(candidates, total_candidates);
         if (bank_version >= 0) {
-          launch(n, [&] { velo_estimate_input_size_kernel<V, false>(p, start); });
+          launch(n, [&] { velo_estimate_input_size_kernel<V, MEP>(p, start); });
         }
       }
 
@@ -304,7 +304,7 @@ namespace {
         p.dev_velo_clusters = sp<Velo::Clusters>(clusters_views.data(), n);
         if (bank_version >= 0) {
           launch(n, [&] {
-            velo_masked_clustering_kernel<V, false>(
+            velo_masked_clustering_kernel<V, MEP>(
               p, start, &geometry, sp_patterns.data(), sp_fx.data(), sp_fy.data());
           });
         }
@@ -513,10 +513,11 @@ extern "C" {
 
 void* velo_ref_run(const VeloCpuInput* in)
 {
+  const bool mep = in->mep_layout != 0;
   switch (in->bank_version) {
-  case 3: return run_chain<3>(*in);
-  case 4: return run_chain<4>(*in);
-  default: return run_chain<2>(*in);
+  case 3: return mep ? run_chain<3, true>(*in) : run_chain<3, false>(*in);
+  case 4: return mep ? run_chain<4, true>(*in) : run_chain<4, false>(*in);
+  default: return mep ? run_chain<2, true>(*in) : run_chain<2, false>(*in);
   }
 }
 

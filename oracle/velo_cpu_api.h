@@ -47,6 +47,9 @@ typedef struct {
   /* 0: super-pixel banks (VP, type 63) through velo_masked_clustering; 1: retina-cluster
    * banks (VPRetinaCluster, type 73) through decode_retinaclusters (velo_reconstruction.py:18-71) */
   int retina_decoding;
+  /* 1: the four raw arrays are in the MEP layout (main/include/MEPTools.h:55-205); only the
+   * reference build (velo_ref_) reads it, the restatement (velo_oracle_) refuses it */
+  int mep_layout;
 } VeloCpuInput;
 
 #ifdef __cplusplus

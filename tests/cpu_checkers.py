@@ -45,6 +45,7 @@ class VeloCpuInput(C.Structure):
         ("phi_tolerance", C.c_float), ("max_scatter", C.c_float),
         ("max_skipped_modules", C.c_uint), ("max_chi2", C.c_float),
         ("beamline_x", C.c_float), ("beamline_y", C.c_float), ("retina_decoding", C.c_int),
+        ("mep_layout", C.c_int),
     ]
 
 
@@ -82,12 +83,14 @@ class Checker:
             event_start, s.n_events - event_start if n_events is None else n_events,
             s.bank_version, keep[4].ctypes.data, len(geometry),
             phi_tolerance, max_scatter, max_skipped_modules, max_chi2, beamline[0], beamline[1],
-            int(retina if retina is not None else getattr(s, "retina", False)))
+            int(retina if retina is not None else getattr(s, "retina", False)), int(getattr(s, "mep", False)))
         return inp, keep
 
     def run(self, s, geometry: bytes, **kw) -> dict:
         inp, keep = self.make_input(s, geometry, **kw)
         h = self._run(C.byref(inp))
+        if not h:
+            raise ValueError(f"{self.kind} checker refused the input (MEP layout?)")
         try:
             out = {}
             for name in list(DTYPES) + U32_BUFFERS:

@@ -177,3 +177,16 @@ def test_retina_front_end(chain, oracle, geometry, version):
     s = generator.generate(30, seed=3).raw
     totals, out = run_chain(chain, s)
     assert parity.compare(out, oracle.run(s, geometry), s.n_events) == []
+
+
+@pytest.mark.parametrize("cfg", [dict(), dict(bank_version=4), dict(raw_format=1, bank_version=3)])
+def test_mep_layout(chain, oracle, geometry, cfg):
+    """The same events in the MEP layout (banks of one source together, MEPTools.h) give the
+    Allen-layout results bit for bit, for super-pixel and retina banks."""
+    from allen_b200 import rawbanks
+    g = generator.generate(80, seed=66, pileup_min=1.0, pileup_max=15.0, **cfg)
+    m = rawbanks.to_mep(g.raw)
+    assert m.mep and m.n_events == g.raw.n_events
+    totals, out = run_chain(chain, m, use_graph=True)
+    assert totals["device_flags"] == 0
+    assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []

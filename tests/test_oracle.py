@@ -84,3 +84,15 @@ def test_kalman_filter_matches_reference_build(oracle, geometry, beamline):
     written = parity.kalman_written_words(reco)
     for k in ("dev_velo_kalman_beamline_states", "dev_velo_kalman_endvelo_states"):
         assert np.array_equal(a[k].view(np.uint32)[written], b[k].view(np.uint32)[written]), k
+
+
+@pytest.mark.parametrize("cfg", [dict(), dict(bank_version=4), dict(raw_format=1, bank_version=3)])
+def test_mep_layout_in_reference_build(geometry, cfg):
+    """The reference's own mep_layout kernels on our MEP transpose give its Allen-layout results:
+    pins rawbanks.to_mep (the layout the GPU kernels read) against MEPTools.h."""
+    if not cpu_checkers.available("ref"):
+        pytest.skip("oracle/_ref not built")
+    from allen_b200 import rawbanks
+    ref = cpu_checkers.load("ref")
+    g = generator.generate(10, seed=4, **cfg)
+    assert parity.compare(ref.run(rawbanks.to_mep(g.raw), geometry), ref.run(g.raw, geometry), g.raw.n_events) == []
