@@ -16,6 +16,7 @@ from __future__ import annotations
 import numpy as np
 
 MIN_WEIGHT = 0.7
+ID_MASK = 0xF3FFFFFF  # clears the retina fraction bits (VPChannelID orfx/orfy, bits 27 and 26)
 
 
 def hit_owner_tables(gen):
@@ -35,7 +36,7 @@ def match_tracks(tracks_ids, table):
     ids, owner = table
     out = []
     for t in tracks_ids:
-        a = np.asarray(t, dtype=np.uint32)
+        a = np.asarray(t, dtype=np.uint32) & np.uint32(ID_MASK)
         pos = np.searchsorted(ids, a)
         pos = np.minimum(pos, max(ids.size - 1, 0))
         found = (ids.size > 0) & (ids[pos] == a) if ids.size else np.zeros(a.size, bool)
@@ -88,3 +89,47 @@ def tracks_from_outputs(out: dict) -> list:
     ids = hits[:4 * th].view(np.uint32)
     return [[tuple(ids[off_hn[t]:off_hn[t + 1]]) for t in range(int(off_all[e]), int(off_all[e + 1]))]
             for e in range(off_all.size - 1)]
+
+
+class DeviceTruth:
+    """Generator truth on the GPU for velo_validate_tracks: per event sorted truth-pixel ids
+    with their owning particle, and per particle the reconstructible flag (hits on at least
+    3 modules, 2 < eta < 5)."""
+
+    def __init__(self, gen):
+        import torch
+        tables = hit_owner_tables(gen)
+        ids = np.concatenate([t[0] for t in tables]) if tables else np.zeros(0, np.uint32)
+        owner = np.concatenate([t[1] for t in tables]) if tables else np.zeros(0, np.uint32)
+        offs = np.zeros(len(tables) + 1, np.uint32)
+        offs[1:] = np.cumsum([t[0].size for t in tables])
+        parts = gen.particles
+        recoble = ((parts["n_modules"] >= 3) & (parts["eta"] > 2) & (parts["eta"] < 5)).astype(np.uint8)
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+        self.n_events = len(tables)
+        self.n_particles = int(parts.size)
+        self.truth_offsets = dev(offs.view(np.int32))
+        self.truth_ids = dev(ids.astype(np.uint32).view(np.int32))
+        self.truth_owner = dev(owner.astype(np.uint32).view(np.int32))
+        self.particle_offsets = dev(np.asarray(gen.particle_offsets, np.uint32).view(np.int32))
+        self.reconstructible = dev(recoble)
+        self.matched = torch.zeros(max(self.n_particles, 1), dtype=torch.int32, device="cuda")
+        self.counts = torch.zeros(5, dtype=torch.int64, device="cuda")
+
+
+def evaluate_device(chain, truth: DeviceTruth) -> dict:
+    """The counts of evaluate(), computed on the GPU from the chain's last run (no track copies)."""
+    import ctypes as C
+    from .chain import _check, _current_stream
+    p = chain.device_outputs()
+    lib = chain.lib
+    lib.velo_validate_tracks.restype = C.c_int
+    lib.velo_validate_tracks.argtypes = [C.c_uint] + [C.c_void_p] * 8 + [C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p]
+    _check(lib, lib.velo_validate_tracks(
+        truth.n_events, p["dev_offsets_all_velo_tracks"], p["dev_offsets_velo_track_hit_number"],
+        p["dev_velo_track_hits"], truth.truth_offsets.data_ptr(), truth.truth_ids.data_ptr(),
+        truth.truth_owner.data_ptr(), truth.particle_offsets.data_ptr(), truth.reconstructible.data_ptr(),
+        truth.n_particles, truth.matched.data_ptr(), truth.counts.data_ptr(), _current_stream()))
+    t, g, rb, r, c = (int(v) for v in truth.counts.cpu().numpy())
+    return {"tracks": t, "ghosts": g, "ghost_rate": g / max(t, 1), "reconstructible": rb, "reconstructed": r,
+            "efficiency": r / max(rb, 1), "clones": c, "clone_rate": c / max(r + c, 1)}

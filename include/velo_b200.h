@@ -278,6 +278,31 @@ VeloStatus velo_kalman_filter(
   unsigned* dev_status,
   VeloStream stream);
 
+/* On-device VELO validation (host/validators/src/HostVeloValidator.cpp:9-30 with
+ * checker/tracking/src/PrepareTracks.cpp and TrackChecker.h:180-320 run on the host in the
+ * reference): efficiency, ghost and clone counts of the consolidated tracks against Monte Carlo
+ * truth, computed on the GPU.  Truth per event: LHCb ids of the truth pixels sorted ascending
+ * (dev_truth_ids [truth_offsets[N]]) with the owning particle's index within the event
+ * (dev_truth_owner), and per particle a reconstructible flag (dev_particle_reconstructible,
+ * particle_offsets [N + 1]).  dev_matched_scratch holds n_particles u32 (zeroed here);
+ * dev_counts receives 5 u64: tracks, ghosts, reconstructible, reconstructed, clones.  Rules: a
+ * track matches the particle owning >= 70 % of its hits (ties to the lower index), unmatched
+ * tracks are ghosts, further matches of a particle are clones.  Allocates nothing. */
+VeloStatus velo_validate_tracks(
+  unsigned n_events,
+  const unsigned* dev_offsets_all_velo_tracks,
+  const unsigned* dev_offsets_velo_track_hit_number,
+  const char* dev_velo_track_hits,
+  const unsigned* dev_truth_offsets,
+  const unsigned* dev_truth_ids,
+  const unsigned* dev_truth_owner,
+  const unsigned* dev_particle_offsets,
+  const uint8_t* dev_particle_reconstructible,
+  unsigned n_particles,
+  unsigned* dev_matched_scratch,
+  unsigned long long* dev_counts,
+  VeloStream stream);
+
 /* Learned seed pruner (no counterpart in the reference).  A 12-32-32-1 network scores each
  * (h0, h1) doublet of the flat seeding (SearchByTriplet.cu:298-446) before its h2 window is
  * scanned; doublets whose logit is not above threshold_logit are not scanned.  An event whose
