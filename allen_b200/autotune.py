@@ -18,7 +18,7 @@ import os
 import time
 
 SEARCH_VARIANTS = [(128, 1), (128, 2), (256, 1), (256, 2), (256, 4), (512, 2), (512, 4), (128, 0), (256, 0), (512, 0)]
-SEARCH_CAPACITIES = [2048, 2560, 3072, 3584, 4096, 5120]
+SEARCH_CAPACITIES = [0, 1024, 2048, 2560, 3072, 4096]
 CLUSTER_CAPACITIES = [0, 1024, 2048, 2560, 3072]
 CLUSTER_BLOBS = [16 * 1024, 24 * 1024, 32 * 1024, 40 * 1024]
 ESTIMATE_BLOBS = [24 * 1024, 32 * 1024, 48 * 1024]

@@ -897,8 +897,12 @@ namespace velo {
   // One instantiation per (block size, lanes per seed); the chain launches the one its
   // launch configuration names (autotuned).  Events whose hits fit the shared-memory
   // capacity run the shared-memory body, the others the global-scratch body.
+  // Flat-seeding kernels are register-capped for five 256-thread CTAs per SM (51 registers):
+  // with the hits staged through L2 (search_hit_capacity 0) shared memory no longer limits
+  // the CTAs per SM, and the extra resident events hide more latency than the few spills cost
+  // (1.40M against 1.29M events/s at four CTAs per SM, measured).
   template<unsigned THREADS, unsigned LPH>
-  __global__ void __launch_bounds__(THREADS) search_by_triplet_kernel(SearchParams p)
+  __global__ void __launch_bounds__(THREADS, LPH == 0 ? 1280 / THREADS : 1) search_by_triplet_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ std::conditional_t<LPH == 0, SearchSharedFlat, SearchShared> s;
