@@ -930,7 +930,9 @@ namespace velo {
     }
   }
 
-  __global__ void __launch_bounds__(decode_threads) cluster_sort_kernel(ClusterSortParams p)
+  // Capped for six CTAs per SM (42 registers, no spills): with the clusters staged through L2
+  // (cluster_stage_capacity 0) shared memory allows that many (measured +10 % on the chain).
+  __global__ void __launch_bounds__(decode_threads, 6) cluster_sort_kernel(ClusterSortParams p)
   {
     __shared__ __align__(8) uint64_t bar;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
