@@ -1005,7 +1005,7 @@ VeloStatus velo_chain_set_seed_model(VeloChain* c, const VeloSeedModel* model)
   c->release_graph();
   if (!model) {
     c->learned = false;
-    return VELO_OK;
+    return configure_kernels(c); // the persistent grid follows the kernel the chain launches
   }
   if (!learned_search_kernel(c->search_threads))
     return fail(VELO_ERR_ARGUMENT, "the learned search needs search_threads 128, 256 or 512");
