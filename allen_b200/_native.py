@@ -4,6 +4,7 @@
   include/velo_b200.h.  There is no CPU fallback: when this library cannot be
   loaded every GPU entry point raises.
 * ``_lib/libvelo_gen.so``  - the host-only synthetic event generator.
+* ``_lib/libvelo_io.so``   - the host-only MDF index and VELO transpose of include/velo_io.h.
 """
 from __future__ import annotations
 
@@ -15,6 +16,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_DIR = os.path.join(PKG, "_lib")
 CHAIN_LIB = os.path.join(LIB_DIR, "libvelo_b200.so")
 GEN_LIB = os.path.join(LIB_DIR, "libvelo_gen.so")
+IO_LIB = os.path.join(LIB_DIR, "libvelo_io.so")
 GEOMETRY = os.path.join(PKG, "data", "velo_geometry.bin")
 
 _lock = threading.Lock()
@@ -42,6 +44,11 @@ def load_chain():
 def load_generator():
     from . import build
     return _load(GEN_LIB, build.build_generator)
+
+
+def load_io():
+    from . import build
+    return _load(IO_LIB, build.build_io)
 
 
 TUNED_CONFIG = os.path.join(PKG, "data", "launch_config.json")

@@ -1,6 +1,6 @@
 """In-tree build of the native parts (no JIT cache, so the built files travel with the tree).
 
-    python -m allen_b200.build            # chain (nvcc, sm_100a) + generator (g++)
+    python -m allen_b200.build            # chain (nvcc, sm_100a) + generator and MDF input (g++)
 
 The CUDA library is compiled for sm_100a only, with -fmad=false: the cluster
 positions, phi values and track fits must round exactly like the reference's
@@ -80,6 +80,18 @@ def build_generator(force: bool = False) -> str:
     return target
 
 
+def build_io(force: bool = False) -> str:
+    """Host-only MDF index and VELO transpose (include/velo_io.h); no CUDA dependency."""
+    os.makedirs(LIB_DIR, exist_ok=True)
+    target = os.path.join(LIB_DIR, "libvelo_io.so")
+    src = os.path.join(CSRC, "velo_io.cpp")
+    if not force and not _stale(target, [src, os.path.join(INCLUDE, "velo_io.h")]):
+        return target
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-pthread", "-Wall", "-I", INCLUDE, "-o", target, src]
+    subprocess.run(cmd, check=True)
+    return target
+
+
 def build_oracle(ref_root: str | None = "/root/reference") -> None:
     """Test infrastructure: the plain-C oracle, and the reference CPU build when its tree exists."""
     oracle = os.path.join(REPO, "oracle")
@@ -90,6 +102,7 @@ def build_oracle(ref_root: str | None = "/root/reference") -> None:
 
 def main():
     build_generator(force="--force" in sys.argv)
+    build_io(force="--force" in sys.argv)
     build_chain(force="--force" in sys.argv, verbose="-v" in sys.argv)
 
 

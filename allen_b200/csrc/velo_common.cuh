@@ -12,6 +12,7 @@
 // phi values and fits are bit-identical to the reference CPU build.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -39,6 +40,7 @@ namespace velo {
     err_output_capacity = 1u << 5,   // consolidated output larger than the reserved buffer
     err_input_capacity = 1u << 6,    // slice larger than the reserved workspace
     err_hits_per_event = 1u << 7,    // more than 65535 estimated hits in one event (u16 indices)
+    err_bad_super_pixel = 1u << 8,   // a candidate's flood fill found no pixel (bank index names another bank)
   };
 
   // Detector description and super-pixel lookup tables, one copy in global memory
@@ -52,6 +54,23 @@ namespace velo {
     float sp_fx[512];
     float sp_fy[512];
   };
+
+  // Pixel-column lookups.  The tables sit in the same order as in the reference's geometry
+  // struct (VeloGeometry, ClusteringDefinitions.cuh:154-161: module z, local x, x pitch,
+  // ltg), so a column beyond the sensor's 768 - from a malformed bank, or retina words
+  // decoded with another bank version - reads on into the next table exactly as the
+  // reference does.  Super-pixel and retina columns stay below 1026; the clamps keep even a
+  // larger one inside the struct.
+  __device__ __forceinline__ float column_local_x(const Geometry* g, uint32_t cx)
+  {
+    const float* flat = reinterpret_cast<const float*>(g) + offsetof(Geometry, local_x) / sizeof(float);
+    return __ldg(flat + min(cx, 2 * n_cols - 1));
+  }
+  __device__ __forceinline__ float column_x_pitch(const Geometry* g, uint32_t cx)
+  {
+    const float* flat = reinterpret_cast<const float*>(g) + offsetof(Geometry, x_pitch) / sizeof(float);
+    return __ldg(flat + min(cx, n_cols + 12 * n_sensors - 1));
+  }
 
   // Scalars computed once on the host (IEEE single precision, as the reference's
   // constexpr values and properties), passed by value to the kernels.

@@ -567,7 +567,8 @@ namespace velo {
     const uint32_t* sorted_words,
     unsigned n_sp,
     int version,
-    ClusterOut& o)
+    ClusterOut& o,
+    bool& bad)
   {
     const uint32_t sp_index = candidate >> 11;
     const uint32_t sensor_number = (candidate >> 3) & 0xFFu;
@@ -638,13 +639,20 @@ namespace velo {
              !(cl.pixels & 0x0001000100010001ull);
     }
     if (!keep) return false;
+    // A candidate whose bank index names another bank (the reference's lookup of the bank by
+    // sensor, when a slice holds more than one bank per sensor) can leave the start pixel
+    // outside the map: no pixel, and the reference divides by zero.
+    if (n == 0) {
+      bad = true;
+      return false;
+    }
     const uint32_t cx = x / n;
     const uint32_t cy = y / n;
     const float fx = __fdiv_rn(__uint2float_rn(x), __uint2float_rn(n)) - __uint2float_rn(cx);
     const float fy = __fdiv_rn(__uint2float_rn(y), __uint2float_rn(n)) - __uint2float_rn(cy);
     const uint32_t chip = cx >> 8;
     o.id = lhcb_id(channel_id(sensor_number, chip, cx & 0xFFu, cy));
-    const float local_x = __ldg(g->local_x + cx) + fx * __ldg(g->x_pitch + cx);
+    const float local_x = column_local_x(g, cx) + fx * column_x_pitch(g, cx);
     const float local_y = (__uint2float_rn(cy) + 0.5f + fy) * 0.055f;
     local_to_global(g, ltg, local_x, local_y, o);
     o.phi = hit_phi_16(k, o.x, o.y);
@@ -679,7 +687,7 @@ namespace velo {
     o.id = lhcb_id(channel_id(sensor_index, chip, cx & 0xFFu, cy));
     const float fx = __ldg(g->sp_fx + sp * 2 + which);
     const float fy = __ldg(g->sp_fy + sp * 2 + which);
-    const float local_x = __ldg(g->local_x + cx) + fx * __ldg(g->x_pitch + cx);
+    const float local_x = column_local_x(g, cx) + fx * column_x_pitch(g, cx);
     const float local_y = (__uint2float_rn(cy) + 0.5f + fy) * 0.055f;
     local_to_global(g, ltg, local_x, local_y, o);
     o.phi = hit_phi_16(k, o.x, o.y);
@@ -848,9 +856,12 @@ namespace velo {
           continue;
         }
         ClusterOut o;
+        bool bad = false;
         const uint32_t* sorted_b2 = sorted && bt.velo[b2] ? sorted + bt.flat[b2] : nullptr;
-        if (rest_of_clusters(g, p.k, candidate, words + bt.words_off[b2], sorted_b2, bt.n_sp[b2], version, o))
+        if (rest_of_clusters(g, p.k, candidate, words + bt.words_off[b2], sorted_b2, bt.n_sp[b2], version, o, bad))
           stage_cluster(o, cand_sensor / 8);
+        else if (bad)
+          set_error(p.status, err_bad_super_pixel);
       }
       __syncthreads();
     }

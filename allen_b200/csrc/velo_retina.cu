@@ -126,9 +126,8 @@ namespace velo {
       or_fy = ((w >> 1) & 0x1u) | (w & 0x1u);
     }
     const unsigned sensor = c.sensor < n_sensors ? c.sensor : 0u;
-    const unsigned col = cx < n_cols ? cx : 0u;
     const float* ltg = g->ltg + 12 * sensor;
-    const float local_x = __ldg(g->local_x + col) + fx * __ldg(g->x_pitch + col);
+    const float local_x = column_local_x(g, cx) + fx * column_x_pitch(g, cx);
     const float local_y = (0.5f + fy) * 0.055f;
     c.x = __ldg(ltg + 0) * local_x + __ldg(ltg + 1) * local_y + __ldg(ltg + 9);
     c.y = __ldg(ltg + 3) * local_x + __ldg(ltg + 4) * local_y + __ldg(ltg + 10);

@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-learned", action="store_true", help="skip the learned-mode measurement")
     p.add_argument("--no-kalman", action="store_true", help="skip the velo_kalman_filter measurement")
     p.add_argument("--no-retina", action="store_true", help="skip the retina-cluster front-end measurement")
+    p.add_argument("--no-mdf", action="store_true", help="skip the host MDF transpose measurement")
     return p.parse_args()
 
 
@@ -182,6 +183,52 @@ def cpu_baseline(slices, geometry, target_s):
             "sample": f"{n_slices * slice_size} events (slices of {slice_size} cycling over the first "
                       f"{s.n_events} events of the workload, one slice per thread at a time), {wall:.1f} s wall; "
                       f"single-thread {rate1:.0f} events/s; CPU: {cpu_model}"}
+
+
+def mdf_measurement(seed: int, n_unique: int = 250, copies: int = 16, repeats: int = 3) -> dict:
+    """Host raw-input path: MDF records to the VELO slice (allen_b200.mdf, all host threads)
+    next to the reference's own transpose (its main/src/Transpose.cpp compiled as CPU C++,
+    one slice on one thread as its MDF provider runs it), on the same stream.  Each record holds
+    a generated event's VELO banks plus 822 banks of other subdetectors (16-300 payload bytes,
+    about 130 KB), the bank count of the 2018 minbias sample beside its VELO banks."""
+    from allen_b200 import generator, mdf, rawbanks
+    rng = np.random.default_rng(seed)
+    g = generator.generate(n_unique, seed=seed + 7).raw
+    events = []
+    for e in range(g.n_events):
+        banks = [(t, g.bank_version, src, p) for (t, src, p) in rawbanks.banks_of_event(g, e)]
+        sizes = rng.integers(16, 301, 822)
+        blob = rng.bytes(int(sizes.sum()))
+        types = rng.choice([9, 13, 21, 22, 32, 33, 64, 66], 822)
+        srcs = rng.integers(0, 2048, 822)
+        at = 0
+        for t, sz, src in zip(types.tolist(), sizes.tolist(), srcs.tolist()):
+            banks.append((t, 0, src, blob[at:at + sz]))
+            at += sz
+        banks.append((16, 7, 0, rng.bytes(40)))
+        order = rng.permutation(len(banks))
+        events.append([banks[i] for i in order])
+    stream = mdf.write_records(events, checksum=False) * copies
+    n = n_unique * copies
+    ev = mdf.scan(stream)
+    threads = os.cpu_count() or 1
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        mdf.transpose_vp(stream, ev, by_source_id=False, n_threads=threads)
+        times.append(time.perf_counter() - t0)
+    ours = n / statistics.median(times)
+    out = {"value": round(ours, 1), "unit": UNIT, "threads": threads,
+           "sample": f"{n} MDF records ({len(stream) / n / 1e3:.0f} KB each: {n_unique} generated events x {copies}), "
+                     f"median of {repeats} transposes into the VELO slice"}
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import cpu_checkers
+    if cpu_checkers.available("ref"):
+        r = cpu_checkers.ref_transpose_vp(stream, n)
+        if r["status"] == 0:
+            out["reference"] = {"value": round(n / r["transpose_seconds"], 1), "unit": UNIT, "threads": 1,
+                                "what": "transpose_events() on one slice, as one thread of its MDF provider"}
+    return out
 
 
 # ----------------------------------------------------------------------------------
@@ -493,6 +540,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(slices, geometry, args.cpu_seconds)
+    mdf_in = None
+    if rank == 0 and not args.no_mdf:
+        mdf_in = mdf_measurement(args.seed)
 
     if rank == 0:
         c0 = counts[0]
@@ -521,6 +571,7 @@ def run_ours(args):
             "learned": learned,
             "kalman": kalman,
             "retina": retina,
+            "mdf": mdf_in,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "device_flags": totals_last["device_flags"],

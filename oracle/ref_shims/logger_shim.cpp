@@ -1,18 +1,18 @@
 // Stand-in for the reference's main/src/Logger.cpp (which needs boost::iostreams):
-// the oracle build logs nothing, so every request goes to a discarding stream.
+// the oracle build logs nothing, so every request goes to a stream without a buffer.  Such a
+// stream is in the bad state, so formatted output returns at once without touching a locale;
+// it is built on first use, after every static initialiser of the library has run.
 #include <ostream>
-#include <streambuf>
 
 namespace logger {
   namespace {
-    struct NullBuffer : std::streambuf {
-      int overflow(int c) override { return c; }
-    };
-    NullBuffer null_buffer;
-    std::ostream null_stream(&null_buffer);
     int level = 0;
   } // namespace
-  std::ostream& logger(int) { return null_stream; }
+  std::ostream& logger(int)
+  {
+    static std::ostream null_stream(nullptr);
+    return null_stream;
+  }
   int verbosity() { return level; }
   void setVerbosity(int l) { level = l; }
 } // namespace logger

@@ -578,6 +578,11 @@ static void rest_of_clusters(
            !popc64(cl.pixels & 0x0001000100010001ull);
   }
   if (!keep) return;
+  /* A candidate whose bank index names another bank (a slice with more than one bank per
+   * sensor, e.g. VP and VPRetinaCluster banks together) can leave the start pixel outside the
+   * map: no pixel, and the reference divides by zero (MaskedVeloClustering.cu:461-462); the
+   * candidate makes no cluster here, as on the GPU. */
+  if (n == 0) return;
   const uint32_t cx = x / n;
   const uint32_t cy = y / n;
   const float fx = (float) x / (float) n - (float) cx;

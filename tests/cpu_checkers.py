@@ -128,3 +128,38 @@ U32_BUFFERS = [
 
 def load(kind: str) -> Checker:
     return Checker(kind)
+
+
+def ref_transpose_vp(stream: bytes, max_events: int, check_checksum: bool = False) -> dict:
+    """The reference's own MDF reader + transpose (oracle/ref_transpose.cpp) on ``stream``:
+    the VP slice it writes, as numpy arrays sized by what it wrote."""
+    path = LIBS["ref"][0]
+    lib = C.CDLL(path)
+    f = lib.ref_transpose_vp
+    f.restype = C.c_int
+    f.argtypes = [C.c_char_p, C.c_size_t, C.c_uint, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p,
+                  C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint), C.POINTER(C.c_uint),
+                  C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    cap = len(stream) + 4096 * (max_events + 1)
+    raw = np.zeros(cap, dtype=np.uint8)
+    offsets = np.zeros(max_events + 1, dtype=np.uint32)
+    words = (len(stream) // 8) + 4 * (max_events + 1)
+    sizes = np.zeros(words, dtype=np.uint32)
+    types = np.zeros(words, dtype=np.uint32)
+    n_ev, n_off, ver, by_src, secs = C.c_uint(0), C.c_uint(0), C.c_int(0), C.c_int(0), C.c_double(0)
+    rc = f(stream, len(stream), max_events, int(check_checksum), raw.ctypes.data, cap, offsets.ctypes.data,
+           sizes.ctypes.data, words, types.ctypes.data, words, C.byref(n_ev), C.byref(n_off), C.byref(ver),
+           C.byref(by_src), C.byref(secs))
+    n = n_ev.value
+    out = {"status": rc, "n_events": n, "n_offsets": n_off.value, "bank_version": ver.value,
+           "by_source_id": bool(by_src.value), "transpose_seconds": secs.value}
+    if rc != 0:
+        return out
+    n_slice = n_off.value - 1  # events the slice holds
+    out["offsets"] = offsets[:n_slice + 1].copy()
+    out["raw"] = raw[:int(offsets[n_slice])].copy()
+    size_words = (4 * (n + 1) + 2 * (int(sizes[n_slice]) - 2 * (n + 1)) + 3) // 4
+    type_words = (4 * (n + 1) + (int(types[n_slice]) - 4 * (n + 1)) + 3) // 4
+    out["sizes"] = sizes[:size_words].copy()
+    out["types"] = types[:type_words].copy()
+    return out

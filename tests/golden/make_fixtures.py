@@ -14,7 +14,16 @@ Outputs:
       reference's outputs for them;
   tests/golden/minbias_retina_10ev.npz
       the VPRetinaCluster banks (type 73, version 3) of the same 10 events, plus the
-      reference's outputs through its retina-cluster decoding and the VELO Kalman filter.
+      reference's outputs through its retina-cluster decoding and the VELO Kalman filter;
+  tests/golden/minbias_mdf_10ev.npz
+      the VELO slice the reference's own MDF reader and transpose (main/src/Transpose.cpp)
+      write for the same file: its VP and VPRetinaCluster banks together, bank version 2,
+      as Allen's MDF provider hands them to the VELO decoding, plus the reference's outputs
+      through the retina-cluster decoding (Allen's default front end) of that slice;
+  tests/golden/mdf_synthetic_8ev.npz
+      two synthetic MDF streams (8 generated events with other subdetectors' banks in
+      shuffled order; source IDs without and with subdetector bits, tests/mdf_streams.py)
+      and the VELO slices the reference's reader and transpose write for them.
 
 The reference outputs come from oracle/_ref/libvelo_ref.so, the reference's VELO
 kernels compiled as CPU C++ (oracle/Makefile).  Usage:
@@ -95,7 +104,13 @@ def main(ref_root, only=()):
     synth = generator.generate(20, seed=7, geometry=geometry, sp_order=0).raw
     retina = rawbanks.build_slice(read_mdf_vp_events(mdf, rawbanks.BANK_TYPE_VP_RETINA, 3), bank_version=3)
 
-    for name, s in (("minbias_vp_10ev", real), ("synthetic_seed7_20ev", synth), ("minbias_retina_10ev", retina)):
+    stream = open(mdf, "rb").read()
+    t = cpu_checkers.ref_transpose_vp(stream, 10, check_checksum=True)
+    assert t["status"] == 0, t
+    provider = rawbanks.RawSlice(t["raw"], t["offsets"], t["sizes"], t["types"], t["bank_version"])
+
+    for name, s in (("minbias_vp_10ev", real), ("synthetic_seed7_20ev", synth), ("minbias_retina_10ev", retina),
+                    ("minbias_mdf_10ev", provider)):
         if only and name not in only:
             continue
         out = ref.run(s, geometry)
@@ -107,6 +122,21 @@ def main(ref_root, only=()):
         print(name, s.n_events, "events;",
               int(out["dev_offsets_all_velo_tracks"][-1]), "tracks;",
               int(out["dev_module_cluster_num"].sum()), "clusters")
+
+    if not only or "mdf_synthetic_8ev" in only:
+        import mdf_streams  # noqa: E402
+        arrays = {}
+        g = generator.generate(8, seed=17, geometry=geometry)
+        for mode, by_source in (("by_type", False), ("by_source", True)):
+            st = mdf_streams.synthetic_stream(g.raw, seed=9, by_source_id=by_source, n_other=30, extra_velo=True)
+            t = cpu_checkers.ref_transpose_vp(st, 8, check_checksum=True)
+            assert t["status"] == 0 and t["by_source_id"] == by_source, t
+            arrays[mode + "__stream"] = np.frombuffer(st, dtype=np.uint8)
+            for k in ("raw", "offsets", "sizes", "types"):
+                arrays[mode + "__" + k] = t[k]
+            arrays[mode + "__bank_version"] = np.array([t["bank_version"]])
+        np.savez_compressed(os.path.join(HERE, "mdf_synthetic_8ev.npz"), **arrays)
+        print("mdf_synthetic_8ev", {k: v.size for k, v in arrays.items()})
 
 
 if __name__ == "__main__":

@@ -6,7 +6,7 @@ import numpy as np
 from allen_b200.rawbanks import RawSlice
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-FIXTURES = ["minbias_vp_10ev", "synthetic_seed7_20ev", "minbias_retina_10ev"]
+FIXTURES = ["minbias_vp_10ev", "synthetic_seed7_20ev", "minbias_retina_10ev", "minbias_mdf_10ev"]
 
 
 def load(name):
