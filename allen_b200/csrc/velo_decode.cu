@@ -415,6 +415,9 @@ namespace velo {
     return pattern_0 || pattern_1;
   }
 
+  constexpr unsigned estimate_queue = 1024; // SPs per chunk of the estimate (and queue entries)
+  static_assert(estimate_queue % decode_threads == 0, "every lane takes the same number of SPs per chunk");
+
   // ------------------------------------------------------------------------------------
   // estimate_kernel: dev_number_of_candidates, dev_velo_bank_index (as a max-reduced
   // key), dev_estimated_input_size and dev_module_candidate_num.
@@ -426,11 +429,14 @@ namespace velo {
     __shared__ unsigned est_mp[n_module_pairs];
     __shared__ unsigned cand_count;
     __shared__ unsigned warp_sums[33];
+    __shared__ uint16_t queue[estimate_queue];
+    __shared__ unsigned queue_count[2];
 
     const unsigned ev = e + p.in.event_start;
     const bool v23 = p.in.bank_version == 2 || p.in.bank_version == 3;
     if (threadIdx.x < n_module_pairs) est_mp[threadIdx.x] = 0;
     if (threadIdx.x == 0) cand_count = 0;
+    if (threadIdx.x < 2) queue_count[threadIdx.x] = 0;
     __syncthreads();
 
     unsigned n_words, staged;
@@ -456,24 +462,52 @@ namespace velo {
       }
     }
 
-    for (unsigned f = threadIdx.x; f < bt.total_sp; f += blockDim.x) {
-      const unsigned b = bank_of(bt, f);
-      const unsigned mp = bank_module_pair(bt.source_id[b], p.in.bank_version);
-      const uint32_t* bank_words = words + bt.words_off[b];
-      const uint32_t word = bank_words[f - bt.flat[b]];
-      unsigned add;
-      if (word & 0x80000000u) {
-        add = isolated_two_clusters(word & 0xFFu) ? 2u : 1u;
+    // Two passes per chunk of SPs, so that the warps do not diverge between the isolated SPs
+    // (about two thirds: one pattern test each) and the neighbour scans of the others: pass 1
+    // counts the isolated SPs and queues the others (warp-aggregated), pass 2 scans the
+    // queued SPs with every lane busy.  The counts are sums, so the order does not matter.
+    const unsigned chunk = estimate_queue;
+    for (unsigned chunk_base = 0, parity = 0; chunk_base < bt.total_sp; chunk_base += chunk, parity ^= 1u) {
+      for (unsigned f = chunk_base + threadIdx.x; f < chunk_base + chunk; f += blockDim.x) {
+        bool queued = false;
+        if (f < bt.total_sp) {
+          const unsigned b = bank_of(bt, f);
+          const uint32_t word = words[bt.words_off[b] + f - bt.flat[b]];
+          if (word & 0x80000000u) {
+            const unsigned mp = bank_module_pair(bt.source_id[b], p.in.bank_version);
+            if (mp < n_module_pairs) atomicAdd(&est_mp[mp], isolated_two_clusters(word & 0xFFu) ? 2u : 1u);
+            else set_error(p.status, err_input_capacity);
+          }
+          else {
+            queued = true;
+          }
+        }
+        const unsigned lane = threadIdx.x & 31u;
+        const unsigned mask = __ballot_sync(0xFFFFFFFFu, queued);
+        if (mask) {
+          const unsigned leader = __ffs(mask) - 1;
+          unsigned at = 0;
+          if (lane == leader) at = atomicAdd(&queue_count[parity], __popc(mask));
+          at = __shfl_sync(0xFFFFFFFFu, at, leader);
+          if (queued) queue[at + __popc(mask & ((1u << lane) - 1u))] = static_cast<uint16_t>(f - chunk_base);
+        }
       }
-      else {
-        const uint32_t c = sp_candidates(word, bank_words, bt.n_sp[b]);
-        add = ((c >> 8) & 1u) + ((c >> 24) & 1u);
+      __syncthreads();
+      const unsigned n_queued = min(queue_count[parity], chunk);
+      if (threadIdx.x == 0) queue_count[parity ^ 1u] = 0;
+      for (unsigned q = threadIdx.x; q < n_queued; q += blockDim.x) {
+        const unsigned f = chunk_base + queue[q];
+        const unsigned b = bank_of(bt, f);
+        const uint32_t* bank_words = words + bt.words_off[b];
+        const uint32_t c = sp_candidates(bank_words[f - bt.flat[b]], bank_words, bt.n_sp[b]);
+        const unsigned add = ((c >> 8) & 1u) + ((c >> 24) & 1u);
         if (add) atomicAdd(&cand_count, add);
+        const unsigned mp = bank_module_pair(bt.source_id[b], p.in.bank_version);
+        if (mp < n_module_pairs) atomicAdd(&est_mp[mp], add);
+        else set_error(p.status, err_input_capacity);
       }
-      if (mp < n_module_pairs) atomicAdd(&est_mp[mp], add);
-      else set_error(p.status, err_input_capacity);
+      __syncthreads();
     }
-    __syncthreads();
     if (threadIdx.x < n_module_pairs) {
       p.estimated_input_size[e * n_module_pairs + threadIdx.x] = est_mp[threadIdx.x];
     }

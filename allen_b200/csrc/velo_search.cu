@@ -902,7 +902,7 @@ namespace velo {
   // the CTAs per SM, and the extra resident events hide more latency than the few spills cost
   // (1.40M against 1.29M events/s at four CTAs per SM, measured).
   template<unsigned THREADS, unsigned LPH>
-  __global__ void __launch_bounds__(THREADS, LPH == 0 ? 1280 / THREADS : 1) search_by_triplet_kernel(SearchParams p)
+  __global__ void __launch_bounds__(THREADS, LPH == 0 ? 1536 / THREADS : 1) search_by_triplet_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ std::conditional_t<LPH == 0, SearchSharedFlat, SearchShared> s;
