@@ -189,7 +189,7 @@ static const SearchVariant search_variants[] = {
 #undef VELO_SEARCH_VARIANT
 };
 
-static constexpr unsigned retina_key_capacity = 4096; // clusters of an event keyed in shared memory (32 KiB)
+static constexpr unsigned retina_key_capacity = 3072; // clusters of an event keyed in shared memory (24 KiB of keys, 6 KiB of order)
 static constexpr size_t n_sensors_total = velo::n_sensors;
 
 static SearchKernel learned_search_kernel(unsigned threads)
@@ -376,7 +376,7 @@ namespace {
       exclusive_scan_kernel<<<1, scan_threads, 0, stream>>>(rs);
       VELO_CUDA(cudaGetLastError());
       VELO_CUDA(mark());
-      retina_decode_kernel<<<n, decode_threads, retina_key_capacity * sizeof(long long), stream>>>(rp);
+      retina_decode_kernel<<<n, decode_threads, retina_key_capacity * (sizeof(long long) + sizeof(uint16_t)), stream>>>(rp);
       VELO_CUDA(cudaGetLastError());
       VELO_CUDA(mark());
     }

@@ -172,12 +172,32 @@ namespace velo {
     return unsigned(r - 1);
   }
 
+  // Rank buckets per module pair: the top 6 bits of the (signed) sort key, so that bucket order
+  // is key order; about 1.3 clusters per bucket at nu = 7.6.
+  constexpr unsigned rank_buckets = 64;
+  constexpr unsigned rank_counters = n_module_pairs * rank_buckets;
+
+  __device__ __forceinline__ unsigned key_bucket(int64_t key)
+  {
+    return static_cast<unsigned>(static_cast<int>(key >> 58) + 32);
+  }
+
+  // u16 counters packed two per 32-bit word; returns the previous value of counter b.
+  __device__ __forceinline__ unsigned bump_u16(uint16_t* counters, unsigned b)
+  {
+    const unsigned shift = 16 * (b & 1u);
+    const uint32_t old = atomicAdd(reinterpret_cast<uint32_t*>(counters) + (b >> 1), 1u << shift);
+    return (old >> shift) & 0xFFFFu;
+  }
+
   __global__ void __launch_bounds__(decode_threads) retina_decode_kernel(RetinaParams p)
   {
     extern __shared__ __align__(16) unsigned char dsmem[];
     __shared__ unsigned so[n_sensors + 1]; // event-relative sensor offsets
     __shared__ unsigned mp_num[n_module_pairs], mp_zero[n_module_pairs];
     __shared__ unsigned warp_sums[33];
+    __shared__ __align__(4) uint16_t bucket_end[rank_counters];
+    __shared__ unsigned irregular;
     const unsigned e = blockIdx.x, ev = e + p.in.event_start, n = p.in.n_events;
     const int version = p.in.bank_version;
     const unsigned per_event = retina_sensors(version);
@@ -201,18 +221,23 @@ namespace velo {
       so[per_event] = total;
       if (e == n - 1) p.offsets_each_sensor_pair_size[size_t(n) * per_event] = base + total;
       if (e == 0) p.offsets_module_pair_cluster[0] = 0;
+      irregular = 0;
     }
     if (threadIdx.x < n_module_pairs) {
       mp_num[threadIdx.x] = 0;
       mp_zero[threadIdx.x] = 0;
     }
+    for (unsigned i = threadIdx.x; i < rank_counters / 2; i += blockDim.x)
+      reinterpret_cast<uint32_t*>(bucket_end)[i] = 0;
     __syncthreads();
     // populate_module_pair_offsets_and_sizes (DecodeRetinaClusters.cu:11-35)
     if (threadIdx.x < n_module_pairs) p.offsets_module_pair_cluster[e * n_module_pairs + threadIdx.x + 1] = base + so[(threadIdx.x + 1) * step];
 
-    // keys: shared memory when the event fits, else its slice of the global scratch
+    // keys (and the bucket order) in shared memory when the event fits, else keys in its slice
+    // of the global scratch
     const bool in_smem = total <= p.smem_key_capacity;
     int64_t* keys = in_smem ? reinterpret_cast<int64_t*>(dsmem) : reinterpret_cast<int64_t*>(p.key_scratch) + base;
+    uint16_t* order = reinterpret_cast<uint16_t*>(dsmem + size_t(p.smem_key_capacity) * sizeof(int64_t));
     const Geometry* g = p.geo;
     const Constants k = p.k;
     // velo_calculate_sorting_key (DecodeRetinaClusters.cu:162-244)
@@ -221,19 +246,57 @@ namespace velo {
       RetinaBank bank;
       uint32_t w;
       int64_t key = 0x7FFFFFFFFFFFFFFFll;
+      bool counted = false;
       if (cluster_word(p, ev, s, c - so[s], bank, w)) {
         const RetinaCluster cl = decode_word(g, k, version, bank.source_id, w);
         const unsigned mp = cl.sensor / 8;
-        if (mp < n_module_pairs) atomicAdd(w != 0 ? &mp_num[mp] : &mp_zero[mp], 1u);
+        if (mp < n_module_pairs) {
+          atomicAdd(w != 0 ? &mp_num[mp] : &mp_zero[mp], 1u);
+          counted = mp == s / step;
+        }
         if (w != 0) key = static_cast<int64_t>((static_cast<uint64_t>(static_cast<uint16_t>(cl.phi)) << 48) | cl.id);
       }
       keys[c] = key;
+      if (in_smem) {
+        if (counted) bump_u16(bucket_end, (s / step) * rank_buckets + key_bucket(key));
+        else irregular = 1; // a cluster the module-pair counts miss: rank by the full comparison
+      }
     }
     __syncthreads();
     if (threadIdx.x < n_module_pairs) p.module_cluster_num[e * n_module_pairs + threadIdx.x] = mp_num[threadIdx.x];
 
     // velo_calculate_permutations + decode_retinaclusters_sorted (DecodeRetinaClusters.cu:37-78,
-    // 305-383): a cluster's slot is its module pair's start plus the number of smaller keys
+    // 305-383): a cluster's slot is its module pair's start plus the number of smaller keys of
+    // the module pair.  When every cluster was counted in its module pair's (key) buckets, the
+    // buckets are laid out in order by a scan of their counts, each cluster is placed in its
+    // bucket, and its rank is the bucket's start plus the smaller keys of the same bucket.
+    const bool bucketed = in_smem && !irregular;
+    if (bucketed) {
+      constexpr unsigned per = (rank_counters + decode_threads - 1) / decode_threads;
+      unsigned v[per];
+      unsigned sum = 0;
+#pragma unroll
+      for (unsigned q = 0; q < per; ++q) {
+        const unsigned b = threadIdx.x * per + q;
+        v[q] = b < rank_counters ? bucket_end[b] : 0u;
+        sum += v[q];
+      }
+      unsigned all;
+      unsigned run = block_exclusive_scan(sum, warp_sums, &all);
+      __syncthreads(); // every count read before the starts overwrite them
+#pragma unroll
+      for (unsigned q = 0; q < per; ++q) {
+        const unsigned b = threadIdx.x * per + q;
+        if (b < rank_counters) bucket_end[b] = static_cast<uint16_t>(run); // start; the fill below ends it
+        run += v[q];
+      }
+      __syncthreads();
+      for (unsigned c = threadIdx.x; c < total; c += blockDim.x) {
+        const unsigned s = rightmost(so, per_event, c);
+        order[bump_u16(bucket_end, (s / step) * rank_buckets + key_bucket(keys[c]))] = static_cast<uint16_t>(c);
+      }
+      __syncthreads();
+    }
     ClusterView out {p.container, T};
     for (unsigned c = threadIdx.x; c < total; c += blockDim.x) {
       const unsigned s = rightmost(so, per_event, c);
@@ -242,11 +305,20 @@ namespace velo {
       if (!cluster_word(p, ev, s, c - so[s], bank, w)) continue;
       const unsigned mp = s / step;
       const unsigned start = so[mp * step];
-      const unsigned num = min(mp_num[mp] + mp_zero[mp], total - start);
       const int64_t key = keys[c];
       unsigned position = 0;
-      for (unsigned j = 0; j < num; ++j)
-        position += (start + j != c) && key > keys[start + j];
+      if (bucketed) {
+        const unsigned b = mp * rank_buckets + key_bucket(key);
+        const unsigned first = b ? bucket_end[b - 1] : 0u, last = bucket_end[b];
+        position = first - start;
+        for (unsigned i = first; i < last; ++i)
+          position += key > keys[order[i]];
+      }
+      else {
+        const unsigned num = min(mp_num[mp] + mp_zero[mp], total - start);
+        for (unsigned j = 0; j < num; ++j)
+          position += (start + j != c) && key > keys[start + j];
+      }
       const RetinaCluster cl = decode_word(g, k, version, bank.source_id, w);
       const unsigned dst = base + start + position;
       if (dst >= T) {

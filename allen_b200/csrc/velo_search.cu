@@ -918,7 +918,7 @@ namespace velo {
   // search, recording training doublets when asked) is a kernel of its own, so the plain
   // kernels keep their register budget.
   template<unsigned THREADS>
-  __global__ void __launch_bounds__(THREADS, 768 / THREADS) search_by_triplet_learned_kernel(SearchParams p)
+  __global__ void __launch_bounds__(THREADS, 1024 / THREADS) search_by_triplet_learned_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ SearchSharedFlat s;
