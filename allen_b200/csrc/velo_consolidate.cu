@@ -15,6 +15,7 @@ namespace velo {
   __global__ void __launch_bounds__(consolidate_threads) consolidate_kernel(ConsolidateParams p)
   {
     __shared__ unsigned warp_sums[33];
+    __shared__ uint16_t chunk_hits[consolidate_threads * max_track_size]; // hit indices of a chunk's tracks
     const unsigned e = blockIdx.x;
     const unsigned n = p.n_events;
     const unsigned to = track_offset(p.offsets_estimated_input_size, e);
@@ -49,6 +50,10 @@ namespace velo {
         p.accepted_velo_tracks[i] = true;
     }
 
+    // Tracks in chunks of one per thread: a scan of the hit numbers places each track, its
+    // thread writes the track's entries and its hit indices (event-relative, in output order)
+    // to shared memory, then all threads gather the chunk's hits - one hit per thread, so the
+    // gathers run in parallel and the writes to the consolidated SoA are contiguous.
     const ClusterView in {const_cast<char*>(p.sorted_container), T};
     const ClusterView out {p.velo_track_hits, TH};
     unsigned carry = 0;
@@ -76,18 +81,24 @@ namespace velo {
           p.velo_track_hit_number[g] = hn;
           p.offsets_velo_track_hit_number[g] = pos;
           p.accepted_velo_tracks[g] = true;
-          for (unsigned j = 0; j < hn; ++j) {
-            const unsigned hi = hit_offset + hits[j];
-            out.x(pos + j) = in.x(hi);
-            out.y(pos + j) = in.y(hi);
-            out.z(pos + j) = in.z(hi);
-            out.id(pos + j) = in.id(hi);
-          }
         }
         else {
           set_error(p.status, err_output_capacity);
         }
+        for (unsigned j = 0; j < hn; ++j)
+          chunk_hits[excl + j] = hits[j];
       }
+      __syncthreads();
+      const unsigned pos0 = hit_base + carry;
+      for (unsigned k = threadIdx.x; k < block_total; k += blockDim.x) {
+        const unsigned hi = hit_offset + chunk_hits[k];
+        if (pos0 + k >= p.track_hit_capacity || hi >= T) continue; // flagged: a track that did not fit
+        out.x(pos0 + k) = in.x(hi);
+        out.y(pos0 + k) = in.y(hi);
+        out.z(pos0 + k) = in.z(hi);
+        out.id(pos0 + k) = in.id(hi);
+      }
+      __syncthreads(); // chunk_hits is reused by the next chunk
       carry += block_total;
     }
   }
