@@ -2,8 +2,9 @@
 
 Sweeps, on a generated workload of the target occupancy, the search kernel's block size and
 lanes per seed candidate (the compiled pairs), the shared-memory staging capacities of the
-search, clustering and estimate kernels, and persistent launches with a work queue (events
-claimed per CTA) against one CTA per event, by coordinate descent: each parameter in turn takes the
+search, clustering and estimate kernels, the place of the search's ring of tracks to follow, and
+persistent launches with a work queue (events claimed per CTA) against one CTA per event, by
+coordinate descent: each parameter in turn takes the
 value with the highest events/s (CUDA-event timed graph replays) while the others stay at
 the current best.  The winner is written to allen_b200/data/launch_config.json, which
 VeloChain loads by default.
@@ -17,7 +18,9 @@ import json
 import os
 import time
 
-SEARCH_VARIANTS = [(128, 1), (128, 2), (256, 1), (256, 2), (256, 4), (512, 2), (512, 4), (128, 0), (256, 0), (512, 0)]
+# (block size, lanes per seed candidate, ring of tracks to follow in global scratch)
+SEARCH_VARIANTS = [(128, 1, 0), (128, 2, 0), (256, 1, 0), (256, 2, 0), (256, 4, 0), (512, 2, 0), (512, 4, 0),
+                   (128, 0, 0), (256, 0, 0), (512, 0, 0), (128, 0, 1), (256, 0, 1)]
 SEARCH_CAPACITIES = [0, 1024, 2048, 2560, 3072, 4096]
 CLUSTER_CAPACITIES = [0, 1024, 2048, 2560, 3072]
 CLUSTER_BLOBS = [16 * 1024, 24 * 1024, 32 * 1024, 40 * 1024]
@@ -43,7 +46,7 @@ def measure(chain, dev_slices, repeats=3) -> float:
     return events / (start.elapsed_time(end) / 1e3)
 
 
-def tune(chain, dev_slices, log=print) -> tuple[dict, float, list]:
+def tune(chain, dev_slices, log=print, max_sweeps: int = 3) -> tuple[dict, float, list]:
     trials = []
     best = chain.get_config()
 
@@ -61,27 +64,44 @@ def tune(chain, dev_slices, log=print) -> tuple[dict, float, list]:
         return rate
 
     best_rate = try_config()
-    for name, values in (
+    coordinates = (
         ("search", SEARCH_VARIANTS),
         ("search_hit_capacity", SEARCH_CAPACITIES),
         ("cluster_stage_capacity", CLUSTER_CAPACITIES),
         ("cluster_blob_bytes", CLUSTER_BLOBS),
         ("estimate_blob_bytes", ESTIMATE_BLOBS),
         ("queue", QUEUES),
-    ):
-        for v in values:
-            if name == "search":
-                upd = {"search_threads": v[0], "search_lanes_per_seed": v[1]}
-            elif name == "queue":
-                upd = {"persistent": v[0], "events_per_claim": v[1]}
-            else:
-                upd = {name: v}
-            rate = try_config(**upd)
-            if rate is not None and rate > best_rate:
-                best_rate = rate
-                best.update(upd)
+    )
+    # sweeps repeat until one changes nothing: the best search kernel depends on the staging
+    # capacities chosen after it (its CTAs per SM), so one greedy sweep can stop short
+    for sweep in range(max_sweeps):
+        before = dict(best)
+        for name, values in coordinates:
+            best_rate = sweep_coordinate(name, values, best, best_rate, try_config)
+        if best == before:
+            break
     chain.configure(**best)
     return best, best_rate, trials
+
+
+def sweep_coordinate(name, values, best, best_rate, try_config):
+    """One coordinate: each value in turn against the current best; returns the new best rate."""
+    for v in values:
+        if name == "search":
+            upd = {"search_threads": v[0], "search_lanes_per_seed": v[1], "search_ring_global": v[2]}
+            if v[2]:
+                upd["persistent"] = 1  # one ring per resident CTA
+        elif name == "queue":
+            upd = {"persistent": v[0], "events_per_claim": v[1]}
+            if best.get("search_ring_global") and not v[0]:
+                continue  # the global rings need persistent launches
+        else:
+            upd = {name: v}
+        rate = try_config(**upd)
+        if rate is not None and rate > best_rate:
+            best_rate = rate
+            best.update(upd)
+    return best_rate
 
 
 def main():

@@ -177,14 +177,14 @@ namespace {
   }
 } // namespace
 
-// search_by_triplet_kernel instantiations (block size, lanes per seed candidate)
+// search_by_triplet_kernel instantiations (block size, lanes per seed candidate, ring place)
 using SearchKernel = void (*)(velo::SearchParams);
 struct SearchVariant {
-  unsigned threads, lanes;
+  unsigned threads, lanes, ring_global;
   SearchKernel fn;
 };
 static const SearchVariant search_variants[] = {
-#define VELO_SEARCH_VARIANT(T, L) {T, L, velo::search_by_triplet_kernel<T, L>},
+#define VELO_SEARCH_VARIANT(T, L, R) {T, L, R, velo::search_by_triplet_kernel<T, L, R>},
   VELO_SEARCH_CONFIGS(VELO_SEARCH_VARIANT)
 #undef VELO_SEARCH_VARIANT
 };
@@ -202,10 +202,10 @@ static SearchKernel learned_search_kernel(unsigned threads)
   }
 }
 
-static const SearchVariant* find_search_variant(unsigned threads, unsigned lanes)
+static const SearchVariant* find_search_variant(unsigned threads, unsigned lanes, unsigned ring_global = 0)
 {
   for (const auto& v : search_variants)
-    if (v.threads == threads && v.lanes == lanes) return &v;
+    if (v.threads == threads && v.lanes == lanes && v.ring_global == ring_global) return &v;
   return nullptr;
 }
 
@@ -235,6 +235,7 @@ struct VeloChain {
   unsigned search_lanes = 2;
   unsigned persistent = 0;
   unsigned events_per_claim = 1;
+  unsigned search_ring_global = 0; // rings of tracks to follow in global scratch (persistent only)
   unsigned resident_estimate = 0, resident_cluster = 0, resident_search = 0; // CTAs that fit the device
 
   // workspace
@@ -244,6 +245,7 @@ struct VeloChain {
     event_base, offsets_est, cluster_num, atomics, n_tracks, offsets_tracks, n_three_out, offsets_three,
     event_track_hits, event_track_hit_base, offsets_all, track_hit_number, offsets_hit_number;
   DeviceBuffer<char> sorted, staging, track_hits, hit_scratch;
+  DeviceBuffer<uint64_t> ring_scratch; // search_ring_global: one ring of 2048 entries per resident search CTA
   DeviceBuffer<velo::TrackHits> tracks;
   DeviceBuffer<velo::TrackletHits> three_hit, three_out;
   DeviceBuffer<uint8_t> hit_used, accepted;
@@ -444,6 +446,7 @@ namespace {
     sp.status = c->status.p;
     sp.smem_hit_capacity = c->search_hit_capacity;
     sp.hit_scratch = c->hit_scratch.p;
+    sp.ring_scratch = c->ring_scratch.p;
     sp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
     sp.seed_stats = c->seed_stats.p;
     sp.seed_model = c->learned ? c->seed_model.p : nullptr;
@@ -455,7 +458,7 @@ namespace {
     const unsigned search_smem = c->search_hit_capacity * search_hit_bytes;
     {
       const SearchKernel fn = (c->learned || c->records) ? learned_search_kernel(c->search_threads) : nullptr;
-      const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes);
+      const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes, c->search_ring_global);
       if (!fn && !v) return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for this launch configuration");
       void* args[] = {&sp};
       VELO_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(fn ? fn : v->fn), dim3(grid(c->resident_search)),
@@ -533,12 +536,18 @@ namespace {
     c->resident_estimate = unsigned(std::max(per_sm, 1) * sms);
     VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel, decode_threads, cluster_smem));
     c->resident_cluster = unsigned(std::max(per_sm, 1) * sms);
-    const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes);
+    const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes, c->search_ring_global);
     const SearchKernel learned = learned_search_kernel(c->search_threads);
     SearchKernel fn = (c->learned || c->records) && learned ? learned : (v ? v->fn : nullptr);
     if (fn) {
       VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, int(c->search_threads), search_smem));
       c->resident_search = unsigned(std::max(per_sm, 1) * sms);
+    }
+    // the global rings: one per CTA of the persistent search grid (the plain kernel's grid;
+    // the learned kernel keeps its ring in shared memory)
+    if (c->search_ring_global && v) {
+      VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v->fn, int(c->search_threads), search_smem));
+      VELO_CUDA(c->ring_scratch.reserve(size_t(std::max(per_sm, 1)) * sms * max_tracks_to_follow));
     }
     return VELO_OK;
   }
@@ -746,9 +755,12 @@ VeloStatus velo_chain_run(VeloChain* c, const VeloDeviceSlice* s, VeloStream str
 VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
 {
   if (!c || !cfg) return fail(VELO_ERR_ARGUMENT, "null argument");
-  if (!find_search_variant(cfg->search_threads, cfg->search_lanes_per_seed))
+  if (!find_search_variant(cfg->search_threads, cfg->search_lanes_per_seed, cfg->search_ring_global))
     return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for (" + std::to_string(cfg->search_threads) + ", " +
-                                     std::to_string(cfg->search_lanes_per_seed) + ")");
+                                     std::to_string(cfg->search_lanes_per_seed) + ", ring " +
+                                     std::to_string(cfg->search_ring_global) + ")");
+  if (cfg->search_ring_global && !cfg->persistent)
+    return fail(VELO_ERR_ARGUMENT, "search_ring_global needs persistent launches (one ring per resident CTA)");
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   const unsigned search_static = 32 * 1024; // upper bound of the kernel's static shared memory
@@ -767,6 +779,7 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
   c->estimate_blob_bytes = cfg->estimate_blob_bytes;
   c->persistent = cfg->persistent;
   c->events_per_claim = cfg->events_per_claim;
+  c->search_ring_global = cfg->search_ring_global;
   return configure_kernels(c);
 }
 
@@ -781,6 +794,7 @@ VeloStatus velo_chain_get_config(const VeloChain* c, VeloLaunchConfig* cfg)
   cfg->estimate_blob_bytes = c->estimate_blob_bytes;
   cfg->persistent = c->persistent;
   cfg->events_per_claim = c->events_per_claim;
+  cfg->search_ring_global = c->search_ring_global;
   return VELO_OK;
 }
 
@@ -1064,6 +1078,7 @@ void velo_chain_destroy(VeloChain* c)
   c->sorted.release();
   c->staging.release();
   c->hit_scratch.release();
+  c->ring_scratch.release();
   c->track_hits.release();
   c->tracks.release();
   c->three_hit.release();

@@ -97,6 +97,7 @@ namespace velo {
     unsigned smem_hit_capacity;                   // hits staged in shared memory per event
     unsigned cluster_capacity;                    // allocated T of the containers
     char* hit_scratch;                            // [16 T] staging of events above the capacity
+    uint64_t* ring_scratch;                       // [2048 grid] rings of tracks to follow (RING = 1)
     // learned seed pruning (search_by_triplet_learned_kernel): the network, or null for the
     // plain search
     const MlpModelDevice* seed_model;
@@ -158,14 +159,16 @@ namespace velo {
 
   __global__ void estimate_kernel(EstimateParams p);
   __global__ void cluster_sort_kernel(ClusterSortParams p);
-  template<unsigned THREADS, unsigned LPH>
+  template<unsigned THREADS, unsigned LPH, unsigned RING>
   __global__ void search_by_triplet_kernel(SearchParams p);
   // flat seeding with the learned seed pruner and doublet recording, THREADS = 128, 256, 512
   template<unsigned THREADS>
   __global__ void search_by_triplet_learned_kernel(SearchParams p);
   // (block size, lanes per seed candidate) pairs compiled for the autotuner
 // lanes 0 = flattened seeding (one thread per h1 candidate)
-#define VELO_SEARCH_CONFIGS(X) X(128, 1) X(128, 2) X(256, 1) X(256, 2) X(256, 4) X(512, 2) X(512, 4) X(128, 0) X(256, 0) X(512, 0)
+#define VELO_SEARCH_CONFIGS(X)                                                                                  \
+  X(128, 1, 0) X(128, 2, 0) X(256, 1, 0) X(256, 2, 0) X(256, 4, 0) X(512, 2, 0) X(512, 4, 0) X(128, 0, 0) X(256, 0, 0) \
+    X(512, 0, 0) X(128, 0, 1) X(256, 0, 1)
   __global__ void consolidate_kernel(ConsolidateParams p);
   // ---- retina-cluster decoding (VPRetinaCluster banks) ----
   struct RetinaParams {

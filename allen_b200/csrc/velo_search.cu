@@ -50,25 +50,32 @@ namespace velo {
   struct SearchShared {
     unsigned scan_sums[2][32]; // double-buffered warp totals of the block scans
     unsigned track_hits;       // sum of hitsNum over the >= 4 hit tracks
-    uint64_t ring[max_tracks_to_follow];
     uint32_t tail[max_tail_tracks]; // last two hits of a track (hit[n-2] | hit[n-1] << 16)
     uint8_t tail_n[max_tail_tracks];
     uint16_t bucket[n_module_pairs][n_buckets + 1];
   };
 
   // Shared state of the flat seeding variant: one slot per (h1, candidate order).
-  struct SearchSharedFlat : SearchShared {
+  // SLOTS doublets per chunk; MLP adds the seed pruner's staging rows (learned kernel).
+  template<unsigned SLOTS, bool MLP>
+  struct SearchSharedFlatT : SearchShared {
+    static constexpr unsigned slots = SLOTS;
     // (h0, h1) doublets of a chunk, packed by pack_doublet(), then overwritten in place
     // with the best scatter found for the doublet
     union {
       uint32_t doublet;
       float fit;
-    } slot[flat_slots];
+    } slot[SLOTS];
     union alignas(16) { // ldmatrix reads 16-byte rows of mlp_rows
-      uint16_t res_h2[flat_slots];
-      uint32_t mlp_rows[8][16][8]; // per warp: 16 doublets x 16 bf16 inputs (learned mode)
+      uint16_t res_h2[SLOTS];
+      uint32_t mlp_rows[MLP ? 8 : 1][16][8]; // per warp: 16 doublets x 16 bf16 inputs (learned mode)
     };
   };
+  using SearchSharedFlat = SearchSharedFlatT<flat_slots, true>;
+  // plain flat-seeding kernels: 512 slots for 128 threads (chunks of 64 or 128 h1), which with
+  // the ring in global scratch leaves room for twelve CTAs per SM
+  template<unsigned THREADS>
+  using SearchSharedFlatPlain = SearchSharedFlatT<(THREADS <= 128 ? flat_slots / 2 : flat_slots), false>;
 
   // Packed doublet: h0 | h1 index in the chunk << 16 | rank << 25 | (found - 1) << 28 | keep << 31
   __device__ __forceinline__ uint32_t pack_doublet(unsigned h0, unsigned h1_local, unsigned rank, unsigned found)
@@ -219,7 +226,8 @@ namespace velo {
   // Seeding over the current module pair (SearchByTriplet.cu:298-446), LPH lanes per h1.
   template<unsigned LPH>
   __device__ __forceinline__ void seeding(
-    SearchShared& s, Counters& cnt, const Constants& k, const HitsSoA& h, const ModulePair* md, unsigned n_candidates)
+    SearchShared& s, uint64_t* ring, Counters& cnt, const Constants& k, const HitsSoA& h, const ModulePair* md,
+    unsigned n_candidates)
   {
     const ModulePair prev = md[0], cur = md[1], next = md[2];
     const unsigned groups = blockDim.x / LPH;
@@ -276,7 +284,7 @@ namespace velo {
       const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | (unused << 16), total);
       if (ok) {
         const unsigned tn = (cnt.ttf + (excl & 0xFFFFu)) % max_tracks_to_follow;
-        s.ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
+        ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
                      (uint64_t(best_h2 & 0xFFFFu) << 32);
       }
       cnt.ttf += total & 0xFFFFu;
@@ -339,9 +347,10 @@ namespace velo {
   // path on every lane and has no idle slots for h1 with fewer than n_candidates doublets.
   // LEARNED kernels can also score the doublets with the seed pruner (only kept doublets
   // reach phase B) and record training doublets.
-  template<bool LEARNED>
+  template<bool LEARNED, typename Flat>
   __device__ __forceinline__ void seeding_flat(
-    SearchSharedFlat& s,
+    Flat& s,
+    uint64_t* ring,
     Counters& cnt,
     const Constants& k,
     const HitsSoA& h,
@@ -353,7 +362,7 @@ namespace velo {
     unsigned hit_offset)
   {
     const ModulePair prev = md[0], cur = md[1], next = md[2];
-    const unsigned per_chunk = min(blockDim.x, flat_slots / n_candidates);
+    const unsigned per_chunk = min(blockDim.x, Flat::slots / n_candidates);
     const int n_prev = static_cast<int>(prev.hit_num);
     const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
     for (unsigned c0 = 0; c0 < cur.hit_num; c0 += per_chunk) {
@@ -385,7 +394,7 @@ namespace velo {
       cnt.doublets += n_doublets;
       // keep_mask bit c: the h2 window of doublet c is scanned (always, in the plain search)
       unsigned keep_mask = (1u << found) - 1u;
-      if (LEARNED && learned) {
+      if constexpr (LEARNED) if (learned) {
         score_doublets(s, p.seed_model, h, cur.hit_start + c0, n_doublets);
         __syncthreads();
         keep_mask = 0;
@@ -473,7 +482,7 @@ namespace velo {
       const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | ((valid ? 1u : 0u) << 16), total);
       if (ok) {
         const unsigned tn = (cnt.ttf + (excl & 0xFFFFu)) % max_tracks_to_follow;
-        s.ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
+        ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
                      (uint64_t(best_h2 & 0xFFFFu) << 32);
       }
       cnt.ttf += total & 0xFFFFu;
@@ -484,6 +493,7 @@ namespace velo {
   // Forwarding of the tracks to follow (SearchByTriplet.cu:451-609), one thread per track.
   __device__ __forceinline__ void forwarding(
     SearchShared& s,
+    uint64_t* ring,
     Counters& cnt,
     const Constants& k,
     const HitsSoA& h,
@@ -504,7 +514,7 @@ namespace velo {
       bool is_seed = false, found = false;
       unsigned best_h2 = 0;
       if (active) {
-        entry = s.ring[(prev_ttf + kk) % max_tracks_to_follow];
+        entry = ring[(prev_ttf + kk) % max_tracks_to_follow];
         is_seed = (entry & seed_flag) != 0;
         if (is_seed) {
           nh = 3;
@@ -606,7 +616,7 @@ namespace velo {
           const uint64_t value =
             found ? uint64_t(track_number) :
                     ((entry & ~(uint64_t(0x7) << skipped_shift)) | (uint64_t(skipped + 1) << skipped_shift));
-          s.ring[(cnt.ttf + ((excl >> 10) & 0x3FFu)) % max_tracks_to_follow] = value;
+          ring[(cnt.ttf + ((excl >> 10) & 0x3FFu)) % max_tracks_to_follow] = value;
         }
         if (three) {
           const unsigned slot = cnt.n_three + ((excl >> 20) & 0x3FFu);
@@ -691,6 +701,7 @@ namespace velo {
   __device__ __forceinline__ Counters search_pass(
     const SearchParams& p,
     Shared& s,
+    uint64_t* ring,
     const Constants& k,
     const HitsSoA& h,
     const unsigned* start,
@@ -710,8 +721,8 @@ namespace velo {
     module_pairs(md, p.geo, first, start, num, hit_offset);
     __syncthreads(); // bucket tables
 
-    if constexpr (LPH == 0) seeding_flat<LEARNED>(s, cnt, k, h, md, 8, p, learned, e, hit_offset);
-    else seeding<LPH>(s, cnt, k, h, md, 8);
+    if constexpr (LPH == 0) seeding_flat<LEARNED>(s, ring, cnt, k, h, md, 8, p, learned, e, hit_offset);
+    else seeding<LPH>(s, ring, cnt, k, h, md, 8);
 
     unsigned last_ttf = 0;
     --first;
@@ -722,13 +733,13 @@ namespace velo {
       const unsigned diff = last_ttf - prev_ttf;
       cnt.local_hits = 0;
       __syncthreads(); // ring entries of the last seeding
-      forwarding(s, cnt, k, h, md[2], prev_ttf, diff, tracks, track_limit, three_hit, p.status);
+      forwarding(s, ring, cnt, k, h, md[2], prev_ttf, diff, tracks, track_limit, three_hit, p.status);
       // The ring holds 2048 entries; beyond that the reference overwrites entries it has
       // not read yet, an order-dependent outcome this kernel does not reproduce.
       if (threadIdx.x == 0 && cnt.ttf - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       __syncthreads(); // hit_used flags written by forwarding
-      if constexpr (LPH == 0) seeding_flat<LEARNED>(s, cnt, k, h, md, 4, p, learned, e, hit_offset);
-      else seeding<LPH>(s, cnt, k, h, md, 4);
+      if constexpr (LPH == 0) seeding_flat<LEARNED>(s, ring, cnt, k, h, md, 4, p, learned, e, hit_offset);
+      else seeding<LPH>(s, ring, cnt, k, h, md, 4);
       if (threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       --first;
     }
@@ -744,7 +755,7 @@ namespace velo {
         uint64_t entry = 0;
         bool seed = false;
         if (kk < diff) {
-          entry = s.ring[(prev_ttf + kk) % max_tracks_to_follow];
+          entry = ring[(prev_ttf + kk) % max_tracks_to_follow];
           seed = (entry & seed_flag) != 0;
         }
         unsigned total;
@@ -768,7 +779,8 @@ namespace velo {
   }
 
   template<unsigned LPH, bool SMEM, bool LEARNED, typename Shared>
-  __device__ __forceinline__ void search_event(const SearchParams& p, Shared& s, unsigned char* dsmem, unsigned e)
+  __device__ __forceinline__ void
+  search_event(const SearchParams& p, Shared& s, uint64_t* ring, unsigned char* dsmem, unsigned e)
   {
     const unsigned n = p.n_events;
     const unsigned* start = p.offsets_estimated_input_size + e * n_module_pairs;
@@ -834,7 +846,7 @@ namespace velo {
     // outside the model's bounds is searched again by the plain search, from scratch.
     const bool learned = LEARNED && p.seed_model != nullptr;
     Counters cnt =
-      search_pass<LPH, LEARNED>(p, s, k, h, start, num, hit_offset, e, tracks, track_limit, three_hit, learned);
+      search_pass<LPH, LEARNED>(p, s, ring, k, h, start, num, hit_offset, e, tracks, track_limit, three_hit, learned);
     unsigned mode = learned ? seed_mode_learned : seed_mode_plain;
     const unsigned doublets = cnt.doublets, kept = cnt.kept;
     if (learned && doublets > 0) {
@@ -844,7 +856,7 @@ namespace velo {
         __syncthreads();
         for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x)
           flags[i] &= static_cast<uint8_t>(~flag_used);
-        cnt = search_pass<LPH, LEARNED>(p, s, k, h, start, num, hit_offset, e, tracks, track_limit, three_hit, false);
+        cnt = search_pass<LPH, LEARNED>(p, s, ring, k, h, start, num, hit_offset, e, tracks, track_limit, three_hit, false);
       }
     }
     if (p.seed_stats != nullptr && threadIdx.x == 0) {
@@ -894,23 +906,28 @@ namespace velo {
     }
   }
 
-  // One instantiation per (block size, lanes per seed); the chain launches the one its
-  // launch configuration names (autotuned).  Events whose hits fit the shared-memory
-  // capacity run the shared-memory body, the others the global-scratch body.
-  // Flat-seeding kernels are register-capped for five 256-thread CTAs per SM (51 registers):
-  // with the hits staged through L2 (search_hit_capacity 0) shared memory no longer limits
-  // the CTAs per SM, and the extra resident events hide more latency than the few spills cost
-  // (1.40M against 1.29M events/s at four CTAs per SM, measured).
-  template<unsigned THREADS, unsigned LPH>
+  // One instantiation per (block size, lanes per seed, ring place); the chain launches the one
+  // its launch configuration names (autotuned).  Events whose hits fit the shared-memory
+  // capacity run the shared-memory body, the others the global-scratch body.  The ring of
+  // tracks to follow (2048 entries, 16 KiB) sits in shared memory, or with RING = 1 in this
+  // CTA's slice of a global scratch (persistent launches only: the slice is the CTA's index),
+  // which leaves room for more resident CTAs per SM.
+  // Flat-seeding kernels are register-capped for six 256-thread CTAs per SM (40 registers, a
+  // few spills): with the hits staged through L2 (search_hit_capacity 0) shared memory no
+  // longer limits the CTAs per SM, and the extra resident events hide more latency than the
+  // spills cost (measured, 5.87 against 5.72 ms per 16000 events at five and six CTAs).
+  template<unsigned THREADS, unsigned LPH, unsigned RING>
   __global__ void __launch_bounds__(THREADS, LPH == 0 ? 1536 / THREADS : 1) search_by_triplet_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
-    __shared__ std::conditional_t<LPH == 0, SearchSharedFlat, SearchShared> s;
+    __shared__ std::conditional_t<LPH == 0, SearchSharedFlatPlain<THREADS>, SearchShared> s;
+    __shared__ uint64_t ring_smem[RING ? 1 : max_tracks_to_follow];
+    uint64_t* ring = RING ? p.ring_scratch + size_t(blockIdx.x) * max_tracks_to_follow : ring_smem;
     for_each_event(p.queue, p.n_events, [&](unsigned e, unsigned) {
       const unsigned* start = p.offsets_estimated_input_size + e * n_module_pairs;
       const unsigned n_hits = start[n_module_pairs] - start[0];
-      if (n_hits <= p.smem_hit_capacity) search_event<LPH, true, false>(p, s, dsmem, e);
-      else search_event<LPH, false, false>(p, s, dsmem, e);
+      if (n_hits <= p.smem_hit_capacity) search_event<LPH, true, false>(p, s, ring, dsmem, e);
+      else search_event<LPH, false, false>(p, s, ring, dsmem, e);
     });
   }
 
@@ -922,16 +939,17 @@ namespace velo {
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ SearchSharedFlat s;
+    __shared__ uint64_t ring[max_tracks_to_follow];
     for_each_event(p.queue, p.n_events, [&](unsigned e, unsigned) {
       const unsigned* start = p.offsets_estimated_input_size + e * n_module_pairs;
       const unsigned n_hits = start[n_module_pairs] - start[0];
-      if (n_hits <= p.smem_hit_capacity) search_event<0, true, true>(p, s, dsmem, e);
-      else search_event<0, false, true>(p, s, dsmem, e);
+      if (n_hits <= p.smem_hit_capacity) search_event<0, true, true>(p, s, ring, dsmem, e);
+      else search_event<0, false, true>(p, s, ring, dsmem, e);
     });
   }
 
-#define VELO_SEARCH_CONFIG(T, L)                                                 \
-  template __global__ void search_by_triplet_kernel<T, L>(SearchParams p);
+#define VELO_SEARCH_CONFIG(T, L, R)                                              \
+  template __global__ void search_by_triplet_kernel<T, L, R>(SearchParams p);
   VELO_SEARCH_CONFIGS(VELO_SEARCH_CONFIG)
 #undef VELO_SEARCH_CONFIG
   template __global__ void search_by_triplet_learned_kernel<128>(SearchParams p);

@@ -195,6 +195,10 @@ typedef struct {
                                       as fit the device, claiming events (largest raw size first)
                                       from a work queue; 0: one CTA per event */
   unsigned events_per_claim;       /* events a persistent CTA claims at once (1..64) */
+  unsigned search_ring_global;     /* 1: the search's ring of tracks to follow (16 KiB per CTA) lives in
+                                      global scratch instead of shared memory, leaving room for more
+                                      resident CTAs; flat seeding with 128 or 256 threads, persistent
+                                      launches only */
 } VeloLaunchConfig;
 VeloStatus velo_chain_configure(VeloChain* chain, const VeloLaunchConfig* config);
 VeloStatus velo_chain_get_config(const VeloChain* chain, VeloLaunchConfig* config);

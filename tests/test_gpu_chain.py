@@ -5,7 +5,7 @@ import pytest
 import golden_io
 import parity
 from allen_b200 import generator
-from allen_b200.chain import upload
+from allen_b200.chain import VeloError, upload
 
 pytestmark = pytest.mark.gpu
 
@@ -154,6 +154,24 @@ def test_persistent_work_queue_identical(chain, oracle, geometry, claim):
     saved = chain.get_config()
     try:
         chain.configure(persistent=1, events_per_claim=claim)
+        totals, out = run_chain(chain, g.raw, use_graph=True)
+        assert totals["device_flags"] == 0
+        assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
+    finally:
+        chain.configure(**saved)
+
+
+@pytest.mark.parametrize("threads", [128, 256])
+def test_search_ring_in_global_scratch(chain, oracle, geometry, threads):
+    """The search's ring of tracks to follow in global scratch (one ring per resident CTA)
+    instead of shared memory: the same results, bit for bit, on an uneven slice; the setting
+    needs persistent launches."""
+    g = generator.generate(300, seed=79, pileup_min=1.0, pileup_max=15.0)
+    saved = chain.get_config()
+    try:
+        with pytest.raises(VeloError):
+            chain.configure(search_threads=threads, search_lanes_per_seed=0, persistent=0, search_ring_global=1)
+        chain.configure(search_threads=threads, search_lanes_per_seed=0, persistent=1, search_ring_global=1)
         totals, out = run_chain(chain, g.raw, use_graph=True)
         assert totals["device_flags"] == 0
         assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
