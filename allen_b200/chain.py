@@ -396,18 +396,22 @@ class VeloChain:
 class HostPipeline:
     """End-to-end processing of slices held in page-locked host memory, through the C ABI.
 
-    Two chains on two CUDA streams alternate: while one chain runs slice i, the other copies
-    slice i + 1 in and the consolidated tracks of slice i - 1 out, so the PCIe transfers
-    overlap the kernels.  Per slice the host receives dev_offsets_all_velo_tracks,
+    Three chains (by default) take the slices in turn, each on its own CUDA stream; the copies
+    run on two more streams, one per direction, so that a slice's input going in, another's
+    tracks coming out and a third one's kernels all overlap (PCIe is full duplex).  A chain's
+    next slice waits, through CUDA events, for its input copy and for the copy-out of the
+    chain's previous results.  Per slice the host receives dev_offsets_all_velo_tracks,
     dev_offsets_velo_track_hit_number and the id + xyz columns of dev_velo_track_hits
     (16 bytes per track hit; the phi column is never written by the reference).
     """
 
-    def __init__(self, geometry: bytes | None = None, n_chains: int = 2, **props):
+    def __init__(self, geometry: bytes | None = None, n_chains: int = 3, **props):
         import torch
         self.torch = torch
         self.chains = [VeloChain(geometry, **props) for _ in range(n_chains)]
         self.streams = [torch.cuda.Stream() for _ in range(n_chains)]
+        self.h2d_stream = torch.cuda.Stream()
+        self.d2h_stream = torch.cuda.Stream()
         self.dev_in = [None] * n_chains
         self.host_out = []
         self.h2d_bytes = 0
@@ -439,10 +443,12 @@ class HostPipeline:
         slice; the outputs of the first `keep_outputs` slices are returned as numpy arrays too."""
         torch = self.torch
         n_c = len(self.chains)
-        pending = [None] * n_c  # (slice index, out buffers) waiting for their results
+        pending = [None] * n_c   # (slice index, out buffers) whose results are still on the device
+        copied_out = [None] * n_c  # event: the chain's previous results are on the host
         totals_all, outputs = {}, {}
 
         def drain(ci):
+            """Waits for chain ci's last run and queues the copy of its results to the host."""
             if pending[ci] is None:
                 return
             k, bufs = pending[ci]
@@ -452,37 +458,46 @@ class HostPipeline:
             n = t["n_events"]
             tracks = t["host_number_of_reconstructed_velo_tracks"]
             TH = t["host_accumulated_number_of_hits_in_velo_tracks"]
-            stream = C.c_void_p(self.streams[ci].cuda_stream)
+            stream = C.c_void_p(self.d2h_stream.cuda_stream)
             sizes = ((bufs[0], p["dev_offsets_all_velo_tracks"], 4 * (n + 1)),
                      (bufs[1], p["dev_offsets_velo_track_hit_number"], 4 * (tracks + 1)),
                      (bufs[2], p["dev_velo_track_hits"], 16 * TH))
             for host, dev, nbytes in sizes:
                 _check(chain.lib, chain.lib.velo_copy_to_host_async(host.data_ptr(), dev, nbytes, stream))
                 self.d2h_bytes += nbytes
+            ev = torch.cuda.Event()
+            ev.record(self.d2h_stream)
+            copied_out[ci] = ev
             totals_all[k] = t
-            if k < keep_outputs:
-                self.streams[ci].synchronize()
-                outputs[k] = ({"dev_offsets_all_velo_tracks": bufs[0][:n + 1].numpy().view(np.uint32).copy(),
-                                "dev_offsets_velo_track_hit_number":
-                                    bufs[1][:tracks + 1].numpy().view(np.uint32).copy(),
-                                "dev_velo_track_hits_id_xyz": bufs[2][:16 * TH].numpy().copy()})
+            if k < keep_outputs:  # copied now: the host buffers are reused every 2 n_c slices
+                ev.synchronize()
+                outputs[k] = {"dev_offsets_all_velo_tracks": bufs[0][:n + 1].numpy().view(np.uint32).copy(),
+                              "dev_offsets_velo_track_hit_number":
+                                  bufs[1][:tracks + 1].numpy().view(np.uint32).copy(),
+                              "dev_velo_track_hits_id_xyz": bufs[2][:16 * TH].numpy().copy()}
             pending[ci] = None
 
         for k, s in enumerate(host_slices):
             ci = k % n_c
-            drain(ci)  # the slot's previous slice: its results go out while the other chain runs
+            drain(ci)  # the chain's previous slice: finished (host waits), its results queued out
             raw_t, off_t, siz_t, typ_t = self.dev_in[ci]
-            stream = self.streams[ci]
-            with torch.cuda.stream(stream):
+            with torch.cuda.stream(self.h2d_stream):
                 for dst, src in ((raw_t, s.raw.view(np.uint8)), (off_t, s.offsets.view(np.int32)),
                                  (siz_t, s.sizes.view(np.int32)), (typ_t, s.types.view(np.int32))):
                     dst[:src.size].copy_(torch.from_numpy(src), non_blocking=True)
                     self.h2d_bytes += src.nbytes
+            copied_in = torch.cuda.Event()
+            copied_in.record(self.h2d_stream)
+            stream = self.streams[ci]
+            stream.wait_event(copied_in)
+            if copied_out[ci] is not None:
+                stream.wait_event(copied_out[ci])  # the chain's outputs are about to be overwritten
             d = DeviceSlice(raw_t, off_t, siz_t, typ_t, s.n_events, s.bank_version)
             self.chains[ci].run(d, stream=C.c_void_p(stream.cuda_stream), use_graph=True)
             pending[ci] = (k, self._out_buffers(k % (2 * n_c)))
         for ci in range(n_c):
             drain(ci)
+        self.d2h_stream.synchronize()
         for st in self.streams:
             st.synchronize()
         return [totals_all[k] for k in sorted(totals_all)], [outputs[k] for k in sorted(outputs)]

@@ -79,18 +79,20 @@ def test_event_slice_offset(chain, oracle, geometry):
 
 
 def test_host_pipeline_matches_oracle(oracle, geometry):
-    """End-to-end path (page-locked host slices, two overlapping chains) against the oracle."""
+    """End-to-end path (page-locked host slices, three chains and two copy streams overlapping,
+    each chain taking several slices) against the oracle."""
     import torch
     from allen_b200.chain import HostPipeline
     from allen_b200.rawbanks import super_pixels_per_event
     import bench
-    slices = [generator.generate(30, seed=40 + i).raw for i in range(3)]
+    slices = [generator.generate(30, seed=40 + i).raw for i in range(8)]
     pinned = [bench.pin(s) for s in slices]
     pipe = HostPipeline()
     pipe.reserve(30, max(int(super_pixels_per_event(s).sum()) for s in slices) + 64,
                  max(s.raw.nbytes for s in slices), max(s.sizes.size for s in slices),
                  max(s.types.size for s in slices))
-    totals, outs = pipe.run(pinned, keep_outputs=3)
+    totals, outs = pipe.run(pinned, keep_outputs=8)
+    assert len(outs) == 8 and [t["n_events"] for t in totals] == [30] * 8
     pipe.close()
     for s, out in zip(slices, outs):
         ref = oracle.run(s, geometry)
