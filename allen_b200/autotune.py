@@ -1,8 +1,8 @@
 """Autotuner of the chain's launch configuration.
 
 Sweeps, on a generated workload of the target occupancy, the search kernel's block size and
-lanes per seed candidate (the compiled pairs), the shared-memory staging capacities of the
-search, clustering and estimate kernels, the place of the search's ring of tracks to follow, and
+lanes per seed candidate (the compiled pairs), the clustering kernel's block size, the
+shared-memory staging capacities of the search, clustering and estimate kernels, the place of the search's ring of tracks to follow, and
 persistent launches with a work queue (events claimed per CTA) against one CTA per event, by
 coordinate descent: each parameter in turn takes the
 value with the highest events/s (CUDA-event timed graph replays) while the others stay at
@@ -23,7 +23,8 @@ SEARCH_VARIANTS = [(128, 1, 0), (128, 2, 0), (256, 1, 0), (256, 2, 0), (256, 4, 
                    (128, 0, 0), (256, 0, 0), (512, 0, 0), (128, 0, 1), (256, 0, 1)]
 SEARCH_CAPACITIES = [0, 1024, 2048, 2560, 3072, 4096]
 CLUSTER_CAPACITIES = [0, 1024, 2048, 2560, 3072]
-CLUSTER_BLOBS = [16 * 1024, 24 * 1024, 32 * 1024, 40 * 1024]
+CLUSTER_BLOBS = [0, 16 * 1024, 24 * 1024, 32 * 1024, 40 * 1024]
+CLUSTER_THREADS = [256, 128]
 ESTIMATE_BLOBS = [24 * 1024, 32 * 1024, 48 * 1024]
 # (persistent, events per claim): one CTA per event, or resident CTAs claiming events
 QUEUES = [(0, 1), (1, 1), (1, 2), (1, 4)]
@@ -68,6 +69,7 @@ def tune(chain, dev_slices, log=print, max_sweeps: int = 3) -> tuple[dict, float
         ("search", SEARCH_VARIANTS),
         ("search_hit_capacity", SEARCH_CAPACITIES),
         ("cluster_stage_capacity", CLUSTER_CAPACITIES),
+        ("cluster_threads", CLUSTER_THREADS),
         ("cluster_blob_bytes", CLUSTER_BLOBS),
         ("estimate_blob_bytes", ESTIMATE_BLOBS),
         ("queue", QUEUES),

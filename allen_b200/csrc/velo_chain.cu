@@ -236,6 +236,7 @@ struct VeloChain {
   unsigned persistent = 0;
   unsigned events_per_claim = 1;
   unsigned search_ring_global = 0; // rings of tracks to follow in global scratch (persistent only)
+  unsigned cluster_threads = 256;  // block size of the clustering kernel (128 or 256)
   unsigned resident_estimate = 0, resident_cluster = 0, resident_search = 0; // CTAs that fit the device
 
   // workspace
@@ -246,6 +247,7 @@ struct VeloChain {
     event_track_hits, event_track_hit_base, offsets_all, track_hit_number, offsets_hit_number;
   DeviceBuffer<char> sorted, staging, track_hits, hit_scratch;
   DeviceBuffer<uint64_t> ring_scratch; // search_ring_global: one ring of 2048 entries per resident search CTA
+  DeviceBuffer<uint32_t> sp_scratch;   // sorted bank copies that do not fit the clustering kernel's blob
   DeviceBuffer<velo::TrackHits> tracks;
   DeviceBuffer<velo::TrackletHits> three_hit, three_out;
   DeviceBuffer<uint8_t> hit_used, accepted;
@@ -416,13 +418,19 @@ namespace {
       cp.module_cluster_num = c->cluster_num.p;
       cp.sorted_container = c->sorted.p;
       cp.staging = c->staging.p;
+      cp.candidates_offsets = c->candidates_offsets.p;
+      cp.sp_scratch = c->sp_scratch.p;
+      cp.sp_capacity = static_cast<unsigned>(c->sp_scratch.n);
       cp.status = c->status.p;
       cp.smem_blob_bytes = c->cluster_blob_bytes;
       cp.smem_cluster_capacity = c->cluster_stage_capacity;
       cp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
       const unsigned cluster_smem = cluster_sort_blob_offset(c->cluster_stage_capacity) + c->cluster_blob_bytes;
       cp.queue = queue(1);
-      cluster_sort_kernel<<<grid(c->resident_cluster), decode_threads, cluster_smem, stream>>>(cp);
+      if (c->cluster_threads == 128)
+        cluster_sort_kernel<128><<<grid(c->resident_cluster), 128, cluster_smem, stream>>>(cp);
+      else
+        cluster_sort_kernel<256><<<grid(c->resident_cluster), 256, cluster_smem, stream>>>(cp);
       VELO_CUDA(cudaGetLastError());
       VELO_CUDA(mark());
     }
@@ -524,7 +532,8 @@ namespace {
     const int cluster_smem = int(cluster_sort_blob_offset(c->cluster_stage_capacity) + c->cluster_blob_bytes);
     const int search_smem = int(c->search_hit_capacity * search_hit_bytes);
     VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(estimate_kernel), int(c->estimate_blob_bytes)));
-    VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(cluster_sort_kernel), cluster_smem));
+    VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(cluster_sort_kernel<128>), cluster_smem));
+    VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(cluster_sort_kernel<256>), cluster_smem));
     for (const auto& v : search_variants)
       VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(v.fn), search_smem));
     for (unsigned threads : {128u, 256u, 512u})
@@ -534,7 +543,10 @@ namespace {
     VELO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
     VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, estimate_kernel, decode_threads, c->estimate_blob_bytes));
     c->resident_estimate = unsigned(std::max(per_sm, 1) * sms);
-    VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel, decode_threads, cluster_smem));
+    if (c->cluster_threads == 128)
+      VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel<128>, 128, cluster_smem));
+    else
+      VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel<256>, 256, cluster_smem));
     c->resident_cluster = unsigned(std::max(per_sm, 1) * sms);
     const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes, c->search_ring_global);
     const SearchKernel learned = learned_search_kernel(c->search_threads);
@@ -668,6 +680,7 @@ VeloStatus velo_chain_reserve(
   RES(c->sorted, velo::element_size * T)
   RES(c->staging, 24 * T)
   RES(c->hit_scratch, 16 * T)
+  RES(c->sp_scratch, size_t(max_super_pixels) + 64)
   RES(c->track_hits, velo::element_size * track_hits)
   RES(c->tracks, tracks)
   RES(c->three_hit, tracks)
@@ -761,6 +774,8 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
                                      std::to_string(cfg->search_ring_global) + ")");
   if (cfg->search_ring_global && !cfg->persistent)
     return fail(VELO_ERR_ARGUMENT, "search_ring_global needs persistent launches (one ring per resident CTA)");
+  if (cfg->cluster_threads != 128 && cfg->cluster_threads != 256)
+    return fail(VELO_ERR_ARGUMENT, "cluster_threads must be 128 or 256");
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   const unsigned search_static = 32 * 1024; // upper bound of the kernel's static shared memory
@@ -780,6 +795,7 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
   c->persistent = cfg->persistent;
   c->events_per_claim = cfg->events_per_claim;
   c->search_ring_global = cfg->search_ring_global;
+  c->cluster_threads = cfg->cluster_threads;
   return configure_kernels(c);
 }
 
@@ -795,6 +811,7 @@ VeloStatus velo_chain_get_config(const VeloChain* c, VeloLaunchConfig* cfg)
   cfg->persistent = c->persistent;
   cfg->events_per_claim = c->events_per_claim;
   cfg->search_ring_global = c->search_ring_global;
+  cfg->cluster_threads = c->cluster_threads;
   return VELO_OK;
 }
 
@@ -1079,6 +1096,7 @@ void velo_chain_destroy(VeloChain* c)
   c->staging.release();
   c->hit_scratch.release();
   c->ring_scratch.release();
+  c->sp_scratch.release();
   c->track_hits.release();
   c->tracks.release();
   c->three_hit.release();

@@ -730,8 +730,9 @@ namespace velo {
   // ------------------------------------------------------------------------------------
   // cluster_sort_kernel
   // ------------------------------------------------------------------------------------
-  constexpr unsigned candidate_queue = 1024; // queued candidates per chunk of 512 SPs
-  static_assert((candidate_queue / 2) % decode_threads == 0, "every lane takes the same number of SPs per chunk");
+  // queued candidates per chunk of 2 THREADS SPs (two candidates at most per SP)
+  template<unsigned THREADS>
+  constexpr unsigned candidate_queue = 4 * THREADS;
 
   __device__ __forceinline__ unsigned sort_bucket(int16_t phi) { return static_cast<unsigned>(phi + 32768) >> 9; }
 
@@ -742,16 +743,18 @@ namespace velo {
     const uint32_t old = atomicAdd(reinterpret_cast<uint32_t*>(counters) + (b >> 1), 1u << shift);
     return static_cast<uint16_t>(old >> shift);
   }
+  template<unsigned THREADS>
   __device__ __forceinline__ void
   cluster_sort_event(const ClusterSortParams& p, unsigned e, uint64_t* bar, unsigned& bar_phase)
   {
+    constexpr unsigned queue_size = candidate_queue<THREADS>;
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ BankTable bt;
     __shared__ unsigned region[n_module_pairs + 1]; // estimated start of each module pair, event-relative
     __shared__ unsigned mp_count[n_module_pairs];
     __shared__ unsigned warp_sums[33];
     __shared__ unsigned sorted_total;
-    __shared__ uint32_t queue[candidate_queue];
+    __shared__ uint32_t queue[queue_size];
     __shared__ unsigned queue_count[2];
 
     const unsigned ev = e + p.in.event_start;
@@ -800,11 +803,17 @@ namespace velo {
     const uint32_t* words = stage_event(p.in, ev, blob, p.smem_blob_bytes, bar, bar_phase, p.status, n_words, staged);
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
     const uint32_t key_mask = sp_key_mask(version);
+    // sorted bank copies: behind the staged event (or at the start of the blob), else in the
+    // event's slice of the global scratch (L2-resident), else none (full neighbour scans)
     uint32_t* sorted = nullptr;
     if (staged + 4 * bt.total_sp <= p.smem_blob_bytes) {
-      sorted = reinterpret_cast<uint32_t*>(blob + staged); // behind the staged event, or at the start
-      sort_bank_words(bt, words, sorted, key_mask);
+      sorted = reinterpret_cast<uint32_t*>(blob + staged);
     }
+    else if (p.sp_scratch != nullptr) {
+      const unsigned sp_base = p.candidates_offsets[e] / 2;
+      if (sp_base + bt.total_sp <= p.sp_capacity) sorted = p.sp_scratch + sp_base;
+    }
+    if (sorted) sort_bank_words(bt, words, sorted, key_mask);
 
     const Geometry* g = p.geo;
     auto stage_cluster = [&](const ClusterOut& o, unsigned mp) {
@@ -827,8 +836,9 @@ namespace velo {
     // SPs (about two thirds, one table lookup each) and the flood fills of candidates:
     // pass 1 makes the clusters of isolated SPs and queues the candidates of the others
     // (EstimateInputSize.cu:72-204 order of codes), pass 2 runs rest_of_clusters on the
-    // queue.  A chunk has candidate_queue / 2 SPs, so the queue cannot overflow.
-    const unsigned chunk = candidate_queue / 2;
+    // queue.  A chunk has queue_size / 2 SPs, so the queue cannot overflow; every lane takes
+    // the same number of SPs per chunk.
+    const unsigned chunk = queue_size / 2;
     for (unsigned chunk_base = 0, parity = 0; chunk_base < bt.total_sp; chunk_base += chunk, parity ^= 1u) {
       for (unsigned f = chunk_base + threadIdx.x; f < chunk_base + chunk; f += blockDim.x) {
         uint32_t cand[2] = {0, 0};
@@ -879,7 +889,7 @@ namespace velo {
         }
       }
       __syncthreads();
-      const unsigned queued = min(queue_count[parity], candidate_queue);
+      const unsigned queued = min(queue_count[parity], queue_size);
       if (threadIdx.x == 0) queue_count[parity ^ 1u] = 0;
       for (unsigned q = threadIdx.x; q < queued; q += blockDim.x) {
         const uint32_t candidate = queue[q];
@@ -906,21 +916,24 @@ namespace velo {
     // cluster's rank is its bucket's start plus the number of smaller (phi, id) keys in the
     // same bucket - the same position as the reference's full count.
     {
-      const unsigned per = (sort_counters + blockDim.x - 1) / blockDim.x;
-      unsigned v[16];
+      // each thread owns `per` consecutive counters: it sums them, and after the scan turns
+      // them into starts in place (no other thread reads them in between)
+      constexpr unsigned per = (sort_counters + THREADS - 1) / THREADS;
       unsigned sum = 0;
       for (unsigned q = 0; q < per; ++q) {
         const unsigned b = threadIdx.x * per + q;
-        v[q & 15] = b < sort_counters ? bucket_start[b] : 0u;
-        sum += v[q & 15];
+        if (b < sort_counters) sum += bucket_start[b];
       }
       unsigned total;
       unsigned excl = block_exclusive_scan(sum, warp_sums, &total);
       if (threadIdx.x == 0) sorted_total = total;
       for (unsigned q = 0; q < per; ++q) {
         const unsigned b = threadIdx.x * per + q;
-        if (b < sort_counters) bucket_start[b] = static_cast<uint16_t>(excl);
-        excl += v[q & 15];
+        if (b < sort_counters) {
+          const unsigned count = bucket_start[b];
+          bucket_start[b] = static_cast<uint16_t>(excl);
+          excl += count;
+        }
       }
     }
     __syncthreads();
@@ -975,16 +988,21 @@ namespace velo {
     }
   }
 
-  // Capped for six CTAs per SM (42 registers, no spills): with the clusters staged through L2
-  // (cluster_stage_capacity 0) shared memory allows that many (measured +10 % on the chain).
-  __global__ void __launch_bounds__(decode_threads, 6) cluster_sort_kernel(ClusterSortParams p)
+  // Capped for 1536 threads per SM (40 registers, no spills: six 256-thread or twelve
+  // 128-thread CTAs): with the clusters staged through L2 (cluster_stage_capacity 0) shared
+  // memory allows that many (measured +10 % on the chain at 256 threads).
+  template<unsigned THREADS>
+  __global__ void __launch_bounds__(THREADS, 1536 / THREADS) cluster_sort_kernel(ClusterSortParams p)
   {
+    static_assert(THREADS == 128 || THREADS == 256, "block size");
     __shared__ __align__(8) uint64_t bar;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     unsigned bar_phase = 0;
-    for_each_event(p.queue, p.in.n_events, [&](unsigned e, unsigned) { cluster_sort_event(p, e, &bar, bar_phase); });
+    for_each_event(p.queue, p.in.n_events, [&](unsigned e, unsigned) { cluster_sort_event<THREADS>(p, e, &bar, bar_phase); });
   }
+  template __global__ void cluster_sort_kernel<128>(ClusterSortParams p);
+  template __global__ void cluster_sort_kernel<256>(ClusterSortParams p);
 
   // Events of the slice by raw size, largest first: a counting sort over 1024 size classes
   // of 64 bytes (order within a class is arbitrary).  One CTA of scan_threads threads.

@@ -69,6 +69,10 @@ namespace velo {
     unsigned* module_cluster_num;               // [26 N]     dev_module_cluster_num
     char* sorted_container;                     // [18 T]     dev_sorted_velo_cluster_container
     char* staging;                              // [24 T]     fallback staging for large events
+    const unsigned* candidates_offsets;         // [N + 1] dev_candidates_offsets (2 x SP words per event)
+    uint32_t* sp_scratch;                       // [S] sorted bank copies of events whose copies do not
+                                                //     fit the shared-memory blob (null: full scans)
+    unsigned sp_capacity;                       // S, allocated words of sp_scratch
     unsigned* status;
     unsigned smem_blob_bytes;
     unsigned smem_cluster_capacity;             // clusters staged in shared memory per event
@@ -158,6 +162,7 @@ namespace velo {
   }
 
   __global__ void estimate_kernel(EstimateParams p);
+  template<unsigned THREADS> // 128 or 256
   __global__ void cluster_sort_kernel(ClusterSortParams p);
   template<unsigned THREADS, unsigned LPH, unsigned RING>
   __global__ void search_by_triplet_kernel(SearchParams p);

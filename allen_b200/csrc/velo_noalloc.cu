@@ -155,7 +155,7 @@ namespace {
       const int cluster_smem = int(velo::cluster_sort_blob_offset(cluster_stage_capacity) + cluster_blob_bytes);
       if (velo::raise_dynamic_smem_limit(reinterpret_cast<const void*>(velo::estimate_kernel), int(estimate_blob_bytes)) !=
             cudaSuccess ||
-          velo::raise_dynamic_smem_limit(reinterpret_cast<const void*>(velo::cluster_sort_kernel), cluster_smem) !=
+          velo::raise_dynamic_smem_limit(reinterpret_cast<const void*>(velo::cluster_sort_kernel<velo::decode_threads>), cluster_smem) !=
             cudaSuccess)
         return fail(VELO_ERR_CUDA, "cannot set the kernels' shared-memory limits");
       scratch_address[device] = static_cast<unsigned char*>(ptr);
@@ -272,7 +272,7 @@ VeloStatus velo_decode_noalloc(
   cp.smem_cluster_capacity = cluster_stage_capacity;
   cp.cluster_capacity = static_cast<unsigned>(bound);
   const unsigned cluster_smem = cluster_sort_blob_offset(cluster_stage_capacity) + cluster_blob_bytes;
-  cluster_sort_kernel<<<n, decode_threads, cluster_smem, stream>>>(cp);
+  cluster_sort_kernel<decode_threads><<<n, decode_threads, cluster_smem, stream>>>(cp);
   const cudaError_t launch = cudaGetLastError();
   if (launch != cudaSuccess) return fail(VELO_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(launch));
   if (dev_status && cudaMemcpyAsync(dev_status, status, sizeof(unsigned), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)

@@ -199,6 +199,8 @@ typedef struct {
                                       global scratch instead of shared memory, leaving room for more
                                       resident CTAs; flat seeding with 128 or 256 threads, persistent
                                       launches only */
+  unsigned cluster_threads;        /* block size of the clustering kernel: 256, or 128 (twice the
+                                      resident CTAs per SM where shared memory allows) */
 } VeloLaunchConfig;
 VeloStatus velo_chain_configure(VeloChain* chain, const VeloLaunchConfig* config);
 VeloStatus velo_chain_get_config(const VeloChain* chain, VeloLaunchConfig* config);

@@ -104,12 +104,14 @@ def test_host_pipeline_matches_oracle(oracle, geometry):
 
 @pytest.mark.parametrize("threads,lanes", [(128, 1), (256, 2), (256, 4), (512, 4), (128, 0), (256, 0), (512, 0)])
 def test_search_variants_identical(chain, oracle, geometry, threads, lanes):
-    """Every compiled search configuration gives the same bit-exact result."""
+    """Every compiled search configuration gives the same bit-exact result (one CTA per event,
+    rings in shared memory; the tuned configuration's persistent launches with global rings are
+    what every other test runs)."""
     g = generator.generate(40, seed=77, pileup_min=1.0, pileup_max=15.0)
     saved = chain.get_config()
     try:
         chain.configure(search_threads=threads, search_lanes_per_seed=lanes, search_hit_capacity=2048,
-                        cluster_stage_capacity=2048)
+                        cluster_stage_capacity=2048, search_ring_global=0, persistent=0)
         totals, out = run_chain(chain, g.raw)
         assert totals["device_flags"] == 0
         assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
@@ -156,6 +158,23 @@ def test_persistent_work_queue_identical(chain, oracle, geometry, claim):
     saved = chain.get_config()
     try:
         chain.configure(persistent=1, events_per_claim=claim)
+        totals, out = run_chain(chain, g.raw, use_graph=True)
+        assert totals["device_flags"] == 0
+        assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
+    finally:
+        chain.configure(**saved)
+
+
+@pytest.mark.parametrize("threads,blob", [(128, 0), (128, 16384), (256, 0)])
+def test_cluster_block_size_and_global_sorted_copies(chain, oracle, geometry, threads, blob):
+    """The clustering kernel with 128 or 256 threads, its sorted bank copies in shared memory
+    or (blob 0: nothing staged) in the global scratch: the same results, bit for bit."""
+    g = generator.generate(200, seed=83, pileup_min=1.0, pileup_max=15.0)
+    saved = chain.get_config()
+    try:
+        with pytest.raises(VeloError):
+            chain.configure(cluster_threads=64)
+        chain.configure(cluster_threads=threads, cluster_blob_bytes=blob)
         totals, out = run_chain(chain, g.raw, use_graph=True)
         assert totals["device_flags"] == 0
         assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
