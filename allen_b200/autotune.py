@@ -25,7 +25,7 @@ SEARCH_CAPACITIES = [0, 1024, 2048, 2560, 3072, 4096]
 CLUSTER_CAPACITIES = [0, 1024, 2048, 2560, 3072]
 CLUSTER_BLOBS = [0, 16 * 1024, 24 * 1024, 32 * 1024, 40 * 1024]
 CLUSTER_THREADS = [256, 128]
-ESTIMATE_BLOBS = [24 * 1024, 32 * 1024, 48 * 1024]
+ESTIMATE_BLOBS = [0, 16 * 1024, 24 * 1024, 32 * 1024, 48 * 1024]
 # (persistent, events per claim): one CTA per event, or resident CTAs claiming events
 QUEUES = [(0, 1), (1, 1), (1, 2), (1, 4)]
 

@@ -192,12 +192,12 @@ static const SearchVariant search_variants[] = {
 static constexpr unsigned retina_key_capacity = 3072; // clusters of an event keyed in shared memory (24 KiB of keys, 6 KiB of order)
 static constexpr size_t n_sensors_total = velo::n_sensors;
 
-static SearchKernel learned_search_kernel(unsigned threads)
+static SearchKernel learned_search_kernel(unsigned threads, unsigned ring_global = 0)
 {
   switch (threads) {
-    case 128: return velo::search_by_triplet_learned_kernel<128>;
-    case 256: return velo::search_by_triplet_learned_kernel<256>;
-    case 512: return velo::search_by_triplet_learned_kernel<512>;
+    case 128: return ring_global ? velo::search_by_triplet_learned_kernel<128, 1> : velo::search_by_triplet_learned_kernel<128, 0>;
+    case 256: return ring_global ? velo::search_by_triplet_learned_kernel<256, 1> : velo::search_by_triplet_learned_kernel<256, 0>;
+    case 512: return ring_global ? nullptr : velo::search_by_triplet_learned_kernel<512, 0>;
     default: return nullptr;
   }
 }
@@ -465,7 +465,8 @@ namespace {
     sp.queue = queue(2);
     const unsigned search_smem = c->search_hit_capacity * search_hit_bytes;
     {
-      const SearchKernel fn = (c->learned || c->records) ? learned_search_kernel(c->search_threads) : nullptr;
+      const SearchKernel fn =
+        (c->learned || c->records) ? learned_search_kernel(c->search_threads, c->search_ring_global) : nullptr;
       const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes, c->search_ring_global);
       if (!fn && !v) return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for this launch configuration");
       void* args[] = {&sp};
@@ -537,7 +538,9 @@ namespace {
     for (const auto& v : search_variants)
       VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(v.fn), search_smem));
     for (unsigned threads : {128u, 256u, 512u})
-      VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(learned_search_kernel(threads)), search_smem));
+      for (unsigned ring : {0u, 1u})
+        if (learned_search_kernel(threads, ring))
+          VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(learned_search_kernel(threads, ring)), search_smem));
     // CTAs of each kernel resident on the device at once: the grid of a persistent launch
     int sms = 0, per_sm = 0;
     VELO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
@@ -549,17 +552,22 @@ namespace {
       VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel<256>, 256, cluster_smem));
     c->resident_cluster = unsigned(std::max(per_sm, 1) * sms);
     const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes, c->search_ring_global);
-    const SearchKernel learned = learned_search_kernel(c->search_threads);
+    const SearchKernel learned = learned_search_kernel(c->search_threads, c->search_ring_global);
     SearchKernel fn = (c->learned || c->records) && learned ? learned : (v ? v->fn : nullptr);
     if (fn) {
       VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, int(c->search_threads), search_smem));
       c->resident_search = unsigned(std::max(per_sm, 1) * sms);
     }
-    // the global rings: one per CTA of the persistent search grid (the plain kernel's grid;
-    // the learned kernel keeps its ring in shared memory)
-    if (c->search_ring_global && v) {
-      VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v->fn, int(c->search_threads), search_smem));
-      VELO_CUDA(c->ring_scratch.reserve(size_t(std::max(per_sm, 1)) * sms * max_tracks_to_follow));
+    // the global rings: one per CTA of the persistent search grid (plain or learned kernel,
+    // whichever has more resident CTAs, so that switching modes needs no new allocation)
+    if (c->search_ring_global) {
+      size_t ctas = 0;
+      for (SearchKernel k : {v ? v->fn : nullptr, learned}) {
+        if (!k) continue;
+        VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, int(c->search_threads), search_smem));
+        ctas = std::max(ctas, size_t(std::max(per_sm, 1)) * sms);
+      }
+      VELO_CUDA(c->ring_scratch.reserve(ctas * max_tracks_to_follow));
     }
     return VELO_OK;
   }
@@ -1038,8 +1046,8 @@ VeloStatus velo_chain_set_seed_model(VeloChain* c, const VeloSeedModel* model)
     c->learned = false;
     return configure_kernels(c); // the persistent grid follows the kernel the chain launches
   }
-  if (!learned_search_kernel(c->search_threads))
-    return fail(VELO_ERR_ARGUMENT, "the learned search needs search_threads 128, 256 or 512");
+  if (!learned_search_kernel(c->search_threads, c->search_ring_global))
+    return fail(VELO_ERR_ARGUMENT, "the learned search needs search_threads 128, 256 or 512 (128 or 256 with global rings)");
   std::vector<float> params(VELO_SEED_PARAMS);
   velo::model_params(*model, params.data());
   velo::MlpModelDevice d;
@@ -1055,8 +1063,8 @@ VeloStatus velo_chain_record_doublets(
 {
   if (!c) return fail(VELO_ERR_ARGUMENT, "null chain");
   if (records && (!dev_count || record_every == 0)) return fail(VELO_ERR_ARGUMENT, "recording needs a counter and record_every > 0");
-  if (records && !learned_search_kernel(c->search_threads))
-    return fail(VELO_ERR_ARGUMENT, "recording needs search_threads 128, 256 or 512");
+  if (records && !learned_search_kernel(c->search_threads, c->search_ring_global))
+    return fail(VELO_ERR_ARGUMENT, "recording needs search_threads 128, 256 or 512 (128 or 256 with global rings)");
   c->release_graph();
   c->records = reinterpret_cast<velo::DoubletRecord*>(records);
   c->record_count = records ? dev_count : nullptr;

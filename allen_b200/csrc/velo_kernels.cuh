@@ -166,8 +166,9 @@ namespace velo {
   __global__ void cluster_sort_kernel(ClusterSortParams p);
   template<unsigned THREADS, unsigned LPH, unsigned RING>
   __global__ void search_by_triplet_kernel(SearchParams p);
-  // flat seeding with the learned seed pruner and doublet recording, THREADS = 128, 256, 512
-  template<unsigned THREADS>
+  // flat seeding with the learned seed pruner and doublet recording, THREADS = 128, 256, 512;
+  // RING = 1 (128 and 256 threads): the ring of tracks to follow in global scratch
+  template<unsigned THREADS, unsigned RING>
   __global__ void search_by_triplet_learned_kernel(SearchParams p);
   // (block size, lanes per seed candidate) pairs compiled for the autotuner
 // lanes 0 = flattened seeding (one thread per h1 candidate)

@@ -934,12 +934,13 @@ namespace velo {
   // The learned search (flat seeding with the seed pruner; with seed_model null, the plain
   // search, recording training doublets when asked) is a kernel of its own, so the plain
   // kernels keep their register budget.
-  template<unsigned THREADS>
+  template<unsigned THREADS, unsigned RING>
   __global__ void __launch_bounds__(THREADS, 1024 / THREADS) search_by_triplet_learned_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ SearchSharedFlat s;
-    __shared__ uint64_t ring[max_tracks_to_follow];
+    __shared__ uint64_t ring_smem[RING ? 1 : max_tracks_to_follow];
+    uint64_t* ring = RING ? p.ring_scratch + size_t(blockIdx.x) * max_tracks_to_follow : ring_smem;
     for_each_event(p.queue, p.n_events, [&](unsigned e, unsigned) {
       const unsigned* start = p.offsets_estimated_input_size + e * n_module_pairs;
       const unsigned n_hits = start[n_module_pairs] - start[0];
@@ -952,8 +953,10 @@ namespace velo {
   template __global__ void search_by_triplet_kernel<T, L, R>(SearchParams p);
   VELO_SEARCH_CONFIGS(VELO_SEARCH_CONFIG)
 #undef VELO_SEARCH_CONFIG
-  template __global__ void search_by_triplet_learned_kernel<128>(SearchParams p);
-  template __global__ void search_by_triplet_learned_kernel<256>(SearchParams p);
-  template __global__ void search_by_triplet_learned_kernel<512>(SearchParams p);
+  template __global__ void search_by_triplet_learned_kernel<128, 0>(SearchParams p);
+  template __global__ void search_by_triplet_learned_kernel<256, 0>(SearchParams p);
+  template __global__ void search_by_triplet_learned_kernel<512, 0>(SearchParams p);
+  template __global__ void search_by_triplet_learned_kernel<128, 1>(SearchParams p);
+  template __global__ void search_by_triplet_learned_kernel<256, 1>(SearchParams p);
 
 } // namespace velo

@@ -106,8 +106,12 @@ def _model_keep_all(rec, n, **kw):
     return m
 
 
-def test_learned_search_keeping_every_doublet_is_the_plain_search(flat_chain, oracle, geometry):
+@pytest.mark.parametrize("threads,ring", [(256, 1), (128, 1), (256, 0)])
+def test_learned_search_keeping_every_doublet_is_the_plain_search(flat_chain, oracle, geometry, threads, ring):
+    """A model that keeps every doublet: the learned kernel (each block size, ring of tracks to
+    follow in global scratch or shared memory) gives the plain search's results bit for bit."""
     g = generator.generate(40, seed=63, pileup_min=1.0, pileup_max=15.0)
+    flat_chain.configure(search_threads=threads, search_ring_global=ring, persistent=1)
     rec, n = _records(flat_chain, g.raw, every=5)
     flat_chain.set_seed_model(_model_keep_all(rec, n))
     totals, out = _run(flat_chain, g.raw)
