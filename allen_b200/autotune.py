@@ -20,7 +20,7 @@ import time
 
 # (block size, lanes per seed candidate, ring of tracks to follow in global scratch)
 SEARCH_VARIANTS = [(128, 1, 0), (128, 2, 0), (256, 1, 0), (256, 2, 0), (256, 4, 0), (512, 2, 0), (512, 4, 0),
-                   (128, 0, 0), (256, 0, 0), (512, 0, 0), (128, 0, 1), (256, 0, 1)]
+                   (128, 0, 0), (256, 0, 0), (512, 0, 0), (64, 0, 1), (96, 0, 1), (128, 0, 1), (256, 0, 1)]
 SEARCH_CAPACITIES = [0, 1024, 2048, 2560, 3072, 4096]
 CLUSTER_CAPACITIES = [0, 1024, 2048, 2560, 3072]
 CLUSTER_BLOBS = [0, 16 * 1024, 24 * 1024, 32 * 1024, 40 * 1024]

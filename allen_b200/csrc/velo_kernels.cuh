@@ -174,7 +174,7 @@ namespace velo {
 // lanes 0 = flattened seeding (one thread per h1 candidate)
 #define VELO_SEARCH_CONFIGS(X)                                                                                  \
   X(128, 1, 0) X(128, 2, 0) X(256, 1, 0) X(256, 2, 0) X(256, 4, 0) X(512, 2, 0) X(512, 4, 0) X(128, 0, 0) X(256, 0, 0) \
-    X(512, 0, 0) X(128, 0, 1) X(256, 0, 1)
+    X(512, 0, 0) X(128, 0, 1) X(256, 0, 1) X(96, 0, 1) X(64, 0, 1)
   __global__ void consolidate_kernel(ConsolidateParams p);
   // ---- retina-cluster decoding (VPRetinaCluster banks) ----
   struct RetinaParams {

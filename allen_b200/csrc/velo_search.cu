@@ -34,7 +34,7 @@ namespace velo {
   constexpr uint64_t seed_flag = 1ull << 63;
   constexpr unsigned skipped_shift = 60;
   constexpr uint64_t track_number_mask64 = 0x0FFFFFFFull;
-  constexpr unsigned max_tail_tracks = 1024; // tracks whose tail lives in shared memory
+  constexpr unsigned max_tail_tracks = 512; // tracks whose tail lives in shared memory (the others: their container)
   constexpr unsigned n_buckets = 128;
   constexpr uint8_t flag_used = 1;
   constexpr uint8_t flag_odd_module = 2;
@@ -75,7 +75,8 @@ namespace velo {
   // plain flat-seeding kernels: 512 slots for 128 threads (chunks of 64 or 128 h1), which with
   // the ring in global scratch leaves room for twelve CTAs per SM
   template<unsigned THREADS>
-  using SearchSharedFlatPlain = SearchSharedFlatT<(THREADS <= 128 ? flat_slots / 2 : flat_slots), false>;
+  using SearchSharedFlatPlain =
+    SearchSharedFlatT<(THREADS <= 64 ? flat_slots / 4 : (THREADS <= 128 ? flat_slots / 2 : flat_slots)), false>;
 
   // Packed doublet: h0 | h1 index in the chunk << 16 | rank << 25 | (found - 1) << 28 | keep << 31
   __device__ __forceinline__ uint32_t pack_doublet(unsigned h0, unsigned h1_local, unsigned rank, unsigned found)

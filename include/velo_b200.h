@@ -197,8 +197,8 @@ typedef struct {
   unsigned events_per_claim;       /* events a persistent CTA claims at once (1..64) */
   unsigned search_ring_global;     /* 1: the search's ring of tracks to follow (16 KiB per CTA) lives in
                                       global scratch instead of shared memory, leaving room for more
-                                      resident CTAs; flat seeding with 128 or 256 threads, persistent
-                                      launches only */
+                                      resident CTAs; flat seeding with 64, 96, 128 or 256 threads,
+                                      persistent launches only */
   unsigned cluster_threads;        /* block size of the clustering kernel: 256, or 128 (twice the
                                       resident CTAs per SM where shared memory allows) */
 } VeloLaunchConfig;

@@ -182,7 +182,7 @@ def test_cluster_block_size_and_global_sorted_copies(chain, oracle, geometry, th
         chain.configure(**saved)
 
 
-@pytest.mark.parametrize("threads", [128, 256])
+@pytest.mark.parametrize("threads", [64, 96, 128, 256])
 def test_search_ring_in_global_scratch(chain, oracle, geometry, threads):
     """The search's ring of tracks to follow in global scratch (one ring per resident CTA)
     instead of shared memory: the same results, bit for bit, on an uneven slice; the setting
