@@ -988,11 +988,12 @@ namespace velo {
     }
   }
 
-  // Capped for 1536 threads per SM (40 registers, no spills: six 256-thread or twelve
-  // 128-thread CTAs): with the clusters staged through L2 (cluster_stage_capacity 0) shared
-  // memory allows that many (measured +10 % on the chain at 256 threads).
+  // Capped for 2048 threads per SM (32 registers, no spills: eight 256-thread CTAs, or
+  // twelve 128-thread ones where shared memory ends them): with the clusters staged through L2
+  // (cluster_stage_capacity 0) and no event staging (cluster_blob_bytes 0) shared memory allows
+  // that many; measured 2.59 -> 2.21 -> 2.13 ms per launch from six CTAs with staging.
   template<unsigned THREADS>
-  __global__ void __launch_bounds__(THREADS, 1536 / THREADS) cluster_sort_kernel(ClusterSortParams p)
+  __global__ void __launch_bounds__(THREADS, 2048 / THREADS) cluster_sort_kernel(ClusterSortParams p)
   {
     static_assert(THREADS == 128 || THREADS == 256, "block size");
     __shared__ __align__(8) uint64_t bar;
