@@ -57,11 +57,7 @@ def parse():
 # ----------------------------------------------------------------------------------
 # helpers
 # ----------------------------------------------------------------------------------
-def dist_env():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+from allen_b200.replicas import aggregate_rate, dist_env, max_over_ranks, rank_seed  # noqa: E402
 
 
 class ClockSampler:
@@ -276,20 +272,16 @@ def run_reference(args):
 # ----------------------------------------------------------------------------------
 def run_ours(args):
     import torch
-    world, rank, local = dist_env()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    else:
+    from allen_b200 import replicas
+    world, rank, local = replicas.init("nccl")
+    if world == 1:
         torch.cuda.set_device(0)
     from allen_b200 import _native
     from allen_b200.chain import VeloChain, upload
     from allen_b200.rawbanks import super_pixels_per_event
 
     geometry = _native.default_geometry()
-    seed = args.seed + 1_000_003 * rank
+    seed = rank_seed(args.seed, rank)
     slices = generate_slices(args.events, args.slice, seed)
     dev = [upload(s) for s in slices]
     sp_max = max(int(super_pixels_per_event(s).sum()) for s in slices)
@@ -333,13 +325,10 @@ def run_ours(args):
         torch.cuda.synchronize()
     ms = start.elapsed_time(end)
     totals_last = chain.synchronize(check=False)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        torch.distributed.barrier()
+    ms = max_over_ranks(ms)
+    replicas.barrier()
     events_step = sum(c["n"] for c in counts)
-    value = world * events_step * args.steps / (ms / 1e3)
+    value = aggregate_rate(world, events_step, args.steps, ms)
 
     # per-kernel durations of the last step (CUDA events captured inside the graphs)
     try:
@@ -401,10 +390,7 @@ def run_ours(args):
         l_end.record(stream)
         torch.cuda.synchronize()
         l_ms = l_start.elapsed_time(l_end)
-        if world > 1:
-            t = torch.tensor([l_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            l_ms = float(t.item())
+        l_ms = max_over_ranks(l_ms)
         doublets = scanned = fallback = 0
         for s, d in zip(slices, dev):
             chain.run(d, use_graph=True)
@@ -438,10 +424,7 @@ def run_ours(args):
         k_end.record(stream)
         torch.cuda.synchronize()
         k_ms = k_start.elapsed_time(k_end)
-        if world > 1:
-            t = torch.tensor([k_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            k_ms = float(t.item())
+        k_ms = max_over_ranks(k_ms)
         try:
             kt, kruns = chain.kernel_times()
             kf_ms = kt.get("kalman_filter_kernel", 0.0) / max(kruns, 1)
@@ -486,10 +469,7 @@ def run_ours(args):
         r_end.record(stream)
         torch.cuda.synchronize()
         r_ms = r_start.elapsed_time(r_end)
-        if world > 1:
-            t = torch.tensor([r_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            r_ms = float(t.item())
+        r_ms = max_over_ranks(r_ms)
         try:
             rt, rruns = chain.kernel_times()
             r_kernels = {"retina_count_kernel": round(rt["estimate_kernel"] / max(rruns, 1), 4),
@@ -529,10 +509,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         wall_ms = (time.perf_counter() - t0) * 1e3
         e_ms = max(e_start.elapsed_time(e_end), wall_ms)
-        if world > 1:
-            t = torch.tensor([e_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks(e_ms)
         e2e = {"value": round(world * events_step * e_steps / (e_ms / 1e3), 1), "unit": UNIT,
                "h2d_bytes_per_step": int(pipe.h2d_bytes / e_steps), "d2h_bytes_per_step": int(pipe.d2h_bytes / e_steps),
                "steps": e_steps, "api": "allen_b200.chain.HostPipeline (3 chains on 3 streams, one copy stream per direction, page-locked buffers; the steps' slices streamed back to back)"}
