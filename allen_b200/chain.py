@@ -429,6 +429,7 @@ class HostPipeline:
                               torch.empty(max_types_words, dtype=torch.int32, device="cuda"))
         self.max_super_pixels = max_super_pixels
         self.max_events = max_events
+        self._out_buffers(2 * len(self.chains) - 1)  # page-locked now, not inside a timed run
 
     def _out_buffers(self, k):
         torch = self.torch
