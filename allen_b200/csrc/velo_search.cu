@@ -913,10 +913,11 @@ namespace velo {
   // tracks to follow (2048 entries, 16 KiB) sits in shared memory, or with RING = 1 in this
   // CTA's slice of a global scratch (persistent launches only: the slice is the CTA's index),
   // which leaves room for more resident CTAs per SM.
-  // Flat-seeding kernels are register-capped for six 256-thread CTAs per SM (40 registers, a
-  // few spills): with the hits staged through L2 (search_hit_capacity 0) shared memory no
-  // longer limits the CTAs per SM, and the extra resident events hide more latency than the
-  // spills cost (measured, 5.87 against 5.72 ms per 16000 events at five and six CTAs).
+  // Flat-seeding kernels are register-capped for 1536 threads per SM (40 registers, a few
+  // spills): with the hits and the ring staged through L2 shared memory no longer limits the
+  // CTAs per SM, and the extra resident events hide more latency than the spills cost
+  // (measured per 16000-event launch: 5.87 / 5.72 ms at five / six 256-thread CTAs, 3.94 ms at
+  // twelve 128-thread CTAs; sixteen at 32 registers, 4.13 ms).
   template<unsigned THREADS, unsigned LPH, unsigned RING>
   __global__ void __launch_bounds__(THREADS, LPH == 0 ? 1536 / THREADS : 1) search_by_triplet_kernel(SearchParams p)
   {
