@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-kalman", action="store_true", help="skip the velo_kalman_filter measurement")
     p.add_argument("--no-retina", action="store_true", help="skip the retina-cluster front-end measurement")
     p.add_argument("--no-mdf", action="store_true", help="skip the host MDF transpose measurement")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the C2 (uneven pileup) and C4 (nu 15, noise, inefficiency) measurements")
     p.add_argument("--e2e-slice", type=int, default=4000,
                    help="events per slice of the end-to-end pipeline (smaller slices overlap the copies better)")
     return p.parse_args()
@@ -489,6 +491,44 @@ def run_ours(args):
         chain.set_front_end(False)
         del r_dev, r_slices
 
+    # the other workloads of the configuration table, same timing rules: C2 uneven pileup (nu
+    # uniform in 1..15) and C4 stress (nu = 15, noise 1e-4 per pixel, 95 % hit efficiency; slices of
+    # 4000, since 16000 such events overflow the 32-bit container offsets)
+    configs = None
+    if not args.no_configs:
+        configs = {}
+        for name, gen, slice_ in (("C2_uneven_nu1-15", dict(pileup_min=1.0, pileup_max=15.0), args.slice),
+                                  ("C4_nu15_noise1e-4_eff0.95",
+                                   dict(mean_pileup=15.0, noise_rate=1e-4, hit_efficiency=0.95), 4000)):
+            c_slices = generate_slices(args.events, slice_, seed + 17, **gen)
+            c_dev = [upload(x) for x in c_slices]
+            chain.reserve(max(x.n_events for x in c_slices), max(int(super_pixels_per_event(x).sum()) for x in c_slices) + 64,
+                          max(x.raw.nbytes for x in c_slices) + 64)
+
+            def c_step():
+                for d in c_dev:
+                    chain.run(d, use_graph=True)
+
+            for _ in range(max(3, args.warmup)):
+                c_step()
+            torch.cuda.synchronize()
+            replicas.barrier()
+            c_start, c_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c_start.record(stream)
+            for _ in range(args.steps):
+                c_step()
+            c_end.record(stream)
+            torch.cuda.synchronize()
+            c_ms = max_over_ranks(c_start.elapsed_time(c_end))
+            c_events = sum(x.n_events for x in c_slices)
+            c_flags = chain.synchronize(check=False)["device_flags"]
+            configs[name] = {"value": round(aggregate_rate(world, c_events, args.steps, c_ms), 1), "unit": UNIT,
+                             "slice": slice_, "events_per_step": c_events * world,
+                             "super_pixels_per_event": round(sum(int(super_pixels_per_event(x).sum()) for x in c_slices)
+                                                             / c_events, 1),
+                             "device_flags": c_flags}
+            del c_dev, c_slices
+
     # end to end through the public API from page-locked host buffers: HostPipeline copies each
     # slice in, runs the chain and copies the consolidated tracks out, two chains overlapping
     e2e = None
@@ -560,6 +600,7 @@ def run_ours(args):
             "kalman": kalman,
             "retina": retina,
             "mdf": mdf_in,
+            "configs": configs,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "device_flags": totals_last["device_flags"],
