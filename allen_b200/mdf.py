@@ -65,19 +65,34 @@ def read_file(path: str) -> np.ndarray:
     return np.fromfile(path, dtype=np.uint8)
 
 
-def scan(stream, check_checksum: bool = False, max_events: int | None = None) -> np.ndarray:
+def scan(stream, check_checksum: bool = False, max_events: int | None = None, batch: int = 65536) -> np.ndarray:
     """Index the complete records of ``stream``; raises MdfError on a bad, compressed or
-    (with ``check_checksum``) corrupted record."""
+    (with ``check_checksum``) corrupted record.  Indexes ``batch`` records per library call,
+    each call resuming where the previous one stopped."""
     s = _as_u8(stream)
-    cap = max_events if max_events is not None else max(1, s.size // 28)
-    events = np.zeros(cap, dtype=EVENT_DTYPE)
-    n, used = C.c_uint(0), C.c_size_t(0)
     lib = _lib()
-    st = lib.velo_mdf_scan(s.ctypes.data, s.size, int(check_checksum), events.ctypes.data, cap,
-                           C.byref(n), C.byref(used))
-    if st != OK:
-        raise MdfError(st, lib.velo_io_last_error().decode())
-    return events[:n.value]
+    parts, pos = [], 0
+    remaining = max_events if max_events is not None else None
+    while pos < s.size and (remaining is None or remaining > 0):
+        cap = batch if remaining is None else min(batch, remaining)
+        events = np.zeros(cap, dtype=EVENT_DTYPE)
+        n, used = C.c_uint(0), C.c_size_t(0)
+        st = lib.velo_mdf_scan(s.ctypes.data + pos, s.size - pos, int(check_checksum), events.ctypes.data, cap,
+                               C.byref(n), C.byref(used))
+        if st != OK:
+            raise MdfError(st, lib.velo_io_last_error().decode())
+        if n.value == 0:
+            break  # an incomplete record (or nothing) is left
+        events = events[:n.value]
+        events["record_offset"] += pos
+        events["banks_offset"] += pos
+        parts.append(events)
+        pos += used.value
+        if remaining is not None:
+            remaining -= n.value
+        if n.value < cap:
+            break
+    return np.concatenate(parts) if parts else np.zeros(0, dtype=EVENT_DTYPE)
 
 
 def select_by_source_id(stream, event) -> bool:

@@ -76,6 +76,9 @@ def test_scan_stops_before_an_incomplete_record_and_rejects_bad_headers():
     assert part.size == 2 and np.array_equal(part, full[:2])
     assert mdf.scan(stream, max_events=1).size == 1
     assert mdf.scan(b"").size == 0
+    # indexed in batches of one record per library call, resuming each time: the same index
+    assert np.array_equal(mdf.scan(stream, batch=1), full)
+    assert np.array_equal(mdf.scan(stream, batch=2, max_events=3), full)
     compressed = bytearray(stream)
     compressed[int(full[1]["record_offset"]) + 16] = 0x12  # zlib-style compression code
     with pytest.raises(mdf.MdfError) as e:
