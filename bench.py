@@ -365,16 +365,29 @@ def run_ours(args):
     peak = peaks.get("hbm_gbs", 6650.0)
     ach = per_kernel[dominant]["gbs"] if dominant else None
     traffic = None
-    try:  # ncu DRAM bytes per event of the dominant kernel, scaled to one launch
+    instructions = None
+    try:  # ncu DRAM bytes and warp instructions per event of the dominant kernel, scaled to one launch
         for line in open(os.path.join(REPO, "profiles", "dram_traffic.md")):
             cells = [c.strip() for c in line.strip().strip("|").split("|")]
             if len(cells) >= 2 and cells[0] == dominant:
                 traffic = int(float(cells[1]) * events_step / len(counts))
+                if len(cells) >= 4:
+                    instructions = float(cells[3]) * events_step / len(counts)
     except Exception:
         pass
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4) if ach else None, "traffic": traffic,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    # What bounds the dominant kernel instead: instruction issue.  One warp instruction per
+    # scheduler per cycle, four schedulers per SM, at the SM clock sampled during the timed region.
+    sm_mhz = clocks.summary().get("sm_mhz")
+    if instructions and sm_mhz and dominant:
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        issue_peak = 4 * sms * sm_mhz * 1e6
+        issue_ach = instructions / (per_kernel[dominant]["ms_per_launch"] / 1e3)
+        roofline["issue"] = {"achieved": round(issue_ach / 1e9, 1), "peak": round(issue_peak / 1e9, 1),
+                             "unit": "G warp instructions/s", "frac": round(issue_ach / issue_peak, 4),
+                             "instructions_per_launch": int(instructions)}
     chain_gbs = sum(chain_bytes(c["n"], c["raw_bytes"], c["H"], c["TH"], c["tracks_all"]) for c in counts) \
         * args.steps / (ms / 1e3) / 1e9
 
