@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--no-retina", action="store_true", help="skip the retina-cluster front-end measurement")
     p.add_argument("--no-mdf", action="store_true", help="skip the host MDF transpose measurement")
     p.add_argument("--no-configs", action="store_true",
-                   help="skip the C2 (uneven pileup) and C4 (nu 15, noise, inefficiency) measurements")
+                   help="skip the C1 small-slice, C2 (uneven pileup) and C4 (nu 15, noise, inefficiency) measurements")
     p.add_argument("--e2e-slice", type=int, default=4000,
                    help="events per slice of the end-to-end pipeline (smaller slices overlap the copies better)")
     return p.parse_args()
@@ -538,13 +538,15 @@ def run_ours(args):
                "api": "allen_b200.chain.HostPipeline (3 chains on 3 streams, one copy stream per direction, page-locked buffers; the steps' slices streamed back to back)"}
         pipe.close()
 
-    # the other workloads of the configuration table, same timing rules: C2 uneven pileup (nu
-    # uniform in 1..15) and C4 stress (nu = 15, noise 1e-4 per pixel, 95 % hit efficiency; slices of
-    # 4000, since 16000 such events overflow the 32-bit container offsets)
+    # the other workloads of the configuration table, same timing rules: C1's smaller slices (4000
+    # and 1000 events), C2 uneven pileup (nu uniform in 1..15) and C4 stress (nu = 15, noise 1e-4
+    # per pixel, 95 % hit efficiency; slices of 4000, since 16000 such events overflow the 32-bit
+    # container offsets)
     configs = None
     if not args.no_configs:
         configs = {}
-        for name, gen, slice_ in (("C2_uneven_nu1-15", dict(pileup_min=1.0, pileup_max=15.0), args.slice),
+        for name, gen, slice_ in (("C1_slice4000", dict(), 4000), ("C1_slice1000", dict(), 1000),
+                                  ("C2_uneven_nu1-15", dict(pileup_min=1.0, pileup_max=15.0), args.slice),
                                   ("C4_nu15_noise1e-4_eff0.95",
                                    dict(mean_pileup=15.0, noise_rate=1e-4, hit_efficiency=0.95), 4000)):
             c_slices = generate_slices(args.events, slice_, seed + 17, **gen)
