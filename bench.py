@@ -549,7 +549,8 @@ def run_ours(args):
                                   ("C2_uneven_nu1-15", dict(pileup_min=1.0, pileup_max=15.0), args.slice),
                                   ("C4_nu15_noise1e-4_eff0.95",
                                    dict(mean_pileup=15.0, noise_rate=1e-4, hit_efficiency=0.95), 4000)):
-            c_slices = generate_slices(args.events, slice_, seed + 17, **gen)
+            # C1: the main line's events in smaller slices; C2, C4: events of their own
+            c_slices = generate_slices(args.events, slice_, seed if name.startswith("C1") else seed + 17, **gen)
             c_dev = [upload(x) for x in c_slices]
             chain.reserve(max(x.n_events for x in c_slices), max(int(super_pixels_per_event(x).sum()) for x in c_slices) + 64,
                           max(x.raw.nbytes for x in c_slices) + 64)
