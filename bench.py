@@ -51,8 +51,8 @@ def parse():
     p.add_argument("--no-kalman", action="store_true", help="skip the velo_kalman_filter measurement")
     p.add_argument("--no-retina", action="store_true", help="skip the retina-cluster front-end measurement")
     p.add_argument("--no-mdf", action="store_true", help="skip the host MDF transpose measurement")
-    p.add_argument("--no-configs", action="store_true",
-                   help="skip the C1 small-slice, C2 (uneven pileup) and C4 (nu 15, noise, inefficiency) measurements")
+    p.add_argument("--no-workloads", action="store_true",
+                   help="skip the small-slice, uneven-pileup and stress (nu 15, noise, inefficiency) measurements")
     p.add_argument("--e2e-slice", type=int, default=4000,
                    help="events per slice of the end-to-end pipeline (smaller slices overlap the copies better)")
     return p.parse_args()
@@ -538,19 +538,18 @@ def run_ours(args):
                "api": "allen_b200.chain.HostPipeline (3 chains on 3 streams, one copy stream per direction, page-locked buffers; the steps' slices streamed back to back)"}
         pipe.close()
 
-    # the other workloads of the configuration table, same timing rules: C1's smaller slices (4000
-    # and 1000 events), C2 uneven pileup (nu uniform in 1..15) and C4 stress (nu = 15, noise 1e-4
-    # per pixel, 95 % hit efficiency; slices of 4000, since 16000 such events overflow the 32-bit
-    # container offsets)
-    configs = None
-    if not args.no_configs:
-        configs = {}
-        for name, gen, slice_ in (("C1_slice4000", dict(), 4000), ("C1_slice1000", dict(), 1000),
-                                  ("C2_uneven_nu1-15", dict(pileup_min=1.0, pileup_max=15.0), args.slice),
-                                  ("C4_nu15_noise1e-4_eff0.95",
+    # more workloads, same timing rules: the same events in slices of 4000 and 1000, uneven
+    # pileup (nu uniform in 1..15), and a stress workload (nu = 15, noise 1e-4 per pixel, 95 % hit
+    # efficiency; slices of 4000, since 16000 such events overflow the 32-bit container offsets)
+    workloads = None
+    if not args.no_workloads:
+        workloads = {}
+        for name, gen, slice_ in (("slice4000", dict(), 4000), ("slice1000", dict(), 1000),
+                                  ("uneven_nu1-15", dict(pileup_min=1.0, pileup_max=15.0), args.slice),
+                                  ("stress_nu15_noise1e-4_eff0.95",
                                    dict(mean_pileup=15.0, noise_rate=1e-4, hit_efficiency=0.95), 4000)):
-            # C1: the main line's events in smaller slices; C2, C4: events of their own
-            c_slices = generate_slices(args.events, slice_, seed if name.startswith("C1") else seed + 17, **gen)
+            # the slice lines re-slice the main line's events; the others have events of their own
+            c_slices = generate_slices(args.events, slice_, seed if name.startswith("slice") else seed + 17, **gen)
             c_dev = [upload(x) for x in c_slices]
             chain.reserve(max(x.n_events for x in c_slices), max(int(super_pixels_per_event(x).sum()) for x in c_slices) + 64,
                           max(x.raw.nbytes for x in c_slices) + 64)
@@ -572,7 +571,7 @@ def run_ours(args):
             c_ms = max_over_ranks(c_start.elapsed_time(c_end))
             c_events = sum(x.n_events for x in c_slices)
             c_flags = chain.synchronize(check=False)["device_flags"]
-            configs[name] = {"value": round(aggregate_rate(world, c_events, args.steps, c_ms), 1), "unit": UNIT,
+            workloads[name] = {"value": round(aggregate_rate(world, c_events, args.steps, c_ms), 1), "unit": UNIT,
                              "slice": slice_, "events_per_step": c_events * world,
                              "super_pixels_per_event": round(sum(int(super_pixels_per_event(x).sum()) for x in c_slices)
                                                              / c_events, 1),
@@ -616,7 +615,7 @@ def run_ours(args):
             "kalman": kalman,
             "retina": retina,
             "mdf": mdf_in,
-            "configs": configs,
+            "workloads": workloads,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "device_flags": totals_last["device_flags"],
