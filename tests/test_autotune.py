@@ -25,7 +25,7 @@ class FakeChain:
         if (c["search_threads"], c["search_lanes_per_seed"], c["search_ring_global"]) == (128, 0, 1):
             r *= 1.5 if c["search_hit_capacity"] == 0 else 0.7
         elif c["search_lanes_per_seed"] == 0:
-            r *= 1.2
+            r *= 1.2 if c["search_threads"] == 256 else 1.1
         r *= 1.1 if c["search_hit_capacity"] == 0 else 1.0
         r *= 1.05 if c["persistent"] else 1.0
         return r
