@@ -229,3 +229,23 @@ def test_mep_layout(chain, oracle, geometry, cfg):
     totals, out = run_chain(chain, m, use_graph=True)
     assert totals["device_flags"] == 0
     assert parity.compare(out, oracle.run(g.raw, geometry), g.raw.n_events) == []
+
+
+def test_full_size_slice(chain, oracle, geometry):
+    """A slice of the benchmark's size (16000 events at nu = 7.6) with the tuned configuration:
+    bit for bit the oracle's, and the same as with one CTA per event, shared-memory rings and
+    staging (the other code paths of every kernel)."""
+    g = generator.generate(16000, seed=2024)
+    saved = chain.get_config()
+    try:
+        totals, tuned = run_chain(chain, g.raw, use_graph=True)
+        assert totals["device_flags"] == 0
+        assert parity.compare(tuned, oracle.run(g.raw, geometry), g.raw.n_events) == []
+        chain.configure(search_threads=256, search_lanes_per_seed=0, search_ring_global=0, persistent=0,
+                        search_hit_capacity=3072, cluster_stage_capacity=2560, cluster_blob_bytes=32768,
+                        estimate_blob_bytes=32768, cluster_threads=256)
+        totals2, other = run_chain(chain, g.raw, use_graph=True)
+        assert totals2 == totals
+        assert parity.compare(other, tuned, g.raw.n_events) == []
+    finally:
+        chain.configure(**saved)
