@@ -394,6 +394,26 @@ class VeloChain:
         return totals, out, up.value, down.value
 
 
+def pin_slice(s: RawSlice) -> RawSlice:
+    """A copy of ``s`` in page-locked host memory (numpy views of pinned torch tensors), as
+    HostPipeline.run takes its slices."""
+    import torch
+
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy()
+        v[:] = np.ascontiguousarray(a).view(np.uint8).reshape(-1)
+        return v.view(a.dtype), t
+
+    raw, t0 = pinned(s.raw)
+    off, t1 = pinned(s.offsets)
+    siz, t2 = pinned(s.sizes)
+    typ, t3 = pinned(s.types)
+    r = RawSlice(raw, off, siz, typ, s.bank_version, getattr(s, "mep", False))
+    r._keep = (t0, t1, t2, t3)
+    return r
+
+
 class HostPipeline:
     """End-to-end processing of slices held in page-locked host memory, through the C ABI.
 
@@ -480,6 +500,8 @@ class HostPipeline:
             pending[ci] = None
 
         for k, s in enumerate(host_slices):
+            if getattr(s, "mep", False):
+                raise ValueError("HostPipeline takes Allen-layout slices (upload MEPs with chain.upload)")
             ci = k % n_c
             drain(ci)  # the chain's previous slice: finished (host waits), its results queued out
             raw_t, off_t, siz_t, typ_t = self.dev_in[ci]
@@ -494,7 +516,7 @@ class HostPipeline:
             stream.wait_event(copied_in)
             if copied_out[ci] is not None:
                 stream.wait_event(copied_out[ci])  # the chain's outputs are about to be overwritten
-            d = DeviceSlice(raw_t, off_t, siz_t, typ_t, s.n_events, s.bank_version)
+            d = DeviceSlice(raw_t, off_t, siz_t, typ_t, s.n_events, s.bank_version, 0, s.retina)
             self.chains[ci].run(d, stream=C.c_void_p(stream.cuda_stream), use_graph=True)
             pending[ci] = (k, self._out_buffers(k % (2 * n_c)))
         for ci in range(n_c):

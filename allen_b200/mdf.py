@@ -134,6 +134,19 @@ def transpose_vp(stream, events: np.ndarray, by_source_id: bool | None = None,
                     bank_version=int(info.bank_version))
 
 
+def slices(stream, events_per_slice: int = 4000, check_checksum: bool = False, by_source_id: bool | None = None,
+           n_threads: int = 0):
+    """The VELO slices of consecutive groups of ``events_per_slice`` records of ``stream``, one
+    RawSlice at a time (for HostPipeline: ``chain.pin_slice`` each)."""
+    s = _as_u8(stream)
+    index = scan(s, check_checksum=check_checksum)
+    if by_source_id is None and index.size:
+        by_source_id = select_by_source_id(s, index[0])
+    for first in range(0, index.size, events_per_slice):
+        yield transpose_vp(s, index[first:first + events_per_slice], by_source_id=bool(by_source_id),
+                           n_threads=n_threads)
+
+
 def write_records(events, header_version: int = 3, checksum: bool = True) -> bytes:
     """An MDF byte stream of uncompressed records (test and tooling helper).
 

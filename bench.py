@@ -122,23 +122,8 @@ def generate_slices(n_events, slice_size, seed, pinned=False, **gen):
 
 
 def pin(s):
-    """Copies a RawSlice into page-locked host memory (numpy views of pinned torch tensors)."""
-    import torch
-    from allen_b200.rawbanks import RawSlice
-
-    def p(a):
-        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
-        v = t.numpy()
-        v[:] = a.view(np.uint8)
-        return v.view(a.dtype), t
-
-    raw, t0 = p(s.raw)
-    off, t1 = p(s.offsets)
-    siz, t2 = p(s.sizes)
-    typ, t3 = p(s.types)
-    r = RawSlice(raw, off, siz, typ, s.bank_version)
-    r._keep = (t0, t1, t2, t3)
-    return r
+    from allen_b200.chain import pin_slice
+    return pin_slice(s)
 
 
 def kernel_bytes(n, raw_bytes, T, H, n4, n3_all, n3_out, TH, tracks_all):
