@@ -523,44 +523,80 @@ def run_ours(args):
                "api": "allen_b200.chain.HostPipeline (3 chains on 3 streams, one copy stream per direction, page-locked buffers; the steps' slices streamed back to back)"}
         pipe.close()
 
-    # more workloads, same timing rules: the same events in slices of 4000 and 1000, uneven
-    # pileup (nu uniform in 1..15), and a stress workload (nu = 15, noise 1e-4 per pixel, 95 % hit
-    # efficiency; slices of 4000, since 16000 such events overflow the 32-bit container offsets)
+    # more workloads, same timing rules: the same events in slices of 4000 and 1000; uneven pileup
+    # (nu uniform in 1..15, twice the events), also run as per-stage launches (one CTA per event,
+    # rings in shared memory, no CUDA graph) for comparison; a stress workload (nu = 15, noise 1e-4
+    # per pixel, 95 % hit efficiency; slices of 4000, since 16000 such events overflow the 32-bit
+    # container offsets), also in learned mode
+    def timed(dev_list, use_graph=True):
+        def once():
+            for d in dev_list:
+                chain.run(d, use_graph=use_graph)
+        for _ in range(max(3, args.warmup)):
+            once()
+        torch.cuda.synchronize()
+        replicas.barrier()
+        t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for _ in range(args.steps):
+            once()
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(t_start.elapsed_time(t_end))
+
     workloads = None
     if not args.no_workloads:
         workloads = {}
-        for name, gen, slice_ in (("slice4000", dict(), 4000), ("slice1000", dict(), 1000),
-                                  ("uneven_nu1-15", dict(pileup_min=1.0, pileup_max=15.0), args.slice),
-                                  ("stress_nu15_noise1e-4_eff0.95",
-                                   dict(mean_pileup=15.0, noise_rate=1e-4, hit_efficiency=0.95), 4000)):
+        for name, gen, n_ev, slice_ in (("slice4000", dict(), args.events, 4000),
+                                        ("slice1000", dict(), args.events, 1000),
+                                        ("uneven_nu1-15", dict(pileup_min=1.0, pileup_max=15.0), 2 * args.events,
+                                         args.slice),
+                                        ("stress_nu15_noise1e-4_eff0.95",
+                                         dict(mean_pileup=15.0, noise_rate=1e-4, hit_efficiency=0.95), args.events,
+                                         4000)):
             # the slice lines re-slice the main line's events; the others have events of their own
-            c_slices = generate_slices(args.events, slice_, seed if name.startswith("slice") else seed + 17, **gen)
+            c_slices = generate_slices(n_ev, slice_, seed if name.startswith("slice") else seed + 17, **gen)
             c_dev = [upload(x) for x in c_slices]
             chain.reserve(max(x.n_events for x in c_slices), max(int(super_pixels_per_event(x).sum()) for x in c_slices) + 64,
                           max(x.raw.nbytes for x in c_slices) + 64)
-
-            def c_step():
-                for d in c_dev:
-                    chain.run(d, use_graph=True)
-
-            for _ in range(max(3, args.warmup)):
-                c_step()
-            torch.cuda.synchronize()
-            replicas.barrier()
-            c_start, c_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            c_start.record(stream)
-            for _ in range(args.steps):
-                c_step()
-            c_end.record(stream)
-            torch.cuda.synchronize()
-            c_ms = max_over_ranks(c_start.elapsed_time(c_end))
             c_events = sum(x.n_events for x in c_slices)
+            c_ms = timed(c_dev)
             c_flags = chain.synchronize(check=False)["device_flags"]
-            workloads[name] = {"value": round(aggregate_rate(world, c_events, args.steps, c_ms), 1), "unit": UNIT,
-                             "slice": slice_, "events_per_step": c_events * world,
-                             "super_pixels_per_event": round(sum(int(super_pixels_per_event(x).sum()) for x in c_slices)
-                                                             / c_events, 1),
-                             "device_flags": c_flags}
+            entry = {"value": round(aggregate_rate(world, c_events, args.steps, c_ms), 1), "unit": UNIT,
+                     "slice": slice_, "events_per_step": c_events * world,
+                     "super_pixels_per_event": round(sum(int(super_pixels_per_event(x).sum()) for x in c_slices)
+                                                     / c_events, 1),
+                     "device_flags": c_flags}
+            if name.startswith("uneven"):
+                tuned = chain.get_config()
+                chain.configure(search_threads=256, search_lanes_per_seed=0, search_ring_global=0, persistent=0,
+                                search_hit_capacity=2560, cluster_stage_capacity=2560, cluster_blob_bytes=32768,
+                                estimate_blob_bytes=24576)
+                p_ms = timed(c_dev, use_graph=False)
+                chain.configure(**tuned)
+                entry["per_stage_launches"] = {
+                    "value": round(aggregate_rate(world, c_events, args.steps, p_ms), 1), "unit": UNIT,
+                    "how": "one CTA per event (rings and staging in shared memory), kernels launched one by one "
+                           "without a CUDA graph"}
+            if name.startswith("stress") and not args.no_learned:
+                from allen_b200 import seed_pruner
+                chain.set_seed_model(seed_pruner.load(os.path.join(REPO, "allen_b200", "data", "seed_pruner.npz")))
+                l_ms = timed(c_dev)
+                fb = sc = db = 0
+                for x, d in zip(c_slices, c_dev):
+                    chain.run(d, use_graph=True)
+                    chain.synchronize(check=False)
+                    st = chain.seed_stats(x.n_events)
+                    db += int(st[:, 0].sum())
+                    sc += int(st[:, 1].sum())
+                    fb += int((st[:, 2] == 2).sum())
+                chain.set_seed_model(None)
+                l_val = aggregate_rate(world, c_events, args.steps, l_ms)
+                entry["learned"] = {"value": round(l_val, 1), "unit": UNIT,
+                                    "ratio_vs_plain": round(l_val / entry["value"], 4),
+                                    "doublets_scanned_fraction": round(sc / max(db, 1), 4),
+                                    "fallback_event_fraction": round(fb / max(c_events, 1), 6)}
+            workloads[name] = entry
             del c_dev, c_slices
 
     cpu = None
