@@ -55,6 +55,7 @@ def parse():
                    help="skip the small-slice, uneven-pileup and stress (nu 15, noise, inefficiency) measurements")
     p.add_argument("--e2e-slice", type=int, default=4000,
                    help="events per slice of the end-to-end pipeline (smaller slices overlap the copies better)")
+    p.add_argument("--e2e-chains", type=int, default=3, help="chains (streams) of the end-to-end pipeline")
     return p.parse_args()
 
 
@@ -498,7 +499,7 @@ def run_ours(args):
         e_slices = slices if args.e2e_slice == args.slice else generate_slices(args.events, args.e2e_slice, seed)
         pinned = [pin(s) for s in e_slices]
         e_sp_max = max(int(super_pixels_per_event(s).sum()) for s in e_slices)
-        pipe = HostPipeline(geometry)
+        pipe = HostPipeline(geometry, n_chains=args.e2e_chains)
         pipe.reserve(max(s.n_events for s in e_slices), e_sp_max + 64, max(s.raw.nbytes for s in e_slices),
                      max(s.sizes.size for s in e_slices), max(s.types.size for s in e_slices))
         pipe.run(pinned)  # warm-up: graph capture per chain
@@ -517,10 +518,27 @@ def run_ours(args):
         wall_ms = (time.perf_counter() - t0) * 1e3
         e_ms = max(e_start.elapsed_time(e_end), wall_ms)
         e_ms = max_over_ranks(e_ms)
+        # the copy rates the pipeline is up against: one 256 MiB page-locked copy each way
+        link = {}
+        n_b = 1 << 28
+        h_buf = torch.empty(n_b, dtype=torch.uint8, pin_memory=True)
+        d_buf = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+        for direction, copy in (("h2d_gbs", lambda: d_buf.copy_(h_buf, non_blocking=True)),
+                                ("d2h_gbs", lambda: h_buf.copy_(d_buf, non_blocking=True))):
+            copy()
+            torch.cuda.synchronize()
+            b_start, b_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            b_start.record()
+            for _ in range(4):
+                copy()
+            b_end.record()
+            torch.cuda.synchronize()
+            link[direction] = round(4 * n_b / (b_start.elapsed_time(b_end) / 1e3) / 1e9, 1)
+        del h_buf, d_buf
         e2e = {"value": round(world * events_step * e_steps / (e_ms / 1e3), 1), "unit": UNIT,
                "h2d_bytes_per_step": int(pipe.h2d_bytes / e_steps), "d2h_bytes_per_step": int(pipe.d2h_bytes / e_steps),
-               "steps": e_steps, "slice": args.e2e_slice,
-               "api": "allen_b200.chain.HostPipeline (3 chains on 3 streams, one copy stream per direction, page-locked buffers; the steps' slices streamed back to back)"}
+               "steps": e_steps, "slice": args.e2e_slice, "chains": args.e2e_chains, "pinned_copy": link,
+               "api": "allen_b200.chain.HostPipeline (chains on their own streams, one copy stream per direction, page-locked buffers; the steps' slices streamed back to back)"}
         pipe.close()
 
     # more workloads, same timing rules: the same events in slices of 4000 and 1000; uneven pileup
