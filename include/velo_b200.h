@@ -182,8 +182,12 @@ VeloStatus velo_chain_outputs(const VeloChain* chain, VeloChainOutputs* outputs)
 /* Launch configuration (no counterpart in the reference, whose block sizes are algorithm
  * PROPERTYs, e.g. SearchByTriplet.cuh:132): block size and lanes per seed candidate of the
  * search kernel (a compiled pair: (128,1) (128,2) (256,1) (256,2) (256,4) (512,2) (512,4), and
- * lanes 0 = flattened seeding, one thread per h1 candidate: (128,0) (256,0) (512,0)),
- * and the shared-memory staging capacities.  Chosen by allen_b200/autotune.py. */
+ * lanes 0 = flattened seeding, one thread per h1 candidate: (128,0) (256,0) (512,0), and with
+ * search_ring_global (64,0) (96,0) (128,0) (256,0)), the shared-memory staging capacities (0:
+ * staged in L2-resident global scratch, or not staged for the raw-event blobs), the work queue
+ * and the clustering block size.  Chosen by allen_b200/autotune.py; the chain starts from
+ * allen_b200/data/launch_config.json through the Python binding, from fixed defaults through the
+ * C ABI. */
 typedef struct {
   unsigned search_threads;
   unsigned search_lanes_per_seed;
