@@ -189,7 +189,11 @@ static const SearchVariant search_variants[] = {
 #undef VELO_SEARCH_VARIANT
 };
 
-static constexpr unsigned retina_key_capacity = 3072; // clusters of an event keyed in shared memory (24 KiB of keys, 6 KiB of order)
+// Retina decoding: keys of an event in L2-resident global scratch (shared memory would hold 24 KiB
+// for 3072 keys and allow six CTAs per SM instead of eight), the bucket order of up to 8192
+// clusters in shared memory (16 KiB).
+static constexpr unsigned retina_key_capacity = 0;
+static constexpr unsigned retina_order_capacity = 8192;
 static constexpr size_t n_sensors_total = velo::n_sensors;
 
 static SearchKernel learned_search_kernel(unsigned threads, unsigned ring_global = 0)
@@ -369,6 +373,7 @@ namespace {
       rp.key_scratch = c->retina_keys.p;
       rp.status = c->status.p;
       rp.smem_key_capacity = retina_key_capacity;
+      rp.smem_order_capacity = retina_order_capacity;
       rp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
       VELO_CUDA(cudaMemsetAsync(c->retina_bank_index.p, 0, n_sensors * sizeof(unsigned), stream));
       VELO_CUDA(cudaMemsetAsync(c->candidates_offsets.p, 0, (n + 1) * sizeof(unsigned), stream));
@@ -380,7 +385,8 @@ namespace {
       exclusive_scan_kernel<<<1, scan_threads, 0, stream>>>(rs);
       VELO_CUDA(cudaGetLastError());
       VELO_CUDA(mark());
-      retina_decode_kernel<<<n, decode_threads, retina_key_capacity * (sizeof(long long) + sizeof(uint16_t)), stream>>>(rp);
+      retina_decode_kernel<<<n, decode_threads,
+                             retina_key_capacity * sizeof(long long) + retina_order_capacity * sizeof(uint16_t), stream>>>(rp);
       VELO_CUDA(cudaGetLastError());
       VELO_CUDA(mark());
     }

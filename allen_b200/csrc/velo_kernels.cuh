@@ -192,6 +192,7 @@ namespace velo {
     long long* key_scratch;                  // [T] keys of events above the shared-memory capacity
     unsigned* status;
     unsigned smem_key_capacity;              // clusters of an event keyed in shared memory
+    unsigned smem_order_capacity;            // clusters of an event ranked through key buckets
     unsigned cluster_capacity;               // allocated T
   };
   __global__ void retina_count_kernel(RetinaParams p);

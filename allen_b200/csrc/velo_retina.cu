@@ -190,7 +190,9 @@ namespace velo {
     return (old >> shift) & 0xFFFFu;
   }
 
-  __global__ void __launch_bounds__(decode_threads) retina_decode_kernel(RetinaParams p)
+  // Capped for eight CTAs per SM (32 registers): with the keys in L2-resident scratch the
+  // shared memory (bucket order and counters, 13 KB) allows that many.
+  __global__ void __launch_bounds__(decode_threads, 8) retina_decode_kernel(RetinaParams p)
   {
     extern __shared__ __align__(16) unsigned char dsmem[];
     __shared__ unsigned so[n_sensors + 1]; // event-relative sensor offsets
@@ -233,10 +235,12 @@ namespace velo {
     // populate_module_pair_offsets_and_sizes (DecodeRetinaClusters.cu:11-35)
     if (threadIdx.x < n_module_pairs) p.offsets_module_pair_cluster[e * n_module_pairs + threadIdx.x + 1] = base + so[(threadIdx.x + 1) * step];
 
-    // keys (and the bucket order) in shared memory when the event fits, else keys in its slice
-    // of the global scratch
-    const bool in_smem = total <= p.smem_key_capacity;
-    int64_t* keys = in_smem ? reinterpret_cast<int64_t*>(dsmem) : reinterpret_cast<int64_t*>(p.key_scratch) + base;
+    // keys in shared memory when the event fits the key capacity, else in its slice of the global
+    // (L2-resident) scratch; the bucket order in shared memory behind them when the event fits the
+    // order capacity, else no buckets (the full comparison)
+    const bool keys_in_smem = total <= p.smem_key_capacity;
+    const bool in_smem = total <= p.smem_order_capacity; // the bucketed rank
+    int64_t* keys = keys_in_smem ? reinterpret_cast<int64_t*>(dsmem) : reinterpret_cast<int64_t*>(p.key_scratch) + base;
     uint16_t* order = reinterpret_cast<uint16_t*>(dsmem + size_t(p.smem_key_capacity) * sizeof(int64_t));
     const Geometry* g = p.geo;
     const Constants k = p.k;
