@@ -322,7 +322,7 @@ namespace {
     p.beamline_states = c->kalman_beamline_states.p;
     p.endvelo_states = c->kalman_endvelo_states.p;
     p.status = c->status.p;
-    const unsigned blocks = std::min<unsigned>(unsigned((c->cap_tracks + 255) / 256), 148u * 8u);
+    const unsigned blocks = std::min<unsigned>(unsigned((c->cap_tracks + 255) / 256), 148u * velo::kalman_ctas_per_sm);
     velo::kalman_filter_kernel<<<std::max(blocks, 1u), velo::kalman_threads, 0, stream>>>(p);
     VELO_CUDA(cudaGetLastError());
     return VELO_OK;
@@ -1038,7 +1038,7 @@ VeloStatus velo_kalman_filter(
   p.beamline_states = reinterpret_cast<float*>(dev_velo_kalman_beamline_states);
   p.endvelo_states = reinterpret_cast<float*>(dev_velo_kalman_endvelo_states);
   p.status = dev_status;
-  const unsigned blocks = std::min<unsigned>((track_capacity + 255) / 256, 148u * 8u);
+  const unsigned blocks = std::min<unsigned>((track_capacity + 255) / 256, 148u * velo::kalman_ctas_per_sm);
   velo::kalman_filter_kernel<<<std::max(blocks, 1u), velo::kalman_threads, 0, static_cast<cudaStream_t>(stream)>>>(p);
   VELO_CUDA(cudaGetLastError());
   return VELO_OK;

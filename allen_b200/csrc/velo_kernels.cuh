@@ -230,6 +230,8 @@ namespace velo {
 
   constexpr unsigned decode_threads = 256;
   constexpr unsigned kalman_threads = 256;
+  constexpr unsigned kalman_ctas_per_sm = 6; // 40 registers a thread; the grid is one wave of 148 SMs
+  constexpr unsigned kalman_warp_hits = 368; // hits of a warp's 32 tracks staged in shared memory (4.4 KB)
   constexpr unsigned scan_threads = 1024;
   constexpr unsigned consolidate_threads = 256;
   constexpr unsigned search_hit_bytes = 15; // x, y, z, phi, flags per staged hit
