@@ -189,7 +189,7 @@ namespace velo {
     unsigned* offsets_module_pair_cluster;   // [26 N + 1] the search's dev_offsets_estimated_input_size
     unsigned* module_cluster_num;            // [26 N]
     char* container;                         // [18 T] dev_velo_cluster_container (sorted)
-    long long* key_scratch;                  // [T] keys of events above the shared-memory capacity
+    long long* key_scratch;                  // [T] cluster keys of the events not keyed in shared memory
     unsigned* status;
     unsigned smem_key_capacity;              // clusters of an event keyed in shared memory
     unsigned smem_order_capacity;            // clusters of an event ranked through key buckets
