@@ -132,7 +132,8 @@ def main():
     chain.reserve(max(s.n_events for s in slices), max(int(super_pixels_per_event(s).sum()) for s in slices) + 64)
     t0 = time.time()
     best, rate, trials = tune(chain, dev)
-    result = {"config": best, "events_per_s": rate, "workload": vars(args), "trials": trials,
+    workload = {k: v for k, v in vars(args).items() if k != "out"}
+    result = {"config": best, "events_per_s": rate, "workload": workload, "trials": trials,
               "device": torch.cuda.get_device_name(0), "seconds": round(time.time() - t0, 1)}
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:

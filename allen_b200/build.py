@@ -8,6 +8,7 @@ CPU build, which never fuses a multiply with an add.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -49,16 +50,19 @@ def build_chain(force: bool = False, verbose: bool = False) -> str:
     deps = cus + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
     if not force and not _stale(target, deps):
         return target
-    objs = []
-    for cu in cus:
-        obj = os.path.join(LIB_DIR, os.path.basename(cu) + ".o")
+    objs = [os.path.join(LIB_DIR, os.path.basename(cu) + ".o") for cu in cus]
+
+    def compile_one(cu, obj):
         cmd = [_nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", cu, "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {cu}:\n{r.stderr}")
-        if verbose:
-            sys.stderr.write(r.stderr)
-        objs.append(obj)
+        return cu, subprocess.run(cmd, capture_output=True, text=True)
+
+    # one nvcc per translation unit, in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cus), os.cpu_count() or 1)) as pool:
+        for cu, r in pool.map(lambda a: compile_one(*a), zip(cus, objs)):
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {cu}:\n{r.stderr}")
+            if verbose:
+                sys.stderr.write(r.stderr)
     cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", target, *objs,
            "-lcudart", "-lcuda"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -90,14 +94,6 @@ def build_io(force: bool = False) -> str:
     cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-pthread", "-Wall", "-I", INCLUDE, "-o", target, src]
     subprocess.run(cmd, check=True)
     return target
-
-
-def build_oracle(ref_root: str | None = "/root/reference") -> None:
-    """Test infrastructure: the plain-C oracle, and the reference CPU build when its tree exists."""
-    oracle = os.path.join(REPO, "oracle")
-    subprocess.run(["make", "-s", "-C", oracle, "oracle"], check=True)
-    if ref_root and os.path.isdir(ref_root):
-        subprocess.run(["make", "-s", "-j8", "-C", oracle, "ref", f"REF_ROOT={ref_root}"], check=True)
 
 
 def main():

@@ -89,7 +89,7 @@ class LaunchConfigC(C.Structure):
     _fields_ = [(f, C.c_uint) for f in (
         "search_threads", "search_lanes_per_seed", "search_hit_capacity", "cluster_stage_capacity",
         "cluster_blob_bytes", "estimate_blob_bytes", "persistent", "events_per_claim", "search_ring_global",
-        "cluster_threads")]
+        "cluster_threads", "retina_order_capacity", "kalman_warp_hits")]
 
 
 class TotalsC(C.Structure):

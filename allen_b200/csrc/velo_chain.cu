@@ -37,14 +37,6 @@ namespace {
 
 namespace velo_host {
   void set_last_error(const std::string& what) { last_error = what; }
-} // namespace velo_host
-
-namespace {
-#define VELO_CUDA(call)                                                                                 \
-  do {                                                                                                  \
-    const cudaError_t e_ = (call);                                                                      \
-    if (e_ != cudaSuccess) return fail(VELO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
 
   // ClusteringCommon.cpp:6-104 restated: 8-connected groups of the 2 x 4 super pixel,
   // seeded in ascending bit order (bit = col * 4 + row); per group the centroid
@@ -116,6 +108,14 @@ namespace {
     std::memcpy(g.ltg, p, velo::n_sensors * 12 * 4);
     return true;
   }
+} // namespace velo_host
+
+namespace {
+#define VELO_CUDA(call)                                                                                 \
+  do {                                                                                                  \
+    const cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) return fail(VELO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
 
   template<typename T>
   struct DeviceBuffer {
@@ -193,7 +193,7 @@ static const SearchVariant search_variants[] = {
 // for 3072 keys and allow six CTAs per SM instead of eight), the bucket order of up to 8192
 // clusters in shared memory (16 KiB).
 static constexpr unsigned retina_key_capacity = 0;
-static constexpr unsigned retina_order_capacity = 8192;
+static constexpr unsigned retina_order_capacity_max = 8192;
 static constexpr size_t n_sensors_total = velo::n_sensors;
 
 static SearchKernel learned_search_kernel(unsigned threads, unsigned ring_global = 0)
@@ -241,6 +241,9 @@ struct VeloChain {
   unsigned events_per_claim = 1;
   unsigned search_ring_global = 0; // rings of tracks to follow in global scratch (persistent only)
   unsigned cluster_threads = 256;  // block size of the clustering kernel (128 or 256)
+  unsigned retina_order_capacity = retina_order_capacity_max; // retina clusters ranked through key buckets
+  unsigned kalman_warp_hits = velo::kalman_warp_hits;         // Kalman: hits of a warp's tracks staged
+  unsigned resident_kalman = 0;                               // Kalman CTAs resident on the device
   unsigned resident_estimate = 0, resident_cluster = 0, resident_search = 0; // CTAs that fit the device
 
   // workspace
@@ -318,11 +321,14 @@ namespace {
     p.beamline_x = c->beamline[0];
     p.beamline_y = c->beamline[1];
     p.track_capacity = static_cast<unsigned>(c->cap_tracks);
+    p.warp_hits = c->kalman_warp_hits;
+    p.abort_flags = velo::err_input_capacity | velo::err_output_capacity;
     p.is_backward = c->is_backward.p;
     p.beamline_states = c->kalman_beamline_states.p;
     p.endvelo_states = c->kalman_endvelo_states.p;
     p.status = c->status.p;
-    const unsigned blocks = std::min<unsigned>(unsigned((c->cap_tracks + 255) / 256), 148u * velo::kalman_ctas_per_sm);
+    // one wave of the device (grid-stride loop over the tracks)
+    const unsigned blocks = std::min<unsigned>(unsigned((c->cap_tracks + 255) / 256), c->resident_kalman);
     velo::kalman_filter_kernel<<<std::max(blocks, 1u), velo::kalman_threads, 0, stream>>>(p);
     VELO_CUDA(cudaGetLastError());
     return VELO_OK;
@@ -373,7 +379,7 @@ namespace {
       rp.key_scratch = c->retina_keys.p;
       rp.status = c->status.p;
       rp.smem_key_capacity = retina_key_capacity;
-      rp.smem_order_capacity = retina_order_capacity;
+      rp.smem_order_capacity = c->retina_order_capacity;
       rp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
       VELO_CUDA(cudaMemsetAsync(c->retina_bank_index.p, 0, n_sensors * sizeof(unsigned), stream));
       VELO_CUDA(cudaMemsetAsync(c->candidates_offsets.p, 0, (n + 1) * sizeof(unsigned), stream));
@@ -386,7 +392,7 @@ namespace {
       VELO_CUDA(cudaGetLastError());
       VELO_CUDA(mark());
       retina_decode_kernel<<<n, decode_threads,
-                             retina_key_capacity * sizeof(long long) + retina_order_capacity * sizeof(uint16_t), stream>>>(rp);
+                             retina_key_capacity * sizeof(long long) + c->retina_order_capacity * sizeof(uint16_t), stream>>>(rp);
       VELO_CUDA(cudaGetLastError());
       VELO_CUDA(mark());
     }
@@ -552,6 +558,8 @@ namespace {
     VELO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
     VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, estimate_kernel, decode_threads, c->estimate_blob_bytes));
     c->resident_estimate = unsigned(std::max(per_sm, 1) * sms);
+    VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kalman_filter_kernel, kalman_threads, 0));
+    c->resident_kalman = unsigned(std::max(per_sm, 1) * sms);
     if (c->cluster_threads == 128)
       VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel<128>, 128, cluster_smem));
     else
@@ -612,9 +620,9 @@ VeloStatus velo_chain_create(
   const VeloStatus dev_ok = velo_device_check();
   if (dev_ok != VELO_OK) return dev_ok;
   velo::Geometry g {};
-  if (!parse_geometry(static_cast<const char*>(geometry), geometry_size, g))
+  if (!velo_host::parse_geometry(static_cast<const char*>(geometry), geometry_size, g))
     return fail(VELO_ERR_ARGUMENT, "malformed velo geometry blob");
-  build_sp_tables(g.sp_patterns, g.sp_fx, g.sp_fy);
+  velo_host::build_sp_tables(g.sp_patterns, g.sp_fx, g.sp_fy);
 
   VeloChainProperties pr;
   velo_default_properties(&pr);
@@ -790,6 +798,10 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
     return fail(VELO_ERR_ARGUMENT, "search_ring_global needs persistent launches (one ring per resident CTA)");
   if (cfg->cluster_threads != 128 && cfg->cluster_threads != 256)
     return fail(VELO_ERR_ARGUMENT, "cluster_threads must be 128 or 256");
+  if (cfg->retina_order_capacity > retina_order_capacity_max)
+    return fail(VELO_ERR_ARGUMENT, "retina_order_capacity above 8192");
+  if (cfg->kalman_warp_hits > velo::kalman_warp_hits)
+    return fail(VELO_ERR_ARGUMENT, "kalman_warp_hits above 368");
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   const unsigned search_static = 32 * 1024; // upper bound of the kernel's static shared memory
@@ -810,6 +822,8 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
   c->events_per_claim = cfg->events_per_claim;
   c->search_ring_global = cfg->search_ring_global;
   c->cluster_threads = cfg->cluster_threads;
+  c->retina_order_capacity = cfg->retina_order_capacity;
+  c->kalman_warp_hits = cfg->kalman_warp_hits;
   return configure_kernels(c);
 }
 
@@ -826,6 +840,8 @@ VeloStatus velo_chain_get_config(const VeloChain* c, VeloLaunchConfig* cfg)
   cfg->events_per_claim = c->events_per_claim;
   cfg->search_ring_global = c->search_ring_global;
   cfg->cluster_threads = c->cluster_threads;
+  cfg->retina_order_capacity = c->retina_order_capacity;
+  cfg->kalman_warp_hits = c->kalman_warp_hits;
   return VELO_OK;
 }
 
@@ -1034,11 +1050,17 @@ VeloStatus velo_kalman_filter(
   p.beamline_x = beamline_x;
   p.beamline_y = beamline_y;
   p.track_capacity = track_capacity;
+  p.warp_hits = velo::kalman_warp_hits;
   p.is_backward = dev_is_backward;
   p.beamline_states = reinterpret_cast<float*>(dev_velo_kalman_beamline_states);
   p.endvelo_states = reinterpret_cast<float*>(dev_velo_kalman_endvelo_states);
   p.status = dev_status;
-  const unsigned blocks = std::min<unsigned>((track_capacity + 255) / 256, 148u * velo::kalman_ctas_per_sm);
+  // one wave of the current device (grid-stride loop over the tracks)
+  int device = 0, sms = 0, per_sm = 0;
+  VELO_CUDA(cudaGetDevice(&device));
+  VELO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, velo::kalman_filter_kernel, velo::kalman_threads, 0));
+  const unsigned blocks = std::min<unsigned>((track_capacity + 255) / 256, unsigned(std::max(per_sm, 1) * sms));
   velo::kalman_filter_kernel<<<std::max(blocks, 1u), velo::kalman_threads, 0, static_cast<cudaStream_t>(stream)>>>(p);
   VELO_CUDA(cudaGetLastError());
   return VELO_OK;

@@ -119,6 +119,8 @@ namespace velo {
 
   __global__ void __launch_bounds__(kalman_threads, kalman_ctas_per_sm) kalman_filter_kernel(KalmanParams p)
   {
+    // in the chain: a stage before this one found the slice too large and wrote no tracks
+    if (p.abort_flags != 0 && p.status != nullptr && (*p.status & p.abort_flags)) return;
     const unsigned total_tracks = p.offsets_all_velo_tracks[p.n_events];
     if (total_tracks > p.track_capacity) {
       if (threadIdx.x == 0 && blockIdx.x == 0 && p.status != nullptr) set_error(p.status, err_output_capacity);
@@ -137,7 +139,7 @@ namespace velo {
       const unsigned end = min(base + 32u, total_tracks);
       const unsigned span_first = hn[base];
       const unsigned span_hits = hn[end] - span_first;
-      const bool in_slot = span_hits <= kalman_warp_hits;
+      const bool in_slot = span_hits <= min(p.warp_hits, kalman_warp_hits);
       if (in_slot) {
         const float* src = coords + 3 * size_t(span_first);
         for (unsigned j = lane; j < 3u * span_hits; j += 32u) slot[j] = src[j];

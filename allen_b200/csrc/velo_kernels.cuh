@@ -207,6 +207,8 @@ namespace velo {
     float beamline_x, beamline_y;                  // Constants::dev_beamline
     unsigned track_capacity;                       // entries of the outputs
     uint8_t* is_backward;                          // [tracks] dev_is_backward
+    unsigned warp_hits;                            // hits of a warp's tracks staged (<= kalman_warp_hits)
+    unsigned abort_flags;                          // status bits that mean the inputs were not written
     float* beamline_states;                        // [14 tracks] dev_velo_kalman_beamline_states
     float* endvelo_states;                         // [14 tracks] dev_velo_kalman_endvelo_states
     unsigned* status;
@@ -230,10 +232,18 @@ namespace velo {
 
   constexpr unsigned decode_threads = 256;
   constexpr unsigned kalman_threads = 256;
-  constexpr unsigned kalman_ctas_per_sm = 6; // 40 registers a thread; the grid is one wave of 148 SMs
+  constexpr unsigned kalman_ctas_per_sm = 6; // 40 registers a thread; the grid is one wave of the device
   constexpr unsigned kalman_warp_hits = 368; // hits of a warp's 32 tracks staged in shared memory (4.4 KB)
   constexpr unsigned scan_threads = 1024;
   constexpr unsigned consolidate_threads = 256;
   constexpr unsigned search_hit_bytes = 15; // x, y, z, phi, flags per staged hit
 
 } // namespace velo
+
+// Host helpers shared by the chain and the allocation-free entry point (velo_chain.cu).
+namespace velo_host {
+  // cache_sp_patterns (ClusteringCommon.cpp:6-104): SP pattern byte and centroid fractions
+  void build_sp_tables(uint8_t* patterns, float* fx, float* fy);
+  // velo_geometry.bin (integration/non_event_data/src/VPGeometry.cpp:21-63); false if malformed
+  bool parse_geometry(const char* blob, size_t size, velo::Geometry& g);
+} // namespace velo_host

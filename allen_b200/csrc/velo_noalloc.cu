@@ -24,7 +24,10 @@
 //     make that first call before any stream capture;
 //   * all calls share the array and it keeps the last call's contents; the parts that
 //     must start at zero are cleared on the stream at every call.  Calls that overlap on
-//     the GPU (different streams, no ordering between them) race on it.
+//     the GPU (different streams, no ordering between them) race on it;
+//   * the geometry is device-wide too: a call with another geometry blob uploads it on its
+//     own stream, which rewrites it under any overlapping call on another stream (the same
+//     race), and inside a stream capture that upload fails (pageable source).
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -74,77 +77,9 @@ static __device__ __align__(256) unsigned char velo_noalloc_scratch[scratch_byte
 static __device__ __align__(16) velo::Geometry velo_noalloc_geometry;
 
 namespace {
-  // SP lookup tables, as velo_chain_create builds them (ClusteringCommon.cpp:6-104).
-  void noalloc_sp_tables(uint8_t* patterns, float* fx, float* fy)
-  {
-    std::memset(patterns, 0, 256);
-    std::memset(fx, 0, 512 * sizeof(float));
-    std::memset(fy, 0, 512 * sizeof(float));
-    for (unsigned sp = 0; sp < 256; ++sp) {
-      unsigned left = sp, clu = 0;
-      for (unsigned seed = 0; seed < 8; ++seed) {
-        if (!(left & (1u << seed))) continue;
-        unsigned group = 1u << seed, before;
-        do {
-          before = group;
-          for (unsigned b = 0; b < 8; ++b) {
-            if (!(left & (1u << b)) || (group & (1u << b))) continue;
-            for (unsigned o = 0; o < 8; ++o) {
-              if (!(group & (1u << o))) continue;
-              const int dc = int(b / 4) - int(o / 4), dr = int(b % 4) - int(o % 4);
-              if (dc >= -1 && dc <= 1 && dr >= -1 && dr <= 1) {
-                group |= 1u << b;
-                break;
-              }
-            }
-          }
-        } while (group != before);
-        left &= ~group;
-        unsigned x = 0, y = 0, n = 0;
-        for (unsigned b = 0; b < 8; ++b)
-          if (group & (1u << b)) {
-            x += b / 4;
-            y += b % 4;
-            ++n;
-          }
-        const unsigned cx = x / n, cy = y / n;
-        fx[2 * sp + clu] = float(x) / float(n) - float(cx);
-        fy[2 * sp + clu] = float(y) / float(n) - float(cy);
-        patterns[sp] |= uint8_t(((cx << 2) | cy) << (4 * clu));
-        patterns[sp] |= uint8_t(clu << 3);
-        ++clu;
-      }
-    }
-  }
-
-  bool noalloc_parse_geometry(const char* p, size_t size, velo::Geometry& g)
-  {
-    const char* end = p + size;
-    auto read = [&](size_t n, float* dst) {
-      uint64_t count;
-      if (p + 8 > end) return false;
-      std::memcpy(&count, p, 8);
-      p += 8;
-      if (count != n || p + n * 4 > end) return false;
-      std::memcpy(dst, p, n * 4);
-      p += n * 4;
-      return true;
-    };
-    if (!read(velo::n_modules, g.module_zs) || !read(velo::n_cols, g.local_x) || !read(velo::n_cols, g.x_pitch))
-      return false;
-    uint64_t n_ltg, n_trans;
-    if (p + 16 > end) return false;
-    std::memcpy(&n_ltg, p, 8);
-    std::memcpy(&n_trans, p + 8, 8);
-    p += 16;
-    if (n_ltg != velo::n_sensors || n_trans != 12 || p + velo::n_sensors * 12 * 4 > end) return false;
-    std::memcpy(g.ltg, p, velo::n_sensors * 12 * 4);
-    return true;
-  }
-
   // Once per device, with that device current: the scratch address, the kernels'
   // shared-memory limits, and (when it changes) the geometry.
-  VeloStatus setup(int device, const void* geometry, size_t geometry_size, unsigned char** scratch)
+  VeloStatus setup(int device, const void* geometry, size_t geometry_size, cudaStream_t stream, unsigned char** scratch)
   {
     std::lock_guard<std::mutex> lock(setup_mutex);
     if (device < 0 || device >= int(max_devices)) return fail(VELO_ERR_ARGUMENT, "device index out of range");
@@ -160,14 +95,18 @@ namespace {
         return fail(VELO_ERR_CUDA, "cannot set the kernels' shared-memory limits");
       scratch_address[device] = static_cast<unsigned char*>(ptr);
     }
-    const std::string blob(static_cast<const char*>(geometry), geometry_size);
-    if (geometry_loaded[device] != blob) {
+    // the blob is compared in place with the one last uploaded to this device
+    std::string& loaded = geometry_loaded[device];
+    if (loaded.size() != geometry_size || std::memcmp(loaded.data(), geometry, geometry_size) != 0) {
       velo::Geometry g {};
-      if (!noalloc_parse_geometry(blob.data(), blob.size(), g)) return fail(VELO_ERR_ARGUMENT, "malformed velo geometry blob");
-      noalloc_sp_tables(g.sp_patterns, g.sp_fx, g.sp_fy);
-      const cudaError_t e = cudaMemcpyToSymbol(velo_noalloc_geometry, &g, sizeof(g));
+      if (!velo_host::parse_geometry(static_cast<const char*>(geometry), geometry_size, g))
+        return fail(VELO_ERR_ARGUMENT, "malformed velo geometry blob");
+      velo_host::build_sp_tables(g.sp_patterns, g.sp_fx, g.sp_fy);
+      // on the caller's stream, after the earlier calls queued there; the source is pageable,
+      // so the copy has read it when the call returns
+      const cudaError_t e = cudaMemcpyToSymbolAsync(velo_noalloc_geometry, &g, sizeof(g), 0, cudaMemcpyHostToDevice, stream);
       if (e != cudaSuccess) return fail(VELO_ERR_CUDA, std::string("geometry upload: ") + cudaGetErrorString(e));
-      geometry_loaded[device] = blob;
+      loaded.assign(static_cast<const char*>(geometry), geometry_size);
     }
     *scratch = scratch_address[device];
     return VELO_OK;
@@ -211,14 +150,14 @@ VeloStatus velo_decode_noalloc(
     return fail(VELO_ERR_CAPACITY, "output container smaller than 18 bytes x 2 x super pixels");
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return fail(VELO_ERR_NO_DEVICE, "no CUDA device");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   unsigned char* scratch = nullptr;
-  const VeloStatus st = setup(device, geometry, geometry_size, &scratch);
+  const VeloStatus st = setup(device, geometry, geometry_size, stream, &scratch);
   if (st != VELO_OK) return st;
   Geometry* geo = nullptr;
   if (cudaGetSymbolAddress(reinterpret_cast<void**>(&geo), velo_noalloc_geometry) != cudaSuccess)
     return fail(VELO_ERR_CUDA, "geometry address");
 
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   const unsigned n = s->n_events;
   RawInput in {s->raw, s->offsets, s->sizes, s->types, s->event_start, s->n_events, s->bank_version, s->mep_layout};
   auto* bank_index = reinterpret_cast<unsigned long long*>(scratch + off_bank_index);

@@ -191,7 +191,8 @@ namespace velo {
   }
 
   // Capped for eight CTAs per SM (32 registers): with the keys in L2-resident scratch the
-  // shared memory (bucket order and counters, 13 KB) allows that many.
+  // shared memory (16 KB of bucket order plus about 4.5 KB of counters and offsets, 21 KB)
+  // allows that many.
   __global__ void __launch_bounds__(decode_threads, 8) retina_decode_kernel(RetinaParams p)
   {
     extern __shared__ __align__(16) unsigned char dsmem[];

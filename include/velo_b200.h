@@ -205,6 +205,11 @@ typedef struct {
                                       persistent launches only */
   unsigned cluster_threads;        /* block size of the clustering kernel: 256, or 128 (twice the
                                       resident CTAs per SM where shared memory allows) */
+  unsigned retina_order_capacity;  /* retina front end: clusters of an event ranked through key buckets
+                                      in shared memory (2 B each, at most 8192, default 8192); larger
+                                      events are ranked by comparing every pair of keys */
+  unsigned kalman_warp_hits;       /* Kalman filter: hits of a warp's 32 tracks staged in shared memory
+                                      (at most 368, default 368); longer spans are read in place */
 } VeloLaunchConfig;
 VeloStatus velo_chain_configure(VeloChain* chain, const VeloLaunchConfig* config);
 VeloStatus velo_chain_get_config(const VeloChain* chain, VeloLaunchConfig* config);
@@ -232,9 +237,12 @@ void velo_chain_destroy(VeloChain* chain);
  * device array of velo_noalloc_scratch_bytes() (8 MiB at most) that every GPU loading the
  * library holds until exit; slices above velo_noalloc_max_events() events or
  * 2 x super_pixels > velo_noalloc_max_clusters() are rejected with VELO_ERR_CAPACITY.
- * The first call on a device makes synchronous set-up calls (scratch address, geometry
- * upload, kernel attributes): make it before any stream capture.  All calls share the
- * scratch, which keeps the last call's contents; calls that overlap on the GPU race.
+ * The first call on a device makes synchronous set-up calls (scratch address, kernel
+ * attributes) and uploads the geometry on `stream`: make it before any stream capture.  All
+ * calls share the scratch, which keeps the last call's contents; calls that overlap on the
+ * GPU race.  The geometry is shared the same way: a call with a different blob uploads it
+ * again on its own stream (not allowed inside a capture), rewriting it under any
+ * overlapping call.
  * dev_status (optional, device u32) receives the kernels' error flags. */
 VeloStatus velo_decode_noalloc(
   const void* geometry,

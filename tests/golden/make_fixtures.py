@@ -140,4 +140,9 @@ def main(ref_root, only=()):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", tuple(sys.argv[2:]))
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import build_checkers as oracle_build  # noqa: E402
+    root = sys.argv[1] if len(sys.argv) > 1 else oracle_build.reference_root()
+    if root is None:
+        sys.exit("the reference tree was not found: pass its path or set ALLEN_REFERENCE_ROOT")
+    main(root, tuple(sys.argv[2:]))

@@ -5,6 +5,7 @@ import ctypes as C
 import os
 import re
 import struct
+import sys
 
 import numpy as np
 import pytest
@@ -14,7 +15,12 @@ import mdf_streams
 from allen_b200 import _native, generator, mdf, rawbanks
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_MDF = "/root/reference/input/minbias/mdf/MiniBrunel_2018_MinBias_FTv4_DIGI_retinacluster_v1.mdf"
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+import build_checkers  # noqa: E402
+
+_REF_ROOT = build_checkers.reference_root()
+REF_MDF = os.path.join(_REF_ROOT or "", "input", "minbias", "mdf",
+                       "MiniBrunel_2018_MinBias_FTv4_DIGI_retinacluster_v1.mdf")
 FIXTURE = os.path.join(REPO, "tests", "golden", "mdf_synthetic_8ev.npz")
 
 needs_ref = pytest.mark.skipif(not cpu_checkers.available("ref"), reason="reference CPU build absent")

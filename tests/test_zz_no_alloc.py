@@ -29,6 +29,12 @@ def _noalloc_lib():
     return lib
 
 
+# Calls in a row: two of the same size, then a smaller slice of v4 banks after a larger one
+# (the scratch still holds the larger call's contents), then a v3 slice.
+CALLS = [(40, 21, {}), (40, 22, {}), (44, 23, dict(pileup_min=1.0, pileup_max=15.0)),
+         (25, 24, dict(bank_version=4)), (30, 25, dict(bank_version=3))]
+
+
 def test_decode_noalloc_matches_chain_on_two_calls(geometry):
     import torch
     if not torch.cuda.is_available():
@@ -38,11 +44,11 @@ def test_decode_noalloc_matches_chain_on_two_calls(geometry):
     from allen_b200.rawbanks import super_pixels_per_event
 
     lib = _noalloc_lib()
-    assert lib.velo_noalloc_max_events() >= 40
+    assert lib.velo_noalloc_max_events() >= max(n for n, _, _ in CALLS)
     chain = VeloChain(geometry)
     try:
-        for seed in (21, 22):
-            g = generator.generate(40, seed=seed)
+        for n_events, seed, cfg in CALLS:
+            g = generator.generate(n_events, seed=seed, **cfg)
             n = g.raw.n_events
             sp = int(super_pixels_per_event(g.raw).sum())
             assert 2 * sp <= lib.velo_noalloc_max_clusters()
@@ -92,3 +98,32 @@ def test_decode_noalloc_rejects_oversized_slices(geometry):
     st = lib.velo_decode_noalloc(geometry, len(geometry), C.byref(d.c_struct()), too_many, _current_stream(),
                                  dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr(), 64, None)
     assert st == 3  # VELO_ERR_CAPACITY, nothing queued
+
+
+def test_decode_noalloc_understated_super_pixels(geometry):
+    """A caller that states fewer super pixels than its banks hold: the estimate needs more
+    clusters than 2 x the stated count, so the clustering writes nothing and dev_status
+    receives err_input_capacity (bit 6); the call itself is accepted."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from allen_b200 import generator
+    from allen_b200.chain import upload, _current_stream
+    from allen_b200.rawbanks import super_pixels_per_event
+
+    lib = _noalloc_lib()
+    g = generator.generate(20, seed=26)
+    n = g.raw.n_events
+    sp = int(super_pixels_per_event(g.raw).sum())
+    stated = sp // 4
+    d = upload(g.raw)
+    off = torch.full((26 * n + 1,), -1, dtype=torch.int32, device="cuda")
+    num = torch.full((26 * n,), -1, dtype=torch.int32, device="cuda")
+    cont = torch.full((18 * 2 * stated,), 0xAB, dtype=torch.uint8, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = lib.velo_decode_noalloc(geometry, len(geometry), C.byref(d.c_struct()), stated, _current_stream(),
+                                 off.data_ptr(), num.data_ptr(), cont.data_ptr(), cont.numel(), status.data_ptr())
+    assert st == 0, lib.velo_noalloc_last_error_string().decode()
+    torch.cuda.synchronize()
+    assert int(status.item()) & (1 << 6)
+    assert bool((off == -1).all()) and bool((num == -1).all()) and bool((cont == 0xAB).all())
