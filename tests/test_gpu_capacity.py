@@ -78,9 +78,10 @@ def test_workspace_too_small(chain, oracle, geometry):
     pixels than reserved: the stages find the slice too large, write nothing, and the run
     ends in VELO_ERR_DEVICE_FLAGS with err_input_capacity; the chain then runs a slice that
     fits as before."""
-    small = generator.generate(20, seed=61).raw
-    big = generator.generate(20, seed=62, mean_pileup=15.0).raw
-    assert super_pixels_per_event(big).sum() > 1.5 * super_pixels_per_event(small).sum()
+    small = generator.generate(20, seed=61, mean_pileup=2.0).raw
+    big = generator.generate(20, seed=62, mean_pileup=15.0, noise_rate=1e-4).raw
+    # the reservation holds 2 estimated clusters per reserved super pixel: exceed that
+    assert super_pixels_per_event(big).sum() > 3 * super_pixels_per_event(small).sum()
     chain.reserve_for(small)
     chain.set_kalman(True, (0.0, 0.0))
     try:
