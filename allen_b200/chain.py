@@ -100,6 +100,26 @@ class TotalsC(C.Structure):
         "track_container_size", "device_flags")]
 
 
+class SizesC(C.Structure):
+    _fields_ = [(f, C.c_ulonglong) for f in (
+        "offsets_estimated_input_size", "module_cluster_num", "sorted_velo_cluster_container_bytes",
+        "offsets_all_velo_tracks", "velo_track_hit_number", "offsets_velo_track_hit_number",
+        "velo_track_hits_bytes", "accepted_velo_tracks", "max_reconstructed_tracks", "workspace_bytes")]
+
+
+class OutputBuffersC(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in (
+        "dev_offsets_estimated_input_size", "dev_module_cluster_num", "dev_sorted_velo_cluster_container",
+        "dev_offsets_all_velo_tracks", "dev_velo_track_hit_number", "dev_offsets_velo_track_hit_number",
+        "dev_velo_track_hits", "dev_accepted_velo_tracks")]
+
+
+COORDINATES_FP32, COORDINATES_FP16 = 0, 1
+# view sizes (Allen::Views::Velo::Consolidated::{Hits, Track, Tracks, MultiEventTracks})
+VIEW_BYTES = {"dev_velo_hits_view": 24, "dev_velo_track_view": 24, "dev_velo_tracks_view": 16,
+              "dev_velo_multi_event_tracks_view": 24, "dev_imec_velo_tracks": 8}
+
+
 def _lib():
     lib = _native.load_chain()
     if getattr(lib, "_typed", False):
@@ -122,6 +142,14 @@ def _lib():
     lib.velo_chain_outputs.restype = C.c_int
     lib.velo_chain_outputs.argtypes = [C.c_void_p, C.POINTER(OutputsC)]
     lib.velo_chain_destroy.argtypes = [C.c_void_p]
+    lib.velo_chain_sizes.restype = C.c_int
+    lib.velo_chain_sizes.argtypes = [C.c_void_p, C.c_uint, C.c_ulonglong, C.c_int, C.POINTER(SizesC)]
+    lib.velo_chain_bind.restype = C.c_int
+    lib.velo_chain_bind.argtypes = [C.c_void_p, C.c_void_p, C.c_ulonglong, C.c_uint, C.c_ulonglong, C.c_int,
+                                    C.POINTER(OutputBuffersC)]
+    lib.velo_create_velo_views.restype = C.c_int
+    lib.velo_create_velo_views.argtypes = [C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.velo_copy_to_host.restype = C.c_int
     lib.velo_copy_to_host.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.velo_copy_to_host_async.restype = C.c_int
@@ -143,8 +171,8 @@ def _lib():
     lib.velo_chain_set_front_end.argtypes = [C.c_void_p, C.c_int]
     lib.velo_chain_set_kalman.restype = C.c_int
     lib.velo_chain_set_kalman.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float]
-    lib.velo_kalman_filter.restype = C.c_int
-    lib.velo_kalman_filter.argtypes = [C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint, C.c_float, C.c_float,
+    lib.velo_run_kalman_filter.restype = C.c_int
+    lib.velo_run_kalman_filter.argtypes = [C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint, C.c_float, C.c_float,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.velo_chain_set_seed_model.restype = C.c_int
     lib.velo_chain_set_seed_model.argtypes = [C.c_void_p, C.POINTER(SeedModelC)]
@@ -239,6 +267,21 @@ class VeloChain:
 
     def reserve(self, max_events: int, max_super_pixels: int, max_raw_bytes: int = 0):
         _check(self.lib, self.lib.velo_chain_reserve(self.handle, max_events, max_super_pixels, max_raw_bytes))
+        self.max_events, self.max_super_pixels = max_events, max_super_pixels
+
+    def sizes(self, max_events: int, max_super_pixels: int, layout: int = COORDINATES_FP32) -> dict:
+        """Element counts of the outputs and the scratch bytes for caller-owned memory."""
+        out = SizesC()
+        _check(self.lib, self.lib.velo_chain_sizes(self.handle, max_events, max_super_pixels, layout, C.byref(out)))
+        return {f: getattr(out, f) for f, _ in SizesC._fields_}
+
+    def bind(self, workspace_ptr: int, workspace_bytes: int, max_events: int, max_super_pixels: int,
+             outputs: dict, layout: int = COORDINATES_FP32):
+        """Runs into caller memory from now on: ``outputs`` maps each OutputBuffersC field to a
+        device pointer (sized by sizes()); the chain allocates nothing more."""
+        o = OutputBuffersC(*[outputs[f] for f, _ in OutputBuffersC._fields_])
+        _check(self.lib, self.lib.velo_chain_bind(self.handle, workspace_ptr, workspace_bytes, max_events,
+                                                  max_super_pixels, layout, C.byref(o)))
         self.max_events, self.max_super_pixels = max_events, max_super_pixels
 
     def reserve_for(self, s: RawSlice, margin: float = 1.0):

@@ -117,26 +117,48 @@ namespace {
     if (e_ != cudaSuccess) return fail(VELO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+  // A device buffer the chain allocated (owned) or a piece of memory it was given (bound).
   template<typename T>
   struct DeviceBuffer {
+    using value_type = T;
     T* p = nullptr;
     size_t n = 0;
+    bool owned = false;
     cudaError_t reserve(size_t count)
     {
-      if (count <= n && p) return cudaSuccess;
-      if (p) cudaFree(p);
-      p = nullptr;
-      n = 0;
+      if (count <= n && p && owned) return cudaSuccess;
+      release();
       const cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
-      if (e == cudaSuccess) n = count;
+      if (e == cudaSuccess) {
+        n = count;
+        owned = true;
+      }
+      else {
+        p = nullptr;
+      }
       return e;
+    }
+    void bind(void* ptr, size_t count)
+    {
+      release();
+      p = static_cast<T*>(ptr);
+      n = count;
     }
     void release()
     {
-      if (p) cudaFree(p);
+      if (p && owned) cudaFree(p);
       p = nullptr;
       n = 0;
+      owned = false;
     }
+  };
+
+  constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+  // Bounds of a slice that a workspace is laid out for: events, estimated clusters T (two per
+  // super pixel at most, EstimateInputSize.cu:66,176-203), track container entries, track hits.
+  struct SliceBounds {
+    size_t n = 0, T = 0, tracks = 0, track_hits = 0, super_pixels = 0;
   };
 
   struct DeviceTotals {
@@ -244,6 +266,7 @@ struct VeloChain {
   unsigned retina_order_capacity = retina_order_capacity_max; // retina clusters ranked through key buckets
   unsigned kalman_warp_hits = velo::kalman_warp_hits;         // Kalman: hits of a warp's tracks staged
   unsigned resident_kalman = 0;                               // Kalman CTAs resident on the device
+  unsigned resident_export = 0;                               // half-layout export CTAs
   unsigned resident_estimate = 0, resident_cluster = 0, resident_search = 0; // CTAs that fit the device
 
   // workspace
@@ -281,6 +304,20 @@ struct VeloChain {
   unsigned* record_count = nullptr;
   unsigned record_capacity = 0, record_every = 1;
 
+  // per-slice workspace: an arena the chain allocated (velo_chain_reserve), or caller memory
+  // (velo_chain_bind); the key of the last binding decides whether cached graphs still hold
+  DeviceBuffer<char> arena;
+  struct BindKey {
+    const void* workspace = nullptr;
+    SliceBounds bounds;
+    long long layout = 0;
+    VeloChainOutputBuffers outputs {};
+  } bind_key;
+  bool bound_external = false;
+  // half-precision layout: the caller's coordinate containers, written from the FP32 ones
+  char* half_sorted_out = nullptr;
+  char* half_track_hits_out = nullptr;
+
   // host-buffer path
   DeviceBuffer<char> in_raw;
   DeviceBuffer<unsigned> in_offsets, in_sizes, in_types;
@@ -309,6 +346,120 @@ struct VeloChain {
     direct_timed = false;
   }
 };
+
+namespace {
+  bool slice_bounds(unsigned max_events, unsigned long long max_super_pixels, SliceBounds& b)
+  {
+    b.n = max_events;
+    b.super_pixels = size_t(max_super_pixels);
+    b.T = 2 * size_t(max_super_pixels) + 64;
+    if (max_events == 0 || b.T > 0xFFFFFFFFull / velo::element_size) return false;
+    b.tracks = std::max<size_t>(size_t(double(b.T) * 0.34) + 64, b.n * velo::minimum_container_size + 64);
+    b.track_hits = b.T;
+    return true;
+  }
+
+  // Every buffer whose size follows from the slice bounds, in workspace order:
+  // f(buffer, element count, kind).  Outputs are the buffers a caller that binds its own memory
+  // supplies separately (the reference's DEVICE_OUTPUTs that later algorithms read); the two
+  // coordinate containers are outputs too, unless the caller takes them in the half-precision
+  // layout, which the chain exports from its FP32 containers (those then stay in the workspace).
+  enum BufferKind { scratch_buffer, output_buffer, coordinate_buffer };
+
+  template<typename F>
+  void for_each_slice_buffer(VeloChain* c, const SliceBounds& b, F&& f)
+  {
+    const size_t n = b.n, T = b.T, tracks = b.tracks;
+    f(c->number_of_candidates, n, scratch_buffer);
+    f(c->candidates_offsets, n + 1, scratch_buffer);
+    f(c->estimated, 26 * n, scratch_buffer);
+    f(c->candidate_num, n, scratch_buffer);
+    f(c->event_estimate, n, scratch_buffer);
+    f(c->event_base, n + 1, scratch_buffer);
+    f(c->atomics, 3 * n, scratch_buffer);
+    f(c->n_tracks, n, scratch_buffer);
+    f(c->offsets_tracks, n + 1, scratch_buffer);
+    f(c->n_three_out, n, scratch_buffer);
+    f(c->offsets_three, n + 1, scratch_buffer);
+    f(c->event_track_hits, n, scratch_buffer);
+    f(c->event_track_hit_base, n + 1, scratch_buffer);
+    f(c->staging, 24 * T, scratch_buffer);
+    f(c->hit_scratch, 16 * T, scratch_buffer);
+    f(c->sp_scratch, b.super_pixels + 64, scratch_buffer);
+    f(c->tracks, tracks, scratch_buffer);
+    f(c->three_hit, tracks, scratch_buffer);
+    f(c->three_out, tracks, scratch_buffer);
+    f(c->hit_used, T, scratch_buffer);
+    f(c->seed_stats, 3 * n, scratch_buffer);
+    f(c->queue_next, 3, scratch_buffer);
+    f(c->is_backward, tracks, scratch_buffer);
+    f(c->retina_sizes, n * n_sensors_total, scratch_buffer);
+    f(c->retina_offsets, n * n_sensors_total + 1, scratch_buffer);
+    f(c->retina_bank_index, n_sensors_total, scratch_buffer);
+    f(c->retina_keys, T, scratch_buffer);
+    f(c->kalman_beamline_states, 14 * tracks, scratch_buffer);
+    f(c->kalman_endvelo_states, 14 * tracks, scratch_buffer);
+    f(c->event_order, n, scratch_buffer);
+    // outputs
+    f(c->offsets_est, 26 * n + 1, output_buffer);
+    f(c->cluster_num, 26 * n, output_buffer);
+    f(c->sorted, velo::element_size * T, coordinate_buffer);
+    f(c->offsets_all, n + 1, output_buffer);
+    f(c->track_hit_number, tracks, output_buffer);
+    f(c->offsets_hit_number, tracks + 1, output_buffer);
+    f(c->track_hits, velo::element_size * b.track_hits, coordinate_buffer);
+    f(c->accepted, 2 * tracks, output_buffer);
+  }
+
+  // Which buffers a workspace holds: all of them (the chain's own arena), or all but the
+  // caller's outputs (FP32 layout), or all but the outputs other than the coordinate containers
+  // (half layout).
+  enum WorkspaceScope { whole_chain, without_outputs, without_outputs_but_coordinates };
+
+  bool in_workspace(BufferKind k, WorkspaceScope w)
+  {
+    return k == scratch_buffer || w == whole_chain || (k == coordinate_buffer && w == without_outputs_but_coordinates);
+  }
+
+  size_t workspace_bytes(VeloChain* c, const SliceBounds& b, WorkspaceScope w)
+  {
+    size_t bytes = 0;
+    for_each_slice_buffer(c, b, [&](auto& buf, size_t count, BufferKind k) {
+      if (in_workspace(k, w)) bytes += align256(count * sizeof(typename std::decay_t<decltype(buf)>::value_type));
+    });
+    return bytes;
+  }
+
+  // Carves the buffers out of `base` (256-byte aligned pieces); the chain's capacities follow.
+  void bind_workspace(VeloChain* c, char* base, const SliceBounds& b, WorkspaceScope w)
+  {
+    size_t at = 0;
+    for_each_slice_buffer(c, b, [&](auto& buf, size_t count, BufferKind k) {
+      if (!in_workspace(k, w)) return;
+      buf.bind(base + at, count);
+      at += align256(count * sizeof(typename std::decay_t<decltype(buf)>::value_type));
+    });
+    c->cap_events = unsigned(b.n);
+    c->cap_clusters = b.T;
+    c->cap_tracks = b.tracks;
+    c->cap_track_hits = b.track_hits;
+  }
+
+  // The element counts of the output buffers of a slice bound (set_arguments_size).
+  void output_sizes(const SliceBounds& b, int layout, VeloChainSizes* s)
+  {
+    const size_t element = layout == VELO_COORDINATES_FP16 ? velo::element_size_half : velo::element_size;
+    s->offsets_estimated_input_size = 26 * b.n + 1;
+    s->module_cluster_num = 26 * b.n;
+    s->sorted_velo_cluster_container_bytes = element * b.T;
+    s->offsets_all_velo_tracks = b.n + 1;
+    s->velo_track_hit_number = b.tracks;
+    s->offsets_velo_track_hit_number = b.tracks + 1;
+    s->velo_track_hits_bytes = element * b.track_hits;
+    s->accepted_velo_tracks = 2 * b.tracks;
+    s->max_reconstructed_tracks = b.tracks;
+  }
+} // namespace
 
 namespace {
   VeloStatus launch_kalman(VeloChain* c, unsigned n, cudaStream_t stream)
@@ -518,6 +669,24 @@ namespace {
     VELO_CUDA(cudaGetLastError());
     VELO_CUDA(mark());
 
+    if (c->half_sorted_out) {
+      // the caller's containers in the half-precision layout of Allen's CUDA build
+      HalfExportParams hp {};
+      hp.n_events = n;
+      hp.offsets_estimated_input_size = c->offsets_est.p;
+      hp.sorted_container = c->sorted.p;
+      hp.offsets_all_velo_tracks = c->offsets_all.p;
+      hp.offsets_velo_track_hit_number = c->offsets_hit_number.p;
+      hp.velo_track_hits = c->track_hits.p;
+      hp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
+      hp.track_capacity = static_cast<unsigned>(c->cap_tracks);
+      hp.track_hit_capacity = static_cast<unsigned>(c->cap_track_hits);
+      hp.sorted_half = c->half_sorted_out;
+      hp.track_hits_half = c->half_track_hits_out;
+      hp.status = c->status.p;
+      export_half_kernel<<<c->resident_export, 256, 0, stream>>>(hp);
+      VELO_CUDA(cudaGetLastError());
+    }
     if (c->kalman) {
       const VeloStatus st = launch_kalman(c, n, stream);
       if (st != VELO_OK) return st;
@@ -560,6 +729,8 @@ namespace {
     c->resident_estimate = unsigned(std::max(per_sm, 1) * sms);
     VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kalman_filter_kernel, kalman_threads, 0));
     c->resident_kalman = unsigned(std::max(per_sm, 1) * sms);
+    VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, export_half_kernel, 256, 0));
+    c->resident_export = unsigned(std::max(per_sm, 1) * sms);
     if (c->cluster_threads == 128)
       VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel<128>, 128, cluster_smem));
     else
@@ -668,61 +839,94 @@ VeloStatus velo_chain_reserve(
   VeloChain* c, unsigned max_events, unsigned long long max_super_pixels, unsigned long long max_raw_bytes)
 {
   if (!c || max_events == 0) return fail(VELO_ERR_ARGUMENT, "bad reserve arguments");
+  SliceBounds b;
+  if (!slice_bounds(max_events, max_super_pixels, b)) return fail(VELO_ERR_CAPACITY, "slice too large for 32-bit offsets");
   c->release_graph();
-  const size_t n = max_events;
-  // every super pixel yields at most two estimated clusters (EstimateInputSize.cu:66,176-203)
-  const size_t T = 2 * size_t(max_super_pixels) + 64;
-  if (T > 0xFFFFFFFFull / velo::element_size) return fail(VELO_ERR_CAPACITY, "slice too large for 32-bit offsets");
-  const size_t tracks = std::max<size_t>(size_t(double(T) * 0.34) + 64, n * velo::minimum_container_size + 64);
-  const size_t track_hits = T;
-  c->cap_events = max_events;
-  c->cap_clusters = T;
-  c->cap_tracks = tracks;
-  c->cap_track_hits = track_hits;
-#define RES(buf, count)                                                        \
-  if ((buf).reserve(count) != cudaSuccess) return fail(VELO_ERR_CUDA, "workspace allocation failed: " #buf);
-  RES(c->number_of_candidates, n)
-  RES(c->candidates_offsets, n + 1)
-  RES(c->estimated, 26 * n)
-  RES(c->candidate_num, n)
-  RES(c->event_estimate, n)
-  RES(c->event_base, n + 1)
-  RES(c->offsets_est, 26 * n + 1)
-  RES(c->cluster_num, 26 * n)
-  RES(c->atomics, 3 * n)
-  RES(c->n_tracks, n)
-  RES(c->offsets_tracks, n + 1)
-  RES(c->n_three_out, n)
-  RES(c->offsets_three, n + 1)
-  RES(c->event_track_hits, n)
-  RES(c->event_track_hit_base, n + 1)
-  RES(c->offsets_all, n + 1)
-  RES(c->track_hit_number, tracks)
-  RES(c->offsets_hit_number, tracks + 1)
-  RES(c->sorted, velo::element_size * T)
-  RES(c->staging, 24 * T)
-  RES(c->hit_scratch, 16 * T)
-  RES(c->sp_scratch, size_t(max_super_pixels) + 64)
-  RES(c->track_hits, velo::element_size * track_hits)
-  RES(c->tracks, tracks)
-  RES(c->three_hit, tracks)
-  RES(c->three_out, tracks)
-  RES(c->hit_used, T)
-  RES(c->accepted, 2 * tracks)
-  RES(c->seed_stats, 3 * n)
-  RES(c->queue_next, 3)
-  RES(c->is_backward, tracks)
-  RES(c->retina_sizes, n * n_sensors_total)
-  RES(c->retina_offsets, n * n_sensors_total + 1)
-  RES(c->retina_bank_index, n_sensors_total)
-  RES(c->retina_keys, T)
-  RES(c->kalman_beamline_states, 14 * tracks)
-  RES(c->kalman_endvelo_states, 14 * tracks)
-  RES(c->event_order, n)
-  if (max_raw_bytes) {
-    RES(c->in_raw, max_raw_bytes + 16)
+  // one owned arena for every per-slice buffer, outputs included; it only grows
+  const size_t bytes = workspace_bytes(c, b, whole_chain);
+  if (!c->arena.owned || c->arena.n < bytes) {
+    c->arena.release();
+    if (c->arena.reserve(bytes) != cudaSuccess) return fail(VELO_ERR_CUDA, "workspace allocation failed");
   }
-#undef RES
+  bind_workspace(c, c->arena.p, b, whole_chain);
+  c->bound_external = false;
+  c->half_sorted_out = c->half_track_hits_out = nullptr;
+  c->bind_key = VeloChain::BindKey {};
+  if (max_raw_bytes && c->in_raw.reserve(max_raw_bytes + 16) != cudaSuccess)
+    return fail(VELO_ERR_CUDA, "workspace allocation failed: input staging");
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_sizes(
+  const VeloChain* c, unsigned max_events, unsigned long long max_super_pixels, int layout, VeloChainSizes* sizes)
+{
+  if (!sizes || max_events == 0) return fail(VELO_ERR_ARGUMENT, "bad size arguments");
+  if (layout != VELO_COORDINATES_FP32 && layout != VELO_COORDINATES_FP16) return fail(VELO_ERR_ARGUMENT, "unknown layout");
+  SliceBounds b;
+  if (!slice_bounds(max_events, max_super_pixels, b)) return fail(VELO_ERR_CAPACITY, "slice too large for 32-bit offsets");
+  output_sizes(b, layout, sizes);
+  VeloChain buffers; // the sizes depend on the bounds only, not on a chain's state
+  sizes->workspace_bytes =
+    workspace_bytes(&buffers, b, layout == VELO_COORDINATES_FP16 ? without_outputs_but_coordinates : without_outputs);
+  return VELO_OK;
+}
+
+VeloStatus velo_chain_bind(
+  VeloChain* c,
+  void* workspace,
+  unsigned long long workspace_size,
+  unsigned max_events,
+  unsigned long long max_super_pixels,
+  int layout,
+  const VeloChainOutputBuffers* o)
+{
+  if (!c || !workspace || !o || max_events == 0) return fail(VELO_ERR_ARGUMENT, "null argument");
+  if (layout != VELO_COORDINATES_FP32 && layout != VELO_COORDINATES_FP16) return fail(VELO_ERR_ARGUMENT, "unknown layout");
+  if (!o->dev_offsets_estimated_input_size || !o->dev_module_cluster_num || !o->dev_sorted_velo_cluster_container ||
+      !o->dev_offsets_all_velo_tracks || !o->dev_velo_track_hit_number || !o->dev_offsets_velo_track_hit_number ||
+      !o->dev_velo_track_hits || !o->dev_accepted_velo_tracks)
+    return fail(VELO_ERR_ARGUMENT, "every output buffer is required");
+  if (reinterpret_cast<uintptr_t>(workspace) & 255) return fail(VELO_ERR_ARGUMENT, "workspace must be 256-byte aligned");
+  const uintptr_t any = reinterpret_cast<uintptr_t>(o->dev_offsets_estimated_input_size) |
+                        reinterpret_cast<uintptr_t>(o->dev_module_cluster_num) |
+                        reinterpret_cast<uintptr_t>(o->dev_sorted_velo_cluster_container) |
+                        reinterpret_cast<uintptr_t>(o->dev_offsets_all_velo_tracks) |
+                        reinterpret_cast<uintptr_t>(o->dev_velo_track_hit_number) |
+                        reinterpret_cast<uintptr_t>(o->dev_offsets_velo_track_hit_number) |
+                        reinterpret_cast<uintptr_t>(o->dev_velo_track_hits);
+  if (any & 15) return fail(VELO_ERR_ARGUMENT, "output buffers must be 16-byte aligned");
+  SliceBounds b;
+  if (!slice_bounds(max_events, max_super_pixels, b)) return fail(VELO_ERR_CAPACITY, "slice too large for 32-bit offsets");
+  const bool half = layout == VELO_COORDINATES_FP16;
+  const WorkspaceScope scope = half ? without_outputs_but_coordinates : without_outputs;
+  if (workspace_size < workspace_bytes(c, b, scope)) return fail(VELO_ERR_CAPACITY, "workspace smaller than velo_chain_sizes()");
+  VeloChain::BindKey key {};
+  key.workspace = workspace;
+  key.bounds = b;
+  key.layout = layout;
+  key.outputs = *o;
+  const bool same = c->bound_external && std::memcmp(&key, &c->bind_key, sizeof(key)) == 0;
+  if (same) return VELO_OK;
+  c->release_graph();
+  c->arena.release();
+  bind_workspace(c, static_cast<char*>(workspace), b, scope);
+  c->offsets_est.bind(o->dev_offsets_estimated_input_size, 26 * b.n + 1);
+  c->cluster_num.bind(o->dev_module_cluster_num, 26 * b.n);
+  c->offsets_all.bind(o->dev_offsets_all_velo_tracks, b.n + 1);
+  c->track_hit_number.bind(o->dev_velo_track_hit_number, b.tracks);
+  c->offsets_hit_number.bind(o->dev_offsets_velo_track_hit_number, b.tracks + 1);
+  c->accepted.bind(o->dev_accepted_velo_tracks, 2 * b.tracks);
+  if (half) {
+    c->half_sorted_out = o->dev_sorted_velo_cluster_container;
+    c->half_track_hits_out = o->dev_velo_track_hits;
+  }
+  else {
+    c->sorted.bind(o->dev_sorted_velo_cluster_container, velo::element_size * b.T);
+    c->track_hits.bind(o->dev_velo_track_hits, velo::element_size * b.track_hits);
+    c->half_sorted_out = c->half_track_hits_out = nullptr;
+  }
+  c->bind_key = key;
+  c->bound_external = true;
   return VELO_OK;
 }
 
@@ -1022,7 +1226,7 @@ VeloStatus velo_chain_set_kalman(VeloChain* c, int enable, float beamline_x, flo
   return VELO_OK;
 }
 
-VeloStatus velo_kalman_filter(
+VeloStatus velo_run_kalman_filter(
   unsigned n_events,
   const unsigned* dev_offsets_all_velo_tracks,
   const unsigned* dev_offsets_velo_track_hit_number,
@@ -1107,6 +1311,7 @@ void velo_chain_destroy(VeloChain* c)
   c->release_graph();
   for (auto& e : c->direct_ev)
     if (e) cudaEventDestroy(e);
+  c->arena.release();
   c->geo.release();
   c->bank_index_key.release();
   c->status.release();

@@ -26,6 +26,7 @@ namespace velo {
   constexpr unsigned max_tracks_to_follow = 2048;
   constexpr unsigned minimum_container_size = 10;
   constexpr unsigned element_size = 18;
+  constexpr unsigned element_size_half = 12; // the same container with half-precision x, y, z (CUDA builds)
   constexpr unsigned bank_type_velo = 8;
   constexpr unsigned bank_type_vp = 63;
   constexpr unsigned bank_type_vp_retina = 73; // LHCb::RawBank::VPRetinaCluster

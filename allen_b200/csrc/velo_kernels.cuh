@@ -215,6 +215,23 @@ namespace velo {
   };
   __global__ void kalman_filter_kernel(KalmanParams p);
 
+  // The sorted cluster container and the consolidated track hits re-encoded with half-precision
+  // coordinates (12 bytes per element: u32 id[T], half xyz[3T], i16 phi[T]), the layout of
+  // Velo::Clusters_t when half_t is half (backend/include/CUDABackend.h, VeloEventModel.cuh:92-189).
+  struct HalfExportParams {
+    unsigned n_events;
+    const unsigned* offsets_estimated_input_size;
+    const char* sorted_container;
+    const unsigned* offsets_all_velo_tracks;
+    const unsigned* offsets_velo_track_hit_number;
+    const char* velo_track_hits;
+    unsigned cluster_capacity, track_capacity, track_hit_capacity;
+    char* sorted_half;
+    char* track_hits_half;
+    unsigned* status;
+  };
+  __global__ void export_half_kernel(HalfExportParams p);
+
   // order[0..n) = the slice's events by raw size, largest first (one CTA)
   __global__ void event_order_kernel(RawInput in, unsigned* order);
   __global__ void exclusive_scan_kernel(ScanParams p);

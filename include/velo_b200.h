@@ -23,8 +23,9 @@
  *
  * Conventions: plain pointers and sizes only; every function returns a VeloStatus
  * (0 = success) instead of throwing (the reference throws from cudaCheck,
- * backend/include/CUDABackend.h:23-41); the caller owns the CUDA stream; the chain owns
- * its device workspace, sized once by velo_chain_reserve().
+ * backend/include/CUDABackend.h:23-41); the caller owns the CUDA stream; the device workspace
+ * is either the chain's own (velo_chain_reserve) or the caller's (velo_chain_sizes +
+ * velo_chain_bind, outputs included).
  */
 #ifndef VELO_B200_H
 #define VELO_B200_H
@@ -147,6 +148,59 @@ VeloStatus velo_chain_create(
  * set_arguments_size() + arena reservation (stream/gear/include/Scheduler.cuh:353-387). */
 VeloStatus velo_chain_reserve(
   VeloChain* chain, unsigned max_events, unsigned long long max_super_pixels, unsigned long long max_raw_bytes);
+
+/* Caller-owned memory (Allen's model: the scheduler's per-stream arena owns every buffer,
+ * stream/store/include/MemoryManager.cuh:100-135, sized by each algorithm's set_arguments_size,
+ * stream/gear/include/Scheduler.cuh:31-137).  velo_chain_sizes() gives, for slices of up to
+ * max_events events and max_super_pixels super pixels, the element count of every output the
+ * caller supplies and the bytes of scratch workspace; velo_chain_bind() then makes the chain use
+ * that memory instead of its own: no allocation happens in it or in the runs that follow (the
+ * chain's fixed buffers, a few KB plus one 16 KiB ring per resident search CTA, come from
+ * velo_chain_create / velo_chain_configure).  Binding the same memory and bounds again is free;
+ * new pointers drop the cached graphs.  Outputs hold the reference's layouts and names;
+ * max_reconstructed_tracks bounds host_number_of_reconstructed_velo_tracks. */
+typedef struct {
+  unsigned long long offsets_estimated_input_size;       /* u32 elements: 26 N + 1 */
+  unsigned long long module_cluster_num;                 /* u32: 26 N */
+  unsigned long long sorted_velo_cluster_container_bytes; /* 18 (FP16: 12) x T, T = 2 x super pixels + 64 */
+  unsigned long long offsets_all_velo_tracks;            /* u32: N + 1 */
+  unsigned long long velo_track_hit_number;              /* u32: tracks */
+  unsigned long long offsets_velo_track_hit_number;      /* u32: tracks + 1 */
+  unsigned long long velo_track_hits_bytes;              /* 18 (FP16: 12) x T */
+  unsigned long long accepted_velo_tracks;               /* bytes: 2 x tracks */
+  unsigned long long max_reconstructed_tracks;           /* tracks = max(0.34 T, 10 N) + 64 */
+  unsigned long long workspace_bytes;                    /* scratch, 256-byte aligned base */
+} VeloChainSizes;
+
+typedef struct {
+  unsigned* dev_offsets_estimated_input_size;
+  unsigned* dev_module_cluster_num;
+  char* dev_sorted_velo_cluster_container;
+  unsigned* dev_offsets_all_velo_tracks;
+  unsigned* dev_velo_track_hit_number;
+  unsigned* dev_offsets_velo_track_hit_number;
+  char* dev_velo_track_hits;
+  uint8_t* dev_accepted_velo_tracks;
+} VeloChainOutputBuffers; /* device pointers, 16-byte aligned (the last one any alignment) */
+
+/* Coordinate layout of the two cluster containers a caller supplies (dev_sorted_velo_cluster_container,
+ * dev_velo_track_hits): FP32, as the reference's CPU build lays out Velo::Clusters_t (half_t = float,
+ * 18 bytes per element), or FP16, as its CUDA build does (half_t = half, backend/include/CUDABackend.h:14;
+ * 12 bytes: u32 id[T], half xyz[3T], i16 phi[T]).  The chain computes in FP32 either way (its
+ * results are the CPU build's) and, for FP16, rounds the coordinates to nearest when it writes
+ * the caller's containers. */
+typedef enum { VELO_COORDINATES_FP32 = 0, VELO_COORDINATES_FP16 = 1 } VeloCoordinateLayout;
+
+VeloStatus velo_chain_sizes( /* chain may be NULL: the sizes depend on the bounds and layout alone */
+  const VeloChain* chain, unsigned max_events, unsigned long long max_super_pixels, int layout, VeloChainSizes* sizes);
+VeloStatus velo_chain_bind(
+  VeloChain* chain,
+  void* dev_workspace,
+  unsigned long long workspace_bytes,
+  unsigned max_events,
+  unsigned long long max_super_pixels,
+  int layout,
+  const VeloChainOutputBuffers* outputs);
 
 /* Enqueues the whole chain on `stream` for a device-resident slice: velo_calculate_number_of_candidates,
  * velo_estimate_input_size, velo_masked_clustering, velo_sort_by_phi, velo_search_by_triplet,
@@ -275,14 +329,14 @@ VeloStatus velo_chain_set_front_end(VeloChain* chain, int retina_clusters);
  * wired at configuration/python/AllenConf/velo_reconstruction.py:295-322): the simplified
  * Kalman fit of every consolidated track to the beamline and to the end of the VELO.
  * velo_chain_set_kalman() appends it to the chain (outputs in VeloChainOutputs; beamline =
- * Constants::dev_beamline, 0, 0 in beamline.bin).  velo_kalman_filter() runs it alone on
+ * Constants::dev_beamline, 0, 0 in beamline.bin).  velo_run_kalman_filter() runs it alone on
  * caller buffers, allocating nothing: inputs are the consolidation outputs, outputs
  * dev_is_backward [tracks] and the two Velo::Consolidated::States containers (56 bytes per
  * track, 8-byte aligned).  States are bit-identical to the reference CPU build; the fields
  * the reference leaves unwritten (qop, chi2, ndof) are written as 0.  track_capacity bounds
  * the reconstructed tracks (more raise err_output_capacity in dev_status, optional). */
 VeloStatus velo_chain_set_kalman(VeloChain* chain, int enable, float beamline_x, float beamline_y);
-VeloStatus velo_kalman_filter(
+VeloStatus velo_run_kalman_filter(
   unsigned n_events,
   const unsigned* dev_offsets_all_velo_tracks,
   const unsigned* dev_offsets_velo_track_hit_number,
@@ -293,6 +347,54 @@ VeloStatus velo_kalman_filter(
   uint8_t* dev_is_backward,
   char* dev_velo_kalman_beamline_states,
   char* dev_velo_kalman_endvelo_states,
+  unsigned* dev_status,
+  VeloStream stream);
+
+/* The consolidated track views (create_velo_views,
+ * device/velo/consolidate_tracks/src/VeloConsolidateTracks.cu:11-46): plain structs with the
+ * layouts of Allen::Views::Velo::Consolidated::{Hits, Track, Tracks, MultiEventTracks}
+ * (device/event_model/velo/include/VeloConsolidated.cuh:58-298; 24, 24, 16 and 24 bytes), so
+ * that the reference's consumers (velo_kalman_filter's dev_velo_tracks_view,
+ * configuration/python/AllenConf/velo_reconstruction.py:295-307) read them as their own types.
+ * velo_create_velo_views() writes them from the consolidated outputs into caller buffers:
+ * dev_velo_hits_view [N], dev_velo_track_view [track_capacity >= reconstructed tracks],
+ * dev_velo_tracks_view [N], dev_velo_multi_event_tracks_view [1] and dev_imec_velo_tracks [1]
+ * (a pointer to the multi-event view).  Allocates nothing; more tracks than track_capacity set
+ * err_output_capacity in dev_status (optional) and write nothing. */
+typedef struct {
+  const void* base_pointer;      /* dev_velo_track_hits */
+  unsigned offset;               /* the event's first track hit */
+  unsigned size;                 /* the event's track hits */
+  unsigned total_number_of_hits; /* track hits of the slice */
+} VeloHitsView;
+typedef struct {
+  const VeloHitsView* hits;        /* the event's Hits view */
+  unsigned track_index;            /* within the event */
+  unsigned track_container_offset; /* the event's first track */
+  unsigned offset;                 /* first hit of the track, relative to the event */
+  unsigned number_of_hits;
+} VeloTrackView;
+typedef struct {
+  const VeloTrackView* track; /* the event's first Track view */
+  unsigned size;
+  unsigned offset;
+} VeloTracksView;
+typedef struct {
+  int type_id; /* Allen::TypeIDs::VeloTracks = 1 */
+  const VeloTracksView* container;
+  unsigned number_of_events;
+} VeloMultiEventTracksView;
+VeloStatus velo_create_velo_views(
+  unsigned n_events,
+  const char* dev_velo_track_hits,
+  const unsigned* dev_offsets_all_velo_tracks,
+  const unsigned* dev_offsets_velo_track_hit_number,
+  VeloHitsView* dev_velo_hits_view,
+  VeloTrackView* dev_velo_track_view,
+  unsigned track_capacity,
+  VeloTracksView* dev_velo_tracks_view,
+  VeloMultiEventTracksView* dev_velo_multi_event_tracks_view,
+  const void** dev_imec_velo_tracks,
   unsigned* dev_status,
   VeloStream stream);
 

@@ -33,5 +33,14 @@ def build_oracle(ref_root: str | None = None, with_reference: bool = True) -> No
         subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={root}"], check=True)
 
 
+def build_allen_harness(ref_root: str | None = None) -> None:
+    """integration/VeloB200Chain.cu with the reference's headers and velo_kalman_filter, and the
+    harness that runs them (tests/allen_harness), where the reference tree exists."""
+    root = ref_root or reference_root()
+    if root:
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(REPO, "tests", "allen_harness"), f"REF_ROOT={root}"],
+                       check=True)
+
+
 if __name__ == "__main__":
     build_oracle(sys.argv[1] if len(sys.argv) > 1 else None)

@@ -32,7 +32,7 @@ def test_chain_kalman_matches_oracle(chain, oracle, geometry, beamline):
 
 
 def test_standalone_kalman_entry_point(chain, oracle, geometry):
-    """velo_kalman_filter() on the chain's consolidated outputs, into caller buffers."""
+    """velo_run_kalman_filter() on the chain's consolidated outputs, into caller buffers."""
     import torch
     from allen_b200.chain import _current_stream
     g = generator.generate(60, seed=56)
@@ -45,7 +45,7 @@ def test_standalone_kalman_entry_point(chain, oracle, geometry):
     beam = torch.zeros(56 * reco + 8, dtype=torch.uint8, device="cuda")
     end = torch.zeros(56 * reco + 8, dtype=torch.uint8, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
-    st = chain.lib.velo_kalman_filter(g.raw.n_events, p["dev_offsets_all_velo_tracks"],
+    st = chain.lib.velo_run_kalman_filter(g.raw.n_events, p["dev_offsets_all_velo_tracks"],
                                       p["dev_offsets_velo_track_hit_number"], p["dev_velo_track_hits"], reco,
                                       0.0, 0.0, back.data_ptr(), beam.data_ptr(), end.data_ptr(), status.data_ptr(),
                                       _current_stream())
@@ -61,7 +61,7 @@ def test_standalone_kalman_entry_point(chain, oracle, geometry):
                           ref["dev_velo_kalman_endvelo_states"].view(np.uint32)[w])
     # too small a capacity is reported, nothing written
     status.zero_()
-    st = chain.lib.velo_kalman_filter(g.raw.n_events, p["dev_offsets_all_velo_tracks"],
+    st = chain.lib.velo_run_kalman_filter(g.raw.n_events, p["dev_offsets_all_velo_tracks"],
                                       p["dev_offsets_velo_track_hit_number"], p["dev_velo_track_hits"], reco - 1,
                                       0.0, 0.0, back.data_ptr(), beam.data_ptr(), end.data_ptr(), status.data_ptr(),
                                       _current_stream())
