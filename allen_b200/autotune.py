@@ -7,7 +7,9 @@ persistent launches with a work queue (events claimed per CTA) against one CTA p
 coordinate descent: each parameter in turn takes the
 value with the highest events/s (CUDA-event timed graph replays) while the others stay at
 the current best.  The winner is written to allen_b200/data/launch_config.json, which
-VeloChain loads by default.
+VeloChain loads by default.  tune_learned() does the same for the learned mode, with the seed
+gate's threshold and the seed window as coordinates constrained by tracking quality (run by
+allen_b200.train_seed_pruner).
 
     python -m allen_b200.autotune [--events 16000] [--pileup-min 1 --pileup-max 15]
 """
@@ -104,6 +106,85 @@ def sweep_coordinate(name, values, best, best_rate, try_config):
             best_rate = rate
             best.update(upd)
     return best_rate
+
+
+# learned mode: the gate's recall targets (each a logit threshold from the calibration), the
+# seed window (h0 candidates per seed candidate; 0 = the reference's 4), the gated search kernels
+# and the events a persistent CTA claims
+GATE_RECALLS = [0.97, 0.98, 0.99, 0.995]
+SEED_WINDOWS = [0, 3, 2]
+GATED_SEARCH = [(128, 1), (256, 1), (96, 1), (64, 1)]
+CLAIMS = [1, 2, 4]
+
+
+def tune_learned(chain, model, thresholds: dict, dev_slices, quality, plain_quality: dict, tolerance: float = 0.002,
+                 log=print, max_sweeps: int = 3) -> tuple[dict, float, list]:
+    """The learned mode's seed gate and window, jointly with its launch configuration.
+
+    thresholds: recall target -> logit threshold; quality(chain) -> {"efficiency", "ghost_rate"}
+    of the chain's current mode on held-out events; plain_quality: the plain search's on the
+    same events.  A (threshold, window) pair is admissible when its efficiency is at most
+    `tolerance` below the plain search's and its ghost rate at most `tolerance` above; among
+    admissible pairs, gated search kernels and claims, coordinate descent on events/s picks the
+    best.  Returns ({"recall", "threshold_logit", "seed_window", launch parameters}, events/s,
+    trials); the chain is left configured with it."""
+    trials = []
+    admissible = []
+    for recall, thr in sorted(thresholds.items()):
+        for window in SEED_WINDOWS:
+            model.threshold_logit = float(thr)
+            chain.set_seed_model(model)
+            chain.configure(seed_window=window)
+            q = quality(chain)
+            ok = (q["efficiency"] >= plain_quality["efficiency"] - tolerance and
+                  q["ghost_rate"] <= plain_quality["ghost_rate"] + tolerance)
+            trials.append({"recall": recall, "seed_window": window, "quality": q, "admissible": ok})
+            log(f"recall {recall} window {window}: {q} {'ok' if ok else 'out of tolerance'}")
+            if ok:
+                admissible.append((recall, window))
+    if not admissible:
+        raise RuntimeError("no gate threshold keeps the learned mode within tolerance")
+    best = {"gate": admissible[-1], "search": (chain.get_config()["search_threads"], 1),
+            "events_per_claim": chain.get_config()["events_per_claim"]}
+
+    def apply(b):
+        recall, window = b["gate"]
+        model.threshold_logit = float(thresholds[recall])
+        chain.configure(search_threads=b["search"][0], search_lanes_per_seed=0, search_ring_global=b["search"][1],
+                        persistent=1, events_per_claim=b["events_per_claim"], seed_window=window)
+        chain.set_seed_model(model)
+
+    def rate_of(b):
+        try:
+            apply(b)
+        except Exception as exc:
+            log(f"skip {b}: {exc}")
+            return None
+        r = measure(chain, dev_slices)
+        trials.append({"learned": dict(b), "events_per_s": r})
+        log(f"{b} -> {r:,.0f} events/s")
+        return r
+
+    best_rate = rate_of(best) or 0.0
+    for _ in range(max_sweeps):
+        before = dict(best)
+        for name, values in (("gate", admissible), ("search", GATED_SEARCH), ("events_per_claim", CLAIMS)):
+            for v in values:
+                cand = dict(best)
+                cand[name] = v
+                if cand == best:
+                    continue
+                r = rate_of(cand)
+                if r is not None and r > best_rate:
+                    best, best_rate = cand, r
+        if best == before:
+            break
+    apply(best)
+    recall, window = best["gate"]
+    result = {"recall": recall, "threshold_logit": float(thresholds[recall]), "seed_window": window,
+              "search_threads": best["search"][0], "search_ring_global": best["search"][1],
+              "events_per_claim": best["events_per_claim"]}
+    return result, best_rate, trials
 
 
 def main():

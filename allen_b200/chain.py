@@ -66,7 +66,7 @@ OUTPUT_FIELDS = [
     "dev_velo_track_hit_number", "dev_offsets_velo_track_hit_number", "dev_velo_track_hits",
     "dev_accepted_velo_tracks", "dev_seed_stats", "dev_is_backward", "dev_velo_kalman_beamline_states",
     "dev_velo_kalman_endvelo_states", "dev_each_sensor_pair_size", "dev_offsets_each_sensor_pair_size",
-    "dev_retina_bank_index",
+    "dev_retina_bank_index", "dev_seed_gate", "dev_gate_stats",
 ]
 
 
@@ -89,7 +89,7 @@ class LaunchConfigC(C.Structure):
     _fields_ = [(f, C.c_uint) for f in (
         "search_threads", "search_lanes_per_seed", "search_hit_capacity", "cluster_stage_capacity",
         "cluster_blob_bytes", "estimate_blob_bytes", "persistent", "events_per_claim", "search_ring_global",
-        "cluster_threads", "retina_order_capacity", "kalman_warp_hits")]
+        "cluster_threads", "retina_order_capacity", "kalman_warp_hits", "seed_window")]
 
 
 class TotalsC(C.Structure):
@@ -176,8 +176,8 @@ def _lib():
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.velo_chain_set_seed_model.restype = C.c_int
     lib.velo_chain_set_seed_model.argtypes = [C.c_void_p, C.POINTER(SeedModelC)]
-    lib.velo_chain_record_doublets.restype = C.c_int
-    lib.velo_chain_record_doublets.argtypes = [C.c_void_p, C.c_void_p, C.c_uint, C.c_uint, C.c_void_p]
+    lib.velo_chain_record_seeds.restype = C.c_int
+    lib.velo_chain_record_seeds.argtypes = [C.c_void_p, C.c_void_p, C.c_uint, C.c_uint, C.c_void_p]
     lib.velo_seed_trainer_create.restype = C.c_int
     lib.velo_seed_trainer_create.argtypes = [C.POINTER(SeedModelC), C.c_float, C.c_float, C.POINTER(C.c_void_p)]
     lib.velo_seed_trainer_step.restype = C.c_int
@@ -351,20 +351,25 @@ class VeloChain:
         """model: a SeedModelC (learned search) or None (plain search)."""
         _check(self.lib, self.lib.velo_chain_set_seed_model(self.handle, C.byref(model) if model is not None else None))
 
-    def record_doublets(self, records, count, every: int = 1):
-        """records: device uint8 tensor of 64-byte VeloDoubletRecord entries, count: device
+    def record_seeds(self, records, count, every: int = 1):
+        """records: device uint8 tensor of 64-byte VeloSeedRecord entries, count: device
         int32 tensor of one element (zeroed by the caller); None stops the recording."""
         if records is None:
-            _check(self.lib, self.lib.velo_chain_record_doublets(self.handle, None, 0, 1, None))
+            _check(self.lib, self.lib.velo_chain_record_seeds(self.handle, None, 0, 1, None))
         else:
-            _check(self.lib, self.lib.velo_chain_record_doublets(self.handle, records.data_ptr(), records.numel() // 64,
-                                                                 every, count.data_ptr()))
+            _check(self.lib, self.lib.velo_chain_record_seeds(self.handle, records.data_ptr(), records.numel() // 64,
+                                                              every, count.data_ptr()))
 
     def seed_stats(self, n_events: int) -> np.ndarray:
-        """[n_events, 3]: doublets formed, doublets scanned, search mode (0 plain, 1 learned,
-        2 learned then plain) of the last run."""
+        """[n_events, 3]: seed candidates met unused, candidates searched, search mode (0 plain,
+        1 learned, 2 gate out of its bounds: plain) of the last run."""
         p = self.device_outputs()["dev_seed_stats"]
         return self._fetch(p, 12 * n_events, np.uint8).view(np.uint32).reshape(n_events, 3)
+
+    def gate_stats(self, n_events: int) -> np.ndarray:
+        """[n_events, 2] of the last learned run: seed candidates, candidates the gate kept."""
+        p = self.device_outputs()["dev_gate_stats"]
+        return self._fetch(p, 8 * n_events, np.uint8).view(np.uint32).reshape(n_events, 2)
 
     def device_outputs(self) -> dict:
         o = OutputsC()

@@ -218,14 +218,14 @@ static constexpr unsigned retina_key_capacity = 0;
 static constexpr unsigned retina_order_capacity_max = 8192;
 static constexpr size_t n_sensors_total = velo::n_sensors;
 
-static SearchKernel learned_search_kernel(unsigned threads, unsigned ring_global = 0)
+// search_by_triplet_gated_kernel instantiations (block size, ring place)
+static SearchKernel gated_search_kernel(unsigned threads, unsigned ring_global)
 {
-  switch (threads) {
-    case 128: return ring_global ? velo::search_by_triplet_learned_kernel<128, 1> : velo::search_by_triplet_learned_kernel<128, 0>;
-    case 256: return ring_global ? velo::search_by_triplet_learned_kernel<256, 1> : velo::search_by_triplet_learned_kernel<256, 0>;
-    case 512: return ring_global ? nullptr : velo::search_by_triplet_learned_kernel<512, 0>;
-    default: return nullptr;
-  }
+#define VELO_GATED_VARIANT(T, R) \
+  if (threads == T && ring_global == R) return velo::search_by_triplet_gated_kernel<T, R>;
+  VELO_GATED_CONFIGS(VELO_GATED_VARIANT)
+#undef VELO_GATED_VARIANT
+  return nullptr;
 }
 
 static const SearchVariant* find_search_variant(unsigned threads, unsigned lanes, unsigned ring_global = 0)
@@ -235,9 +235,9 @@ static const SearchVariant* find_search_variant(unsigned threads, unsigned lanes
   return nullptr;
 }
 
-static constexpr unsigned n_timed_kernels = 8;
+static constexpr unsigned n_timed_kernels = 9;
 static const char* const kernel_names[n_timed_kernels] = {
-  "estimate_kernel", "exclusive_scan_kernel(candidates, estimates)", "cluster_sort_kernel",
+  "estimate_kernel", "exclusive_scan_kernel(candidates, estimates)", "cluster_sort_kernel", "seed_gate_kernel",
   "search_by_triplet_kernel", "exclusive_scan_kernel(tracks, three-hit, track hits)", "consolidate_kernel",
   "kalman_filter_kernel", "totals_kernel"};
 
@@ -265,6 +265,7 @@ struct VeloChain {
   unsigned cluster_threads = 256;  // block size of the clustering kernel (128 or 256)
   unsigned retina_order_capacity = retina_order_capacity_max; // retina clusters ranked through key buckets
   unsigned kalman_warp_hits = velo::kalman_warp_hits;         // Kalman: hits of a warp's tracks staged
+  unsigned seed_window = 0;                                   // learned mode: h0 candidates per seed candidate
   unsigned resident_kalman = 0;                               // Kalman CTAs resident on the device
   unsigned resident_export = 0;                               // half-layout export CTAs
   unsigned resident_estimate = 0, resident_cluster = 0, resident_search = 0; // CTAs that fit the device
@@ -286,9 +287,12 @@ struct VeloChain {
   cudaEvent_t done = nullptr;
   cudaStream_t capture_stream = nullptr; // graphs are captured here (the legacy stream cannot be)
 
-  // learned seed pruner and training-doublet recording
+  // learned seed gate and training-record recording
   DeviceBuffer<velo::MlpModelDevice> seed_model;
   bool learned = false;
+  float kept_lo = 0.f, kept_hi = 1.f; // per-event bounds of the gate's kept fraction
+  DeviceBuffer<uint8_t> seed_gate, h1_outcome;
+  DeviceBuffer<unsigned> gate_stats;
   DeviceBuffer<unsigned> seed_stats;
   DeviceBuffer<unsigned> queue_next, event_order; // persistent launches: 3 claim counters, event order
   // velo_kalman_filter after consolidation (optional)
@@ -300,7 +304,7 @@ struct VeloChain {
   DeviceBuffer<unsigned> retina_sizes, retina_offsets, retina_bank_index;
   DeviceBuffer<long long> retina_keys;
   DeviceBuffer<float> kalman_beamline_states, kalman_endvelo_states;
-  velo::DoubletRecord* records = nullptr;
+  velo::SeedRecord* records = nullptr;
   unsigned* record_count = nullptr;
   unsigned record_capacity = 0, record_every = 1;
 
@@ -391,6 +395,9 @@ namespace {
     f(c->three_out, tracks, scratch_buffer);
     f(c->hit_used, T, scratch_buffer);
     f(c->seed_stats, 3 * n, scratch_buffer);
+    f(c->seed_gate, T, scratch_buffer);
+    f(c->h1_outcome, T, scratch_buffer);
+    f(c->gate_stats, 2 * n, scratch_buffer);
     f(c->queue_next, 3, scratch_buffer);
     f(c->is_backward, tracks, scratch_buffer);
     f(c->retina_sizes, n * n_sensors_total, scratch_buffer);
@@ -620,21 +627,51 @@ namespace {
     sp.ring_scratch = c->ring_scratch.p;
     sp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
     sp.seed_stats = c->seed_stats.p;
-    sp.seed_model = c->learned ? c->seed_model.p : nullptr;
-    sp.records = c->records;
-    sp.record_count = c->record_count;
-    sp.record_capacity = c->record_capacity;
-    sp.record_every = c->record_every;
+    sp.seed_gate = c->learned ? c->seed_gate.p : nullptr;
+    sp.gate_stats = c->gate_stats.p;
+    sp.kept_lo = c->kept_lo;
+    sp.kept_hi = c->kept_hi;
+    sp.h1_outcome = c->records ? c->h1_outcome.p : nullptr;
+    sp.seed_window = c->seed_window;
     sp.queue = queue(2);
+    GateParams gp {};
+    gp.geo = c->geo.p;
+    gp.k = c->k;
+    gp.n_events = n;
+    gp.offsets_estimated_input_size = c->offsets_est.p;
+    gp.module_cluster_num = c->cluster_num.p;
+    gp.sorted_container = c->sorted.p;
+    gp.cluster_capacity = static_cast<unsigned>(c->cap_clusters);
+    gp.model = c->seed_model.p;
+    gp.gate = c->seed_gate.p;
+    gp.gate_stats = c->gate_stats.p;
+    gp.h1_outcome = c->h1_outcome.p;
+    gp.records = c->records;
+    gp.record_count = c->record_count;
+    gp.record_capacity = c->record_capacity;
+    gp.record_every = c->record_every;
+    gp.status = c->status.p;
+    if (c->learned) {
+      // the gate of every seed candidate, before the search
+      seed_gate_kernel<false><<<n, gate_threads, 0, stream>>>(gp);
+      VELO_CUDA(cudaGetLastError());
+    }
+    VELO_CUDA(mark());
+    if (c->records) VELO_CUDA(cudaMemsetAsync(c->h1_outcome.p, 0, c->cap_clusters, stream));
     const unsigned search_smem = c->search_hit_capacity * search_hit_bytes;
     {
       const SearchKernel fn =
-        (c->learned || c->records) ? learned_search_kernel(c->search_threads, c->search_ring_global) : nullptr;
+        (c->learned || c->records) ? gated_search_kernel(c->search_threads, c->search_ring_global) : nullptr;
       const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes, c->search_ring_global);
       if (!fn && !v) return fail(VELO_ERR_ARGUMENT, "no compiled search kernel for this launch configuration");
       void* args[] = {&sp};
       VELO_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(fn ? fn : v->fn), dim3(grid(c->resident_search)),
                                  dim3(c->search_threads), args, search_smem, stream));
+    }
+    if (c->records) {
+      // training records: the features of the candidates the search met, with its outcomes
+      seed_gate_kernel<true><<<n, gate_threads, 0, stream>>>(gp);
+      VELO_CUDA(cudaGetLastError());
     }
     VELO_CUDA(mark());
 
@@ -718,10 +755,10 @@ namespace {
     VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(cluster_sort_kernel<256>), cluster_smem));
     for (const auto& v : search_variants)
       VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(v.fn), search_smem));
-    for (unsigned threads : {128u, 256u, 512u})
-      for (unsigned ring : {0u, 1u})
-        if (learned_search_kernel(threads, ring))
-          VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(learned_search_kernel(threads, ring)), search_smem));
+#define VELO_GATED_LIMIT(T, R) \
+    VELO_CUDA(raise_dynamic_smem_limit(reinterpret_cast<const void*>(search_by_triplet_gated_kernel<T, R>), search_smem));
+    VELO_GATED_CONFIGS(VELO_GATED_LIMIT)
+#undef VELO_GATED_LIMIT
     // CTAs of each kernel resident on the device at once: the grid of a persistent launch
     int sms = 0, per_sm = 0;
     VELO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
@@ -737,7 +774,7 @@ namespace {
       VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_sort_kernel<256>, 256, cluster_smem));
     c->resident_cluster = unsigned(std::max(per_sm, 1) * sms);
     const SearchVariant* v = find_search_variant(c->search_threads, c->search_lanes, c->search_ring_global);
-    const SearchKernel learned = learned_search_kernel(c->search_threads, c->search_ring_global);
+    const SearchKernel learned = gated_search_kernel(c->search_threads, c->search_ring_global);
     SearchKernel fn = (c->learned || c->records) && learned ? learned : (v ? v->fn : nullptr);
     if (fn) {
       VELO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, int(c->search_threads), search_smem));
@@ -1006,6 +1043,7 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
     return fail(VELO_ERR_ARGUMENT, "retina_order_capacity above 8192");
   if (cfg->kalman_warp_hits > velo::kalman_warp_hits)
     return fail(VELO_ERR_ARGUMENT, "kalman_warp_hits above 368");
+  if (cfg->seed_window > 4) return fail(VELO_ERR_ARGUMENT, "seed_window above 4");
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   const unsigned search_static = 32 * 1024; // upper bound of the kernel's static shared memory
@@ -1028,6 +1066,7 @@ VeloStatus velo_chain_configure(VeloChain* c, const VeloLaunchConfig* cfg)
   c->cluster_threads = cfg->cluster_threads;
   c->retina_order_capacity = cfg->retina_order_capacity;
   c->kalman_warp_hits = cfg->kalman_warp_hits;
+  c->seed_window = cfg->seed_window;
   return configure_kernels(c);
 }
 
@@ -1046,6 +1085,7 @@ VeloStatus velo_chain_get_config(const VeloChain* c, VeloLaunchConfig* cfg)
   cfg->cluster_threads = c->cluster_threads;
   cfg->retina_order_capacity = c->retina_order_capacity;
   cfg->kalman_warp_hits = c->kalman_warp_hits;
+  cfg->seed_window = c->seed_window;
   return VELO_OK;
 }
 
@@ -1138,6 +1178,8 @@ VeloStatus velo_chain_outputs(const VeloChain* c, VeloChainOutputs* o)
   o->dev_each_sensor_pair_size = c->retina ? c->retina_sizes.p : nullptr;
   o->dev_offsets_each_sensor_pair_size = c->retina ? c->retina_offsets.p : nullptr;
   o->dev_retina_bank_index = c->retina ? c->retina_bank_index.p : nullptr;
+  o->dev_seed_gate = c->seed_gate.p;
+  o->dev_gate_stats = c->gate_stats.p;
   o->dev_velo_kalman_beamline_states = reinterpret_cast<char*>(c->kalman_beamline_states.p);
   o->dev_velo_kalman_endvelo_states = reinterpret_cast<char*>(c->kalman_endvelo_states.p);
   return VELO_OK;
@@ -1278,27 +1320,29 @@ VeloStatus velo_chain_set_seed_model(VeloChain* c, const VeloSeedModel* model)
     c->learned = false;
     return configure_kernels(c); // the persistent grid follows the kernel the chain launches
   }
-  if (!learned_search_kernel(c->search_threads, c->search_ring_global))
-    return fail(VELO_ERR_ARGUMENT, "the learned search needs search_threads 128, 256 or 512 (128 or 256 with global rings)");
+  if (!gated_search_kernel(c->search_threads, c->search_ring_global))
+    return fail(VELO_ERR_ARGUMENT, "the learned search needs flat seeding (search_lanes_per_seed 0)");
   std::vector<float> params(VELO_SEED_PARAMS);
   velo::model_params(*model, params.data());
   velo::MlpModelDevice d;
   velo::make_model_device(params.data(), *model, d);
   if (c->seed_model.reserve(1) != cudaSuccess) return fail(VELO_ERR_CUDA, "seed model allocation failed");
   VELO_CUDA(cudaMemcpy(c->seed_model.p, &d, sizeof(d), cudaMemcpyHostToDevice));
+  c->kept_lo = model->kept_lo;
+  c->kept_hi = model->kept_hi;
   c->learned = true;
   return configure_kernels(c);
 }
 
-VeloStatus velo_chain_record_doublets(
-  VeloChain* c, VeloDoubletRecord* records, unsigned capacity, unsigned record_every, unsigned* dev_count)
+VeloStatus velo_chain_record_seeds(
+  VeloChain* c, VeloSeedRecord* records, unsigned capacity, unsigned record_every, unsigned* dev_count)
 {
   if (!c) return fail(VELO_ERR_ARGUMENT, "null chain");
   if (records && (!dev_count || record_every == 0)) return fail(VELO_ERR_ARGUMENT, "recording needs a counter and record_every > 0");
-  if (records && !learned_search_kernel(c->search_threads, c->search_ring_global))
-    return fail(VELO_ERR_ARGUMENT, "recording needs search_threads 128, 256 or 512 (128 or 256 with global rings)");
+  if (records && !gated_search_kernel(c->search_threads, c->search_ring_global))
+    return fail(VELO_ERR_ARGUMENT, "recording needs flat seeding (search_lanes_per_seed 0)");
   c->release_graph();
-  c->records = reinterpret_cast<velo::DoubletRecord*>(records);
+  c->records = reinterpret_cast<velo::SeedRecord*>(records);
   c->record_count = records ? dev_count : nullptr;
   c->record_capacity = records ? capacity : 0;
   c->record_every = records ? record_every : 1;

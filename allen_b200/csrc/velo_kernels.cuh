@@ -102,15 +102,15 @@ namespace velo {
     unsigned cluster_capacity;                    // allocated T of the containers
     char* hit_scratch;                            // [16 T] staging of events above the capacity
     uint64_t* ring_scratch;                       // [2048 grid] rings of tracks to follow (RING = 1)
-    // learned seed pruning (search_by_triplet_learned_kernel): the network, or null for the
-    // plain search
-    const MlpModelDevice* seed_model;
-    unsigned* seed_stats;                         // [3 N] doublets found, doublets kept, mode
-    // recording of training doublets (search_by_triplet_learned_kernel): null = off
-    DoubletRecord* records;
-    unsigned* record_count;
-    unsigned record_capacity;
-    unsigned record_every;                        // record the doublets of one h1 in record_every
+    // learned seed gate (search_by_triplet_gated_kernel): a byte per hit, 0 = the hit is not
+    // searched as a seed's middle hit; null = the plain search
+    const uint8_t* seed_gate;                     // [T]
+    const unsigned* gate_stats;                   // [2 N] seed candidates, candidates the gate keeps
+    float kept_lo, kept_hi;                       // an event whose kept fraction is outside: plain search
+    unsigned* seed_stats;                         // [3 N] candidates met, candidates searched, mode
+    uint8_t* h1_outcome;                          // [T] training labels (gated kernel): 1 no seed, 2 seed
+    unsigned seed_window;                         // learned mode: h0 candidates per seed candidate after
+                                                  // the first module pair (0: the reference's 4)
     WorkQueue queue;
   };
 
@@ -166,10 +166,11 @@ namespace velo {
   __global__ void cluster_sort_kernel(ClusterSortParams p);
   template<unsigned THREADS, unsigned LPH, unsigned RING>
   __global__ void search_by_triplet_kernel(SearchParams p);
-  // flat seeding with the learned seed pruner and doublet recording, THREADS = 128, 256, 512;
-  // RING = 1 (128 and 256 threads): the ring of tracks to follow in global scratch
+  // flat seeding behind the learned seed gate (and seed-candidate outcome recording);
+  // RING = 1: the ring of tracks to follow in global scratch (persistent launches)
   template<unsigned THREADS, unsigned RING>
-  __global__ void search_by_triplet_learned_kernel(SearchParams p);
+  __global__ void search_by_triplet_gated_kernel(SearchParams p);
+#define VELO_GATED_CONFIGS(X) X(128, 0) X(256, 0) X(512, 0) X(128, 1) X(256, 1) X(96, 1) X(64, 1)
   // (block size, lanes per seed candidate) pairs compiled for the autotuner
 // lanes 0 = flattened seeding (one thread per h1 candidate)
 #define VELO_SEARCH_CONFIGS(X)                                                                                  \
@@ -235,6 +236,61 @@ namespace velo {
   // order[0..n) = the slice's events by raw size, largest first (one CTA)
   __global__ void event_order_kernel(RawInput in, unsigned* order);
   __global__ void exclusive_scan_kernel(ScanParams p);
+
+  // Phi buckets of a module pair's sorted hits, shared by the search and the seed gate:
+  // bucket[b] = first index with phi >= b * 512 - 32768 (128 buckets + the end).
+  constexpr unsigned n_buckets = 128;
+  __device__ __forceinline__ unsigned bucket_of(int16_t v) { return static_cast<unsigned>(v + 32768) >> 9; }
+
+  // binary_search_leftmost (BinarySearch.cuh:15-30) through the bucket table of the
+  // module pair: the first index with phi >= value.
+  __device__ __forceinline__ int leftmost(const uint16_t* table, const int16_t* phis, unsigned n, int16_t value)
+  {
+    unsigned i = table[bucket_of(value)];
+    while (i < n && phis[i] < value)
+      ++i;
+    return static_cast<int>(i);
+  }
+
+  // The bucket tables of an event's 26 module pairs (one CTA; phis event-relative).
+  __device__ __forceinline__ void build_bucket_tables(
+    uint16_t (*table)[n_buckets + 1], const int16_t* phis, const unsigned* start, const unsigned* num, unsigned hit_offset)
+  {
+    for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
+      const unsigned s0 = start[mp] - hit_offset;
+      const unsigned cnt = num[mp];
+      uint16_t* t = table[mp];
+      for (unsigned i = threadIdx.x; i <= cnt; i += blockDim.x) {
+        const unsigned lo = i == 0 ? 0u : bucket_of(phis[s0 + i - 1]) + 1;
+        const unsigned hi = i == cnt ? n_buckets : bucket_of(phis[s0 + i]);
+        for (unsigned b = lo; b <= hi; ++b)
+          t[b] = static_cast<uint16_t>(i);
+      }
+    }
+  }
+
+  // ---- learned seed gate (velo_gate.cu): one byte per hit, 1 = searched as a seed's middle hit ----
+  struct GateParams {
+    Geometry const* geo;
+    Constants k;
+    unsigned n_events;
+    const unsigned* offsets_estimated_input_size;
+    const unsigned* module_cluster_num;
+    const char* sorted_container;
+    unsigned cluster_capacity;
+    const MlpModelDevice* model; // inference
+    uint8_t* gate;               // [T] inference output
+    unsigned* gate_stats;        // [2 N] seed candidates (hits of module pairs 1..24), kept
+    const uint8_t* h1_outcome;   // [T] recording input: 1 no seed, 2 seed (from the search)
+    SeedRecord* records;         // recording output
+    unsigned* record_count;
+    unsigned record_capacity;
+    unsigned record_every;       // one candidate in record_every (hash of event and hit)
+    unsigned* status;
+  };
+  template<bool RECORD>
+  __global__ void seed_gate_kernel(GateParams p);
+  constexpr unsigned gate_threads = 256;
 
   // Raises a kernel's dynamic shared-memory limit to at least `bytes`, never lowers it: the
   // limit is per kernel and per device, shared by every chain and entry point in the process.

@@ -1,7 +1,7 @@
 // Training of the learned seed pruner on sm_100a, and the host conversion of a model to
 // its device form.  No counterpart in the reference (see velo_mlp.cuh).
 //
-// mlp_train_kernel: each warp takes 16-doublet tiles; the forward pass keeps every layer in
+// mlp_train_kernel: each warp takes 16-record tiles; the forward pass keeps every layer in
 // mma.sync fragments (C layout of one layer = A layout of the next); the backward pass gets
 // the transposed operands of the weight gradients (dZ^T as A, the layer input as B) with
 // movmatrix, so no tile goes through shared memory.  Per-warp gradient sums are reduced in
@@ -92,7 +92,7 @@ namespace velo {
 namespace velo {
 
   struct TrainParams {
-    const DoubletRecord* records;
+    const SeedRecord* records;
     unsigned long long first;
     unsigned batch;
     float inv_batch;
@@ -103,7 +103,7 @@ namespace velo {
   };
 
   // Standardised input of one record, feature i (0 beyond the 12 features or the batch).
-  __device__ __forceinline__ float train_input(const MlpModelDevice& m, const DoubletRecord* r, bool valid, unsigned i)
+  __device__ __forceinline__ float train_input(const MlpModelDevice& m, const SeedRecord* r, bool valid, unsigned i)
   {
     if (!valid || i >= mlp_features) return 0.0f;
     return fminf(fmaxf((__ldg(&r->f[i]) - __ldg(&m.mean[i])) * __ldg(&m.inv_std[i]), -8.0f), 8.0f);
@@ -126,8 +126,8 @@ namespace velo {
     for (unsigned t = blockIdx.x * warps + (threadIdx.x >> 5); t < n_tiles; t += gridDim.x * warps) {
       const unsigned r0 = 16 * t + g, r1 = r0 + 8;
       const bool v0 = r0 < p.batch, v1 = r1 < p.batch;
-      const DoubletRecord* rec0 = p.records + p.first + (v0 ? r0 : 0);
-      const DoubletRecord* rec1 = p.records + p.first + (v1 ? r1 : 0);
+      const SeedRecord* rec0 = p.records + p.first + (v0 ? r0 : 0);
+      const SeedRecord* rec1 = p.records + p.first + (v1 ? r1 : 0);
       uint32_t x[4];
       x[0] = pack_bf16(train_input(m, rec0, v0, 2 * c), train_input(m, rec0, v0, 2 * c + 1));
       x[1] = pack_bf16(train_input(m, rec1, v1, 2 * c), train_input(m, rec1, v1, 2 * c + 1));
@@ -144,7 +144,7 @@ namespace velo {
       float dz[2] = {0.0f, 0.0f};
       const float zs[2] = {z0, z1};
       const bool vs[2] = {v0, v1};
-      const DoubletRecord* rs[2] = {rec0, rec1};
+      const SeedRecord* rs[2] = {rec0, rec1};
 #pragma unroll
       for (unsigned q = 0; q < 2; ++q) {
         if (!vs[q]) continue;
@@ -310,7 +310,7 @@ namespace velo {
   }
 
   __global__ void __launch_bounds__(256) mlp_score_kernel(
-    const DoubletRecord* records, unsigned long long n, const MlpModelDevice* model, float* logits)
+    const SeedRecord* records, unsigned long long n, const MlpModelDevice* model, float* logits)
   {
     const unsigned lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
     const unsigned long long n_tiles = (n + 15) / 16;
@@ -318,8 +318,8 @@ namespace velo {
     for (unsigned long long t = blockIdx.x * 8ull + (threadIdx.x >> 5); t < n_tiles; t += gridDim.x * 8ull) {
       const unsigned long long r0 = 16 * t + g, r1 = r0 + 8;
       const bool v0 = r0 < n, v1 = r1 < n;
-      const DoubletRecord* rec0 = records + (v0 ? r0 : 0);
-      const DoubletRecord* rec1 = records + (v1 ? r1 : 0);
+      const SeedRecord* rec0 = records + (v0 ? r0 : 0);
+      const SeedRecord* rec1 = records + (v1 ? r1 : 0);
       uint32_t x[4];
       x[0] = pack_bf16(train_input(m, rec0, v0, 2 * c), train_input(m, rec0, v0, 2 * c + 1));
       x[1] = pack_bf16(train_input(m, rec1, v1, 2 * c), train_input(m, rec1, v1, 2 * c + 1));
@@ -365,10 +365,10 @@ namespace {
   } while (0)
 
   VeloStatus accumulate(
-    VeloSeedTrainer* t, const VeloDoubletRecord* records, unsigned long long first, unsigned batch, cudaStream_t s)
+    VeloSeedTrainer* t, const VeloSeedRecord* records, unsigned long long first, unsigned batch, cudaStream_t s)
   {
     velo::TrainParams p;
-    p.records = reinterpret_cast<const velo::DoubletRecord*>(records);
+    p.records = reinterpret_cast<const velo::SeedRecord*>(records);
     p.first = first;
     p.batch = batch;
     p.inv_batch = 1.0f / float(batch);
@@ -385,7 +385,7 @@ namespace {
   }
 } // namespace
 
-static_assert(sizeof(VeloDoubletRecord) == sizeof(velo::DoubletRecord), "record layout");
+static_assert(sizeof(VeloSeedRecord) == sizeof(velo::SeedRecord), "record layout");
 
 VeloStatus velo_seed_trainer_create(const VeloSeedModel* init, float learning_rate, float pos_weight, VeloSeedTrainer** out)
 {
@@ -425,7 +425,7 @@ VeloStatus velo_seed_trainer_create(const VeloSeedModel* init, float learning_ra
 }
 
 VeloStatus velo_seed_trainer_step(
-  VeloSeedTrainer* t, const VeloDoubletRecord* records, unsigned long long first, unsigned batch, VeloStream stream, float* loss)
+  VeloSeedTrainer* t, const VeloSeedRecord* records, unsigned long long first, unsigned batch, VeloStream stream, float* loss)
 {
   if (!t || !records || batch == 0) return fail(VELO_ERR_ARGUMENT, "bad argument");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -447,7 +447,7 @@ VeloStatus velo_seed_trainer_step(
 
 VeloStatus velo_seed_trainer_gradients(
   VeloSeedTrainer* t,
-  const VeloDoubletRecord* records,
+  const VeloSeedRecord* records,
   unsigned long long first,
   unsigned batch,
   VeloStream stream,
@@ -467,14 +467,14 @@ VeloStatus velo_seed_trainer_gradients(
 }
 
 VeloStatus velo_seed_trainer_score(
-  VeloSeedTrainer* t, const VeloDoubletRecord* records, unsigned long long n, float* logits, VeloStream stream)
+  VeloSeedTrainer* t, const VeloSeedRecord* records, unsigned long long n, float* logits, VeloStream stream)
 {
   if (!t || !records || !logits) return fail(VELO_ERR_ARGUMENT, "bad argument");
   if (n == 0) return VELO_OK;
   const unsigned long long tiles = (n + 15) / 16;
   const unsigned grid = unsigned(std::min<unsigned long long>((tiles + 7) / 8, unsigned(t->sm_count) * 8ull));
   velo::mlp_score_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-    reinterpret_cast<const velo::DoubletRecord*>(records), n, t->model, logits);
+    reinterpret_cast<const velo::SeedRecord*>(records), n, t->model, logits);
   VELO_TRY(cudaGetLastError());
   return VELO_OK;
 }

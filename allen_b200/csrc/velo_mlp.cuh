@@ -1,12 +1,13 @@
-// Learned seed pruner of the triplet search: doublet features, the device copy of the
-// 12-32-32-1 network and the warp-level tensor-core building blocks (mma.sync m16n8k16,
-// bf16 operands, fp32 accumulators; ldmatrix and movmatrix for fragment layouts).
+// Learned seed gate of the triplet search: the device copy of the 12-32-32-1 network and the
+// warp-level tensor-core building blocks (mma.sync m16n8k16, bf16 operands, fp32
+// accumulators; ldmatrix and movmatrix for fragment layouts).  The features are in
+// velo_gate.cu.
 //
 // No counterpart in the reference: the reference's seeding (SearchByTriplet.cu:298-446)
-// scans the h2 window of every (h0, h1) doublet among the n_candidates nearest unused h0.
-// The network scores each doublet before that scan; doublets below the threshold are not
-// scanned.  It is trained on the plain search's own choices (label 1 = the doublet the
-// plain seeding turned into a seed).
+// searches every unused hit of the module pair as the middle hit h1 of a seed.  The network
+// scores each seed candidate h1 from its neighbours before the search; candidates below the
+// threshold are not searched.  It is trained on the plain search's own outcomes (label 1 =
+// the plain seeding made a seed with this h1).
 //
 // Fragment layouts (PTX ISA, mma.m16n8k16 with .bf16): lane = 4 g + c.
 //   A (16 x 16, row-major): a0 = A[g][2c..2c+1], a1 = A[g+8][2c..], a2 = A[g][2c+8..],
@@ -41,8 +42,8 @@ namespace velo {
     float b3;
     float mean[mlp_features];
     float inv_std[mlp_features];
-    float threshold_logit;                    // keep a doublet when its logit > threshold
-    float kept_lo, kept_hi;                   // per-event bounds of kept / found doublets
+    float threshold_logit;                    // search a seed candidate when its logit > threshold
+    float kept_lo, kept_hi;                   // per-event bounds of kept / all seed candidates
   };
 
   // Host: a model (flat parameters w1, b1, w2, b2, w3, b3 and meta's standardisation,
@@ -50,12 +51,12 @@ namespace velo {
   void make_model_device(const float* params, const VeloSeedModel& meta, MlpModelDevice& d);
   void model_params(const VeloSeedModel& m, float* params);
 
-  // One training example, written by the search in recording mode (64 bytes).
-  struct DoubletRecord {
+  // One training example, written by the seed gate in recording mode (64 bytes).
+  struct SeedRecord {
     float f[mlp_features]; // raw features (before standardisation)
-    float label;           // 1 if the plain seeding chose this doublet
+    float label;           // 1 if the plain seeding made a seed with this middle hit
     uint32_t event;        // event index in the slice
-    uint32_t h0, h1;       // hit indices in the sorted container
+    uint32_t h0, h1;       // h0: 0xFFFFFFFF (the candidate is h1 alone); h1: index in the sorted container
   };
 
   __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
@@ -90,40 +91,6 @@ namespace velo {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
                  : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
                  : "r"(addr));
-  }
-
-  // Features of the doublet (h0 on the module pair already searched, h1 on the current one).
-  // All in fp32 with correctly rounded division and square root, so the host restatement
-  // reproduces them bit for bit:
-  //   0 tx, 1 ty (slopes), 2 |t|, 3 signed distance of the line to the beam axis,
-  //   4 z of its closest approach, 5 phi(h1) - phi(h0) (rad / pi), 6 r(h1),
-  //   7 dr/dz, 8 |dz| (module gap), 9 candidate rank, 10 candidates of h1, 11 phi(h1) (rad / pi).
-  __device__ __forceinline__ void doublet_features(
-    float x0, float y0, float z0, int16_t phi0, float x1, float y1, float z1, int16_t phi1, unsigned rank,
-    unsigned found, float (&f)[mlp_features])
-  {
-    const float dz = z1 - z0;
-    const float inv = __fdiv_rn(1.0f, dz);
-    const float tx = (x1 - x0) * inv;
-    const float ty = (y1 - y0) * inv;
-    const float t2 = tx * tx + ty * ty;
-    const float t = __fsqrt_rn(t2);
-    const float doca = __fdiv_rn(x1 * ty - y1 * tx, fmaxf(t, 1e-6f));
-    const float zpoca = z1 - __fdiv_rn(x1 * tx + y1 * ty, fmaxf(t2, 1e-12f));
-    const float r0 = __fsqrt_rn(x0 * x0 + y0 * y0);
-    const float r1 = __fsqrt_rn(x1 * x1 + y1 * y1);
-    f[0] = tx;
-    f[1] = ty;
-    f[2] = t;
-    f[3] = doca;
-    f[4] = zpoca;
-    f[5] = static_cast<float>(static_cast<int16_t>(phi1 - phi0)) * 3.0517578125e-05f;
-    f[6] = r1;
-    f[7] = (r1 - r0) * inv;
-    f[8] = fabsf(dz);
-    f[9] = static_cast<float>(rank);
-    f[10] = static_cast<float>(found);
-    f[11] = static_cast<float>(phi1) * 3.0517578125e-05f;
   }
 
   // Standardised, clamped to [-8, 8] and rounded to bf16 pairs: word w holds inputs 2w, 2w+1.

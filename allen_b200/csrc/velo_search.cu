@@ -35,7 +35,6 @@ namespace velo {
   constexpr unsigned skipped_shift = 60;
   constexpr uint64_t track_number_mask64 = 0x0FFFFFFFull;
   constexpr unsigned max_tail_tracks = 512; // tracks whose tail lives in shared memory (the others: their container)
-  constexpr unsigned n_buckets = 128;
   constexpr uint8_t flag_used = 1;
   constexpr uint8_t flag_odd_module = 2;
   constexpr unsigned flat_slots = 1024; // (h1, h0 candidate) slots per chunk of the flat seeding
@@ -56,8 +55,7 @@ namespace velo {
   };
 
   // Shared state of the flat seeding variant: one slot per (h1, candidate order).
-  // SLOTS doublets per chunk; MLP adds the seed pruner's staging rows (learned kernel).
-  template<unsigned SLOTS, bool MLP>
+  template<unsigned SLOTS>
   struct SearchSharedFlatT : SearchShared {
     static constexpr unsigned slots = SLOTS;
     // (h0, h1) doublets of a chunk, packed by pack_doublet(), then overwritten in place
@@ -66,24 +64,20 @@ namespace velo {
       uint32_t doublet;
       float fit;
     } slot[SLOTS];
-    union alignas(16) { // ldmatrix reads 16-byte rows of mlp_rows
-      uint16_t res_h2[SLOTS];
-      uint32_t mlp_rows[MLP ? 8 : 1][16][8]; // per warp: 16 doublets x 16 bf16 inputs (learned mode)
-    };
+    uint16_t res_h2[SLOTS];
+    uint16_t cand_list[SLOTS]; // the window's searched candidates (index in the window), h1 order
   };
-  using SearchSharedFlat = SearchSharedFlatT<flat_slots, true>;
-  // plain flat-seeding kernels: 512 slots for 128 threads (chunks of 64 or 128 h1), which with
-  // the ring in global scratch leaves room for twelve CTAs per SM
+  // flat-seeding kernels: 512 slots for 128 threads (chunks of 64 or 128 h1), which with the
+  // ring in global scratch leaves room for twelve CTAs per SM
   template<unsigned THREADS>
   using SearchSharedFlatPlain =
-    SearchSharedFlatT<(THREADS <= 64 ? flat_slots / 4 : (THREADS <= 128 ? flat_slots / 2 : flat_slots)), false>;
+    SearchSharedFlatT<(THREADS <= 64 ? flat_slots / 4 : (THREADS <= 128 ? flat_slots / 2 : flat_slots))>;
 
-  // Packed doublet: h0 | h1 index in the chunk << 16 | rank << 25 | (found - 1) << 28 | keep << 31
+  // Packed doublet: h0 | h1 index in the chunk << 16 | rank << 25 | (found - 1) << 28
   __device__ __forceinline__ uint32_t pack_doublet(unsigned h0, unsigned h1_local, unsigned rank, unsigned found)
   {
     return h0 | (h1_local << 16) | (rank << 25) | ((found - 1u) << 28);
   }
-  constexpr uint32_t doublet_keep = 1u << 31;
 
   struct HitsSoA {
     const float* x;
@@ -101,8 +95,8 @@ namespace velo {
     unsigned local_hits; // atomics::local_number_of_hits
     unsigned n_tracks;   // dev_number_of_velo_tracks
     unsigned scan_parity;
-    unsigned doublets;   // (h0, h1) doublets formed by the flat seeding
-    unsigned kept;       // doublets whose h2 window was scanned
+    unsigned candidates; // unused h1 met by the seeding (seed candidates)
+    unsigned searched;   // candidates whose h0 and h2 windows were searched (the gate let through)
   };
 
   // Block-wide exclusive scan with a single barrier: warp totals go to one of two
@@ -130,17 +124,6 @@ namespace velo {
     return before + incl - v;
   }
 
-  __device__ __forceinline__ unsigned bucket_of(int16_t v) { return static_cast<unsigned>(v + 32768) >> 9; }
-
-  // binary_search_leftmost (BinarySearch.cuh:15-30) through the bucket table of the
-  // module pair: the first index with phi >= value.
-  __device__ __forceinline__ int leftmost(const uint16_t* table, const int16_t* phis, unsigned n, int16_t value)
-  {
-    unsigned i = table[bucket_of(value)];
-    while (i < n && phis[i] < value)
-      ++i;
-    return static_cast<int>(i);
-  }
 
   __device__ __forceinline__ bool phi_outside(int16_t phi, int16_t extrapolated, int16_t tol)
   {
@@ -298,57 +281,18 @@ namespace velo {
     return static_cast<unsigned>((c < 4 ? lo >> (16 * c) : hi >> (16 * (c - 4))) & 0xFFFFu);
   }
 
-  // Learned mode: scores the n doublets of the list with the network and sets the keep bit
-  // of those above the threshold.  Warps 0..7 take 16-doublet tiles; lanes 0..15 compute one
-  // doublet's inputs each into the warp's staging rows, ldmatrix forms the A fragment.
-  __device__ __forceinline__ void score_doublets(
-    SearchSharedFlat& s, const MlpModelDevice* m, const HitsSoA& h, unsigned h1_base, unsigned n)
-  {
-    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const unsigned n_warps = min(blockDim.x >> 5, 8u);
-    if (warp >= n_warps) return;
-    uint32_t(*rows)[8] = s.mlp_rows[warp];
-    for (unsigned t = warp; 16 * t < n; t += n_warps) {
-      if (lane < 16) {
-        const unsigned q = 16 * t + lane;
-        uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (q < n) {
-          const uint32_t d = s.slot[q].doublet;
-          const unsigned h0 = d & 0xFFFFu, h1 = h1_base + ((d >> 16) & 0x1FFu);
-          float f[mlp_features];
-          doublet_features(h.x[h0], h.y[h0], h.z[h0], h.phi[h0], h.x[h1], h.y[h1], h.z[h1], h.phi[h1], (d >> 25) & 7u,
-                           ((d >> 28) & 7u) + 1u, f);
-          standardise_pairs(*m, f, w);
-        }
-#pragma unroll
-        for (unsigned i = 0; i < 8; ++i)
-          rows[lane][i] = w[i];
-      }
-      __syncwarp();
-      uint32_t a[4];
-      ldmatrix_x4(a, &rows[lane & 15u][(lane >> 4) * 4]);
-      float lg, lg8;
-      mlp_forward_tile(m, a, lg, lg8);
-      if ((lane & 3u) == 0) {
-        const float thr = __ldg(&m->threshold_logit);
-        const unsigned q0 = 16 * t + (lane >> 2), q1 = q0 + 8;
-        if (q0 < n && lg > thr) s.slot[q0].doublet |= doublet_keep;
-        if (q1 < n && lg8 > thr) s.slot[q1].doublet |= doublet_keep;
-      }
-      __syncwarp();
-    }
-  }
-
-  // Seeding with the candidates flattened (SearchByTriplet.cu:298-446).  Phase A, one
-  // thread per h1, walks the pendulum and keeps its first n_candidates unused h0 in
-  // registers; a block scan packs all (h0, h1) doublets of the chunk into one list.
+  // Seeding with the candidates flattened (SearchByTriplet.cu:298-446).  The window's unused
+  // h1 are first compacted to threads 0, 1, ... in h1 order.  Phase A, one thread per h1,
+  // walks the pendulum and keeps its first n_candidates unused h0 in registers; a block scan
+  // packs all (h0, h1) doublets of the chunk into one list.
   // Phase B, one thread per doublet, extrapolates and scans the h2 window.  Phase C, one
   // thread per h1, keeps the first strictly best of its doublets in candidate order (the
   // reference's sequential choice) and queues the seed in h1 order.  Phase B runs the same
   // path on every lane and has no idle slots for h1 with fewer than n_candidates doublets.
-  // LEARNED kernels can also score the doublets with the seed pruner (only kept doublets
-  // reach phase B) and record training doublets.
-  template<bool LEARNED, typename Flat>
+  // GATED kernels take the learned seed gate (gate, event-relative, or null): an unused h1
+  // whose gate byte is 0 is not searched; and, for training, record each unused h1's
+  // outcome (outcome: 1 no seed, 2 seed; null = off).
+  template<bool GATED, typename Flat>
   __device__ __forceinline__ void seeding_flat(
     Flat& s,
     uint64_t* ring,
@@ -357,10 +301,8 @@ namespace velo {
     const HitsSoA& h,
     const ModulePair* md,
     unsigned n_candidates,
-    const SearchParams& p,
-    bool learned,
-    unsigned event,
-    unsigned hit_offset)
+    const uint8_t* gate,
+    uint8_t* outcome)
   {
     const ModulePair prev = md[0], cur = md[1], next = md[2];
     const unsigned per_chunk = min(blockDim.x, Flat::slots / n_candidates);
@@ -368,12 +310,39 @@ namespace velo {
     const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
     for (unsigned c0 = 0; c0 < cur.hit_num; c0 += per_chunk) {
       const unsigned n_h1 = min(per_chunk, cur.hit_num - c0);
+      // Gated: the window's candidates compacted in h1 order (its unused hits that the gate
+      // lets through, one per thread from thread 0 on), so that the phases below run on as
+      // few warps as there are candidates.  Plain: thread i takes the window's hit i (the
+      // compaction's scan and barrier cost the plain search more than they save).
+      bool searched;
+      unsigned hl;
+      if constexpr (GATED) {
+        unsigned n_searched;
+        {
+          const unsigned hw = cur.hit_start + c0 + threadIdx.x;
+          const bool valid = threadIdx.x < n_h1 && !(h.flags[hw] & flag_used);
+          const bool pass = valid && (gate == nullptr || gate[hw] != 0);
+          unsigned total;
+          const unsigned excl = scan1(s, cnt, (pass ? 1u : 0u) | ((valid ? 1u : 0u) << 16), total);
+          if (pass) s.cand_list[excl & 0xFFFFu] = static_cast<uint16_t>(threadIdx.x);
+          n_searched = total & 0xFFFFu;
+          cnt.local_hits += total >> 16;
+          cnt.candidates += total >> 16;
+          cnt.searched += n_searched;
+        }
+        __syncthreads();
+        searched = threadIdx.x < n_searched;
+        hl = searched ? s.cand_list[threadIdx.x] : 0u;
+      }
+      else {
+        hl = threadIdx.x;
+        searched = threadIdx.x < n_h1 && !(h.flags[cur.hit_start + c0 + hl] & flag_used);
+      }
+      const unsigned h1 = cur.hit_start + c0 + hl;
       // Phase A: candidates c < 4 in the 16-bit fields of cand_lo, 4..7 in cand_hi
-      const unsigned h1 = cur.hit_start + c0 + threadIdx.x;
-      const bool valid = threadIdx.x < n_h1 && !(h.flags[h1] & flag_used);
       uint64_t cand_lo = 0, cand_hi = 0;
       unsigned found = 0;
-      if (valid) {
+      if (searched) {
         const int p0 = leftmost(s.bucket[prev.mp], h.phi + prev.hit_start, prev.hit_num, h.phi[h1]);
         int pos = p0;
         for (unsigned i = 0; i < prev.hit_num && found < n_candidates; ++i) {
@@ -388,28 +357,12 @@ namespace velo {
         }
       }
       unsigned n_doublets;
-      unsigned first = scan1(s, cnt, found, n_doublets);
+      const unsigned first = scan1(s, cnt, found, n_doublets);
       for (unsigned c = 0; c < found; ++c)
-        s.slot[first + c].doublet = pack_doublet(candidate_h0(cand_lo, cand_hi, c), threadIdx.x, c, found);
+        s.slot[first + c].doublet = pack_doublet(candidate_h0(cand_lo, cand_hi, c), hl, c, found);
       __syncthreads();
-      cnt.doublets += n_doublets;
-      // keep_mask bit c: the h2 window of doublet c is scanned (always, in the plain search)
-      unsigned keep_mask = (1u << found) - 1u;
-      if constexpr (LEARNED) if (learned) {
-        score_doublets(s, p.seed_model, h, cur.hit_start + c0, n_doublets);
-        __syncthreads();
-        keep_mask = 0;
-        for (unsigned c = 0; c < found; ++c)
-          keep_mask |= (s.slot[first + c].doublet >> 31) << c;
-        // pack the kept doublets (reads above, writes after the scan's barrier)
-        first = scan1(s, cnt, __popc(keep_mask), n_doublets);
-        unsigned at = first;
-        for (unsigned c = 0; c < found; ++c)
-          if (keep_mask & (1u << c))
-            s.slot[at++].doublet = pack_doublet(candidate_h0(cand_lo, cand_hi, c), threadIdx.x, c, found);
-        __syncthreads();
-      }
-      cnt.kept += n_doublets;
+      // keep_mask bit c: doublet c's slot in the packed list (every doublet is scanned)
+      const unsigned keep_mask = (1u << found) - 1u;
       // Phase B
       for (unsigned q = threadIdx.x; q < n_doublets; q += blockDim.x) {
         const uint32_t d = s.slot[q].doublet;
@@ -448,7 +401,7 @@ namespace velo {
       // Phase C
       bool ok = false;
       unsigned best_h0 = 0, best_h2 = 0, best_c = 0xFFFFFFFFu;
-      if (valid) {
+      if (searched) {
         float best_fit = k.max_scatter;
         unsigned at = first;
         for (unsigned c = 0; c < found; ++c) {
@@ -463,31 +416,21 @@ namespace velo {
           ++at;
         }
         ok = best_fit < k.max_scatter;
-        // training doublets: every candidate of one h1 in record_every, labelled by the choice
-        if (LEARNED && p.records != nullptr && found > 0 &&
-            ((event * 0x9E3779B1u) ^ ((hit_offset + h1) * 0x85EBCA77u)) % p.record_every == 0) {
-          const unsigned slot0 = atomicAdd(p.record_count, found);
-          for (unsigned c = 0; c < found && slot0 + found <= p.record_capacity; ++c) {
-            const unsigned h0 = candidate_h0(cand_lo, cand_hi, c);
-            DoubletRecord r;
-            doublet_features(h.x[h0], h.y[h0], h.z[h0], h.phi[h0], h.x[h1], h.y[h1], h.z[h1], h.phi[h1], c, found, r.f);
-            r.label = (ok && c == best_c) ? 1.0f : 0.0f;
-            r.event = event;
-            r.h0 = hit_offset + h0;
-            r.h1 = hit_offset + h1;
-            p.records[slot0 + c] = r;
-          }
-        }
+        if (GATED && outcome != nullptr) outcome[h1] = ok ? 2 : 1;
       }
       unsigned total;
-      const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | ((valid ? 1u : 0u) << 16), total);
+      const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | ((!GATED && searched ? 1u : 0u) << 16), total);
       if (ok) {
         const unsigned tn = (cnt.ttf + (excl & 0xFFFFu)) % max_tracks_to_follow;
         ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
                      (uint64_t(best_h2 & 0xFFFFu) << 32);
       }
       cnt.ttf += total & 0xFFFFu;
-      cnt.local_hits += total >> 16;
+      if constexpr (!GATED) {
+        cnt.local_hits += total >> 16;
+        cnt.candidates += total >> 16;
+        cnt.searched += total >> 16;
+      }
     }
   }
 
@@ -698,7 +641,7 @@ namespace velo {
   // Seeding, forwarding and the tail of one event over staged hits (hit_used clear):
   // SearchByTriplet.cu:165-264.  Returns the event's counters; the track containers hold
   // its tracks and three-hit tracks.
-  template<unsigned LPH, bool LEARNED, typename Shared>
+  template<unsigned LPH, bool GATED, typename Shared>
   __device__ __forceinline__ Counters search_pass(
     const SearchParams& p,
     Shared& s,
@@ -708,11 +651,11 @@ namespace velo {
     const unsigned* start,
     const unsigned* num,
     unsigned hit_offset,
-    unsigned e,
     TrackHits* tracks,
     unsigned track_limit,
     TrackletHits* three_hit,
-    bool learned)
+    const uint8_t* gate,
+    uint8_t* outcome)
   {
     if (threadIdx.x == 0) s.track_hits = 0;
     Counters cnt {0, 0, 0, 0, 0, 0, 0};
@@ -722,7 +665,7 @@ namespace velo {
     module_pairs(md, p.geo, first, start, num, hit_offset);
     __syncthreads(); // bucket tables
 
-    if constexpr (LPH == 0) seeding_flat<LEARNED>(s, ring, cnt, k, h, md, 8, p, learned, e, hit_offset);
+    if constexpr (LPH == 0) seeding_flat<GATED>(s, ring, cnt, k, h, md, 8, gate, outcome);
     else seeding<LPH>(s, ring, cnt, k, h, md, 8);
 
     unsigned last_ttf = 0;
@@ -739,7 +682,9 @@ namespace velo {
       // not read yet, an order-dependent outcome this kernel does not reproduce.
       if (threadIdx.x == 0 && cnt.ttf - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       __syncthreads(); // hit_used flags written by forwarding
-      if constexpr (LPH == 0) seeding_flat<LEARNED>(s, ring, cnt, k, h, md, 4, p, learned, e, hit_offset);
+      if constexpr (LPH == 0)
+        seeding_flat<GATED>(s, ring, cnt, k, h, md, GATED && gate != nullptr && p.seed_window ? p.seed_window : 4u, gate,
+                            outcome);
       else seeding<LPH>(s, ring, cnt, k, h, md, 4);
       if (threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       --first;
@@ -779,7 +724,7 @@ namespace velo {
     return cnt;
   }
 
-  template<unsigned LPH, bool SMEM, bool LEARNED, typename Shared>
+  template<unsigned LPH, bool SMEM, bool GATED, typename Shared>
   __device__ __forceinline__ void
   search_event(const SearchParams& p, Shared& s, uint64_t* ring, unsigned char* dsmem, unsigned e)
   {
@@ -830,39 +775,29 @@ namespace velo {
       }
     }
     const HitsSoA h {xs, ys, zs, phis, flags};
-    // bucket tables: bucket[mp][b] = first index of the module pair with phi >= b * 512 - 32768
-    for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
-      const unsigned s0 = start[mp] - hit_offset;
-      const unsigned cnt = num[mp];
-      uint16_t* table = s.bucket[mp];
-      for (unsigned i = threadIdx.x; i <= cnt; i += blockDim.x) {
-        const unsigned lo = i == 0 ? 0u : bucket_of(phis[s0 + i - 1]) + 1;
-        const unsigned hi = i == cnt ? n_buckets : bucket_of(phis[s0 + i]);
-        for (unsigned b = lo; b <= hi; ++b)
-          table[b] = static_cast<uint16_t>(i);
-      }
-    }
+    build_bucket_tables(s.bucket, phis, start, num, hit_offset);
 
-    // Learned mode: the pruned search first; an event whose fraction of kept doublets falls
-    // outside the model's bounds is searched again by the plain search, from scratch.
-    const bool learned = LEARNED && p.seed_model != nullptr;
-    Counters cnt =
-      search_pass<LPH, LEARNED>(p, s, ring, k, h, start, num, hit_offset, e, tracks, track_limit, three_hit, learned);
-    unsigned mode = learned ? seed_mode_learned : seed_mode_plain;
-    const unsigned doublets = cnt.doublets, kept = cnt.kept;
-    if (learned && doublets > 0) {
-      const float frac = __fdiv_rn(__uint2float_rn(kept), __uint2float_rn(doublets));
-      if (frac < __ldg(&p.seed_model->kept_lo) || frac > __ldg(&p.seed_model->kept_hi)) {
+    // Learned mode: the gate of the event's seed candidates, unless the fraction it lets
+    // through falls outside the model's bounds, in which case the plain search runs
+    unsigned mode = seed_mode_plain;
+    const uint8_t* gate = nullptr;
+    if (GATED && p.seed_gate != nullptr) {
+      const unsigned cand = p.gate_stats[2 * e], kept = p.gate_stats[2 * e + 1];
+      const float frac = cand > 0 ? __fdiv_rn(__uint2float_rn(kept), __uint2float_rn(cand)) : 1.0f;
+      if (frac >= p.kept_lo && frac <= p.kept_hi) {
+        gate = p.seed_gate + hit_offset;
+        mode = seed_mode_learned;
+      }
+      else {
         mode = seed_mode_fallback;
-        __syncthreads();
-        for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x)
-          flags[i] &= static_cast<uint8_t>(~flag_used);
-        cnt = search_pass<LPH, LEARNED>(p, s, ring, k, h, start, num, hit_offset, e, tracks, track_limit, three_hit, false);
       }
     }
+    uint8_t* outcome = GATED && p.h1_outcome != nullptr ? p.h1_outcome + hit_offset : nullptr;
+    Counters cnt =
+      search_pass<LPH, GATED>(p, s, ring, k, h, start, num, hit_offset, tracks, track_limit, three_hit, gate, outcome);
     if (p.seed_stats != nullptr && threadIdx.x == 0) {
-      p.seed_stats[3 * e] = doublets;
-      p.seed_stats[3 * e + 1] = kept;
+      p.seed_stats[3 * e] = cnt.candidates;
+      p.seed_stats[3 * e + 1] = cnt.searched;
       p.seed_stats[3 * e + 2] = mode;
     }
 
@@ -933,14 +868,14 @@ namespace velo {
     });
   }
 
-  // The learned search (flat seeding with the seed pruner; with seed_model null, the plain
-  // search, recording training doublets when asked) is a kernel of its own, so the plain
-  // kernels keep their register budget.
+  // The learned search: flat seeding behind the seed gate (with seed_gate null, the plain
+  // search, recording each seed candidate's outcome when h1_outcome is set).  The gate costs
+  // one byte read per candidate, so this kernel keeps the plain kernel's register budget.
   template<unsigned THREADS, unsigned RING>
-  __global__ void __launch_bounds__(THREADS, 1024 / THREADS) search_by_triplet_learned_kernel(SearchParams p)
+  __global__ void __launch_bounds__(THREADS, 1536 / THREADS) search_by_triplet_gated_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
-    __shared__ SearchSharedFlat s;
+    __shared__ SearchSharedFlatPlain<THREADS> s;
     __shared__ uint64_t ring_smem[RING ? 1 : max_tracks_to_follow];
     uint64_t* ring = RING ? p.ring_scratch + size_t(blockIdx.x) * max_tracks_to_follow : ring_smem;
     for_each_event(p.queue, p.n_events, [&](unsigned e, unsigned) {
@@ -955,10 +890,8 @@ namespace velo {
   template __global__ void search_by_triplet_kernel<T, L, R>(SearchParams p);
   VELO_SEARCH_CONFIGS(VELO_SEARCH_CONFIG)
 #undef VELO_SEARCH_CONFIG
-  template __global__ void search_by_triplet_learned_kernel<128, 0>(SearchParams p);
-  template __global__ void search_by_triplet_learned_kernel<256, 0>(SearchParams p);
-  template __global__ void search_by_triplet_learned_kernel<512, 0>(SearchParams p);
-  template __global__ void search_by_triplet_learned_kernel<128, 1>(SearchParams p);
-  template __global__ void search_by_triplet_learned_kernel<256, 1>(SearchParams p);
+#define VELO_GATED_CONFIG(T, R) template __global__ void search_by_triplet_gated_kernel<T, R>(SearchParams p);
+  VELO_GATED_CONFIGS(VELO_GATED_CONFIG)
+#undef VELO_GATED_CONFIG
 
 } // namespace velo

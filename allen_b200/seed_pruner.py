@@ -1,24 +1,27 @@
-"""Learned seed pruner of the triplet search: training data, GPU training, calibration.
+"""Learned seed gate of the triplet search: training data, GPU training, calibration.
 
 Workflow (all GPU work through the C ABI of libvelo_b200.so):
 
-1. ``collect``: the chain runs the plain search over generated slices and records the
-   (h0, h1) doublets of one h1 candidate in ``every`` with their 12 features and the plain
-   seeding's choice as label (velo_chain_record_doublets).
+1. ``collect``: the chain runs the plain search over generated slices and records one seed
+   candidate (a hit the seeding met unused as middle hit h1) in ``every``, with its 12
+   features and, as label, whether the plain seeding made a seed with it
+   (velo_chain_record_seeds).
 2. ``initial_model``: feature standardisation from a sample of the records, He-initialised
    weights from a seeded generator.
 3. ``train``: Adam steps of the tensor-core forward/backward kernels (velo_seed_trainer_step)
    over shuffled batches held in HBM.
-4. ``calibrate``: the logit threshold that keeps ``recall`` of the positive doublets of
-   held-out records, and the per-event bounds on the kept fraction beyond which an event is
-   searched again by the plain search.
+4. ``calibrate_threshold``: the logit threshold that keeps ``recall`` of the positive
+   candidates of held-out records; the per-event bounds on the kept fraction beyond which an
+   event is searched by the plain search instead come from held-out events.
 
-No counterpart in the reference (its seeding, SearchByTriplet.cu:298-446, scans every
-candidate doublet).
+No counterpart in the reference (its seeding, SearchByTriplet.cu:298-446, searches every
+unused hit as h1).
 """
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
 
 import numpy as np
 
@@ -68,6 +71,26 @@ def load(path: str) -> SeedModelC:
                              float(z["kept_hi"]))
 
 
+LEARNED_CONFIG = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "launch_config_learned.json")
+DEFAULT_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "seed_pruner.npz")
+
+
+def load_learned_config(path: str = LEARNED_CONFIG) -> dict:
+    """The launch configuration tuned for the learned mode (seed window, gated search kernel,
+    events per claim), for VeloChain.configure; empty when none was tuned."""
+    try:
+        with open(path) as f:
+            return dict(json.load(f)["config"])
+    except (OSError, KeyError, ValueError):
+        return {}
+
+
+def use_learned(chain: VeloChain, path: str = DEFAULT_MODEL, config_path: str = LEARNED_CONFIG):
+    """Switches a chain to learned mode with the committed model and its tuned configuration."""
+    chain.configure(**load_learned_config(config_path))
+    chain.set_seed_model(load(path))
+
+
 def he_params(seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     w1 = rng.normal(0, np.sqrt(2.0 / N_FEATURES), (HIDDEN, N_FEATURES))
@@ -86,23 +109,21 @@ def records_to_host(records, n: int) -> np.ndarray:
 
 
 def collect(chain: VeloChain, dev_slices, capacity: int, every: int = 1):
-    """Runs the plain search over the slices, recording training doublets.  Returns the
-    device tensor of records (uint8, 64 bytes each) and how many were written."""
+    """Runs the plain search over the slices, recording training candidates.  Returns the
+    device tensor of records (uint8, 64 bytes each), how many were written and how many counted."""
     import torch
     records = torch.empty(RECORD_BYTES * capacity, dtype=torch.uint8, device="cuda")
     count = torch.zeros(1, dtype=torch.int32, device="cuda")
     chain.set_seed_model(None)
-    chain.record_doublets(records, count, every)
+    chain.record_seeds(records, count, every)
     try:
         for d in dev_slices:
             chain.run(d, use_graph=False)
             chain.synchronize()
     finally:
-        chain.record_doublets(None, None)
+        chain.record_seeds(None, None)
     n = int(count.item())
-    # an h1 whose doublets would cross the capacity is not written, so past an overflow only
-    # the records below capacity - 8 are known to be complete
-    return records, n if n <= capacity else capacity - 8, n
+    return records, min(n, capacity), n
 
 
 def feature_stats(records, n: int, sample: int = 262144, seed: int = 0):
@@ -198,7 +219,7 @@ def train(trainer: Trainer, records, n: int, epochs: int = 2, batch: int = 65536
 
 
 def calibrate_threshold(trainer: Trainer, records, n: int, recall: float) -> tuple[float, dict]:
-    """Logit threshold that keeps `recall` of the positive doublets among records [0, n)."""
+    """Logit threshold that keeps `recall` of the positive candidates among records [0, n)."""
     logits = trainer.score(records, n).cpu().numpy()
     labels = records_to_host(records, n)["label"]
     pos = np.sort(logits[labels > 0.5])
@@ -207,7 +228,7 @@ def calibrate_threshold(trainer: Trainer, records, n: int, recall: float) -> tup
     k = int(np.floor((1.0 - recall) * pos.size))
     thr = float(np.nextafter(pos[k], np.float32(-np.inf))) if k < pos.size else float(pos[-1])
     kept = logits > thr
-    stats = {"positives": int(pos.size), "doublets": int(n), "recall": float(np.mean(pos > thr)),
+    stats = {"positives": int(pos.size), "candidates": int(n), "recall": float(np.mean(pos > thr)),
              "kept_fraction": float(kept.mean()),
              "precision": float(np.mean(labels[kept] > 0.5)) if kept.any() else 0.0}
     return thr, stats
@@ -215,7 +236,7 @@ def calibrate_threshold(trainer: Trainer, records, n: int, recall: float) -> tup
 
 def collect_generated(chain: VeloChain, n_events: int, slice_events: int, seed: int, every: int, capacity: int, **gen):
     """Generates n_events events (stream `seed`) slice by slice and records their training
-    doublets from the plain search.  Returns (records, n, n_total_counted)."""
+    candidates from the plain search.  Returns (records, n, n_total_counted)."""
     import torch
     from . import generator
     from .chain import upload
@@ -223,7 +244,7 @@ def collect_generated(chain: VeloChain, n_events: int, slice_events: int, seed: 
     records = torch.empty(RECORD_BYTES * capacity, dtype=torch.uint8, device="cuda")
     count = torch.zeros(1, dtype=torch.int32, device="cuda")
     chain.set_seed_model(None)
-    chain.record_doublets(records, count, every)
+    chain.record_seeds(records, count, every)
     try:
         for first in range(0, n_events, slice_events):
             s = generator.generate(min(slice_events, n_events - first), seed=seed, first_event=first, **gen).raw
@@ -231,9 +252,9 @@ def collect_generated(chain: VeloChain, n_events: int, slice_events: int, seed: 
             chain.run(upload(s), use_graph=False)
             chain.synchronize()
     finally:
-        chain.record_doublets(None, None)
+        chain.record_seeds(None, None)
     n = int(count.item())
-    return records, n if n <= capacity else capacity - 8, n
+    return records, min(n, capacity), n
 
 
 def measure(chain: VeloChain, dev_slices, repeats: int = 3) -> float:
@@ -253,16 +274,16 @@ def measure(chain: VeloChain, dev_slices, repeats: int = 3) -> float:
 
 
 def quality(chain: VeloChain, gen) -> dict:
-    """Tracking efficiency, ghost and clone rates (TrackChecker rules) of one generated slice."""
+    """Tracking efficiency, ghost and clone rates (TrackChecker rules) of one generated slice,
+    counted on the device (velo_validate_tracks), with the seeding's candidate statistics."""
     from .chain import upload
-    from .validation import evaluate, tracks_from_outputs
+    from .validation import DeviceTruth, evaluate_device
     chain.reserve_for(gen.raw)
     chain.run(upload(gen.raw), use_graph=False)
-    totals = chain.synchronize()
-    out = chain.outputs_to_host(totals)
-    res = evaluate(gen, tracks_from_outputs(out))
+    chain.synchronize()
+    res = evaluate_device(chain, DeviceTruth(gen))
     st = chain.seed_stats(gen.raw.n_events)
-    res["doublets"] = int(st[:, 0].sum())
-    res["doublets_scanned"] = int(st[:, 1].sum())
+    res["candidates"] = int(st[:, 0].sum())
+    res["candidates_searched"] = int(st[:, 1].sum())
     res["fallback_events"] = int((st[:, 2] == 2).sum())
     return res

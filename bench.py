@@ -113,13 +113,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def generate_slices(n_events, slice_size, seed, pinned=False, **gen):
+def generate_events(n_events, slice_size, seed, **gen):
+    """Generated slices with their Monte Carlo truth (allen_b200.generator.Generated)."""
     from allen_b200 import generator
-    out = []
-    for first in range(0, n_events, slice_size):
-        n = min(slice_size, n_events - first)
-        out.append(generator.generate(n, seed=seed, first_event=first, **gen).raw)
-    return out
+    return [generator.generate(min(slice_size, n_events - first), seed=seed, first_event=first, **gen)
+            for first in range(0, n_events, slice_size)]
+
+
+def generate_slices(n_events, slice_size, seed, pinned=False, **gen):
+    return [g.raw for g in generate_events(n_events, slice_size, seed, **gen)]
 
 
 def pin(s):
@@ -272,7 +274,8 @@ def run_ours(args):
 
     geometry = _native.default_geometry()
     seed = rank_seed(args.seed, rank)
-    slices = generate_slices(args.events, args.slice, seed)
+    gens = generate_events(args.events, args.slice, seed)
+    slices = [g.raw for g in gens]
     dev = [upload(s) for s in slices]
     sp_max = max(int(super_pixels_per_event(s).sum()) for s in slices)
     chain = VeloChain(geometry)
@@ -377,41 +380,100 @@ def run_ours(args):
     chain_gbs = sum(chain_bytes(c["n"], c["raw_bytes"], c["H"], c["TH"], c["tracks_all"]) for c in counts) \
         * args.steps / (ms / 1e3) / 1e9
 
-    # the same workload in learned mode (the committed seed pruner), same timing rules
+    def timed(dev_list, use_graph=True):
+        def once():
+            for d in dev_list:
+                chain.run(d, use_graph=use_graph)
+        for _ in range(max(3, args.warmup)):
+            once()
+        torch.cuda.synchronize()
+        replicas.barrier()
+        t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for _ in range(args.steps):
+            once()
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(t_start.elapsed_time(t_end))
+
+    def stage_ms():
+        kt, kruns = chain.kernel_times()
+        return {k: v / max(kruns, 1) for k, v in kt.items()}
+
+    # The metric's comparison: learned + batched (the seed gate, persistent launches, CUDA graphs)
+    # against the plain search, both batched and as per-stage launches (one CTA per event, no
+    # graph), on the same events and timing rules; tracking quality of both modes over every
+    # event of the step, counted on the GPU against the generator's truth.
     learned = None
     if not args.no_learned:
         from allen_b200 import seed_pruner
-        model_path = os.path.join(REPO, "allen_b200", "data", "seed_pruner.npz")
-        chain.set_seed_model(seed_pruner.load(model_path))
-        for _ in range(max(3, args.warmup)):
-            step()
-        torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
-        l_start, l_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        l_start.record(stream)
-        for _ in range(args.steps):
-            step()
-        l_end.record(stream)
-        torch.cuda.synchronize()
-        l_ms = l_start.elapsed_time(l_end)
-        l_ms = max_over_ranks(l_ms)
-        doublets = scanned = fallback = 0
-        for s, d in zip(slices, dev):
-            chain.run(d, use_graph=True)
-            chain.synchronize(check=False)
-            st = chain.seed_stats(s.n_events)
-            doublets += int(st[:, 0].sum())
-            scanned += int(st[:, 1].sum())
-            fallback += int((st[:, 2] == 2).sum())
+        from allen_b200.validation import DeviceTruth, evaluate_device
+        plain_cfg = chain.get_config()
+        plain_stages = {k: v["ms_per_launch"] for k, v in per_kernel.items()}
+        truths = [DeviceTruth(g) for g in gens]
+
+        def quality():
+            tot = dict(tracks=0, ghosts=0, reconstructible=0, reconstructed=0, clones=0)
+            cand = searched = fallback = 0
+            for s_, d, t in zip(slices, dev, truths):
+                chain.run(d, use_graph=True)
+                chain.synchronize(check=False)
+                r = evaluate_device(chain, t)
+                for k in tot:
+                    tot[k] += r[k]
+                st = chain.seed_stats(s_.n_events)
+                cand += int(st[:, 0].sum())
+                searched += int(st[:, 1].sum())
+                fallback += int((st[:, 2] == 2).sum())
+            return {"efficiency": round(tot["reconstructed"] / max(tot["reconstructible"], 1), 6),
+                    "ghost_rate": round(tot["ghosts"] / max(tot["tracks"], 1), 6),
+                    "clone_rate": round(tot["clones"] / max(tot["reconstructed"] + tot["clones"], 1), 6),
+                    "tracks": tot["tracks"], "reconstructible": tot["reconstructible"],
+                    "candidates_searched_fraction": round(searched / max(cand, 1), 4),
+                    "fallback_event_fraction": round(fallback / max(events_step, 1), 6)}
+
+        q_plain = quality()
+        seed_pruner.use_learned(chain)
+        l_ms = timed(dev)
+        l_stages = stage_ms()
+        q_learned = quality()
+        l_value = aggregate_rate(world, events_step, args.steps, l_ms)
+        # the plain search as per-stage launches (the reference's way: one CTA per event, one
+        # kernel after the other, no graph)
         chain.set_seed_model(None)
-        l_value = world * events_step * args.steps / (l_ms / 1e3)
-        learned = {"value": round(l_value, 1), "unit": UNIT, "ratio_vs_plain": round(l_value / value, 4),
-                   "doublets_scanned_fraction": round(scanned / max(doublets, 1), 4),
-                   "fallback_event_fraction": round(fallback / max(events_step, 1), 6),
-                   "model": "allen_b200/data/seed_pruner.npz",
-                   "quality": "efficiency and ghost-rate deltas vs plain: "
-                              "profiles/seed_pruner_train300k_eval100k_nu7.6.md"}
+        chain.configure(search_threads=256, search_lanes_per_seed=0, search_ring_global=0, persistent=0,
+                        search_hit_capacity=2560, cluster_stage_capacity=2560, cluster_blob_bytes=32768,
+                        estimate_blob_bytes=24576, seed_window=0)
+        p_ms = timed(dev, use_graph=False)
+        chain.configure(**plain_cfg)
+        p_value = aggregate_rate(world, events_step, args.steps, p_ms)
+        plain_chain_ms = ms / args.steps / len(slices)
+        search_plain = plain_stages.get("search_by_triplet_kernel", 0.0)
+        learned = {
+            "value": round(l_value, 1), "unit": UNIT,
+            "ratio_vs_plain": round(l_value / value, 4),
+            "ratio_vs_per_stage_plain": round(l_value / p_value, 4),
+            "per_stage_plain": {"value": round(p_value, 1), "unit": UNIT,
+                                "how": "one CTA per event (rings and staging in shared memory), kernels launched one "
+                                       "by one without a CUDA graph, plain search"},
+            "quality": {"events": events_step, "plain": q_plain, "learned": q_learned,
+                        "efficiency_delta": round(q_learned["efficiency"] - q_plain["efficiency"], 6),
+                        "ghost_rate_delta": round(q_learned["ghost_rate"] - q_plain["ghost_rate"], 6),
+                        "clone_rate_delta": round(q_learned["clone_rate"] - q_plain["clone_rate"], 6),
+                        "tolerance": 0.002,
+                        "within_tolerance": bool(q_learned["efficiency"] - q_plain["efficiency"] >= -0.002 and
+                                                 q_learned["ghost_rate"] - q_plain["ghost_rate"] <= 0.002)},
+            "phase_split_ms_per_slice": {
+                "plain": {"search": round(search_plain, 4), "chain": round(plain_chain_ms, 4)},
+                "learned": {"seed_gate": round(l_stages.get("seed_gate_kernel", 0.0), 4),
+                            "search": round(l_stages.get("search_by_triplet_kernel", 0.0), 4),
+                            "chain": round(l_ms / args.steps / len(slices), 4)}},
+            "amdahl": {"search_share_plain": round(search_plain / plain_chain_ms, 4) if plain_chain_ms else None,
+                       "ceiling_if_the_search_were_free": round(plain_chain_ms / (plain_chain_ms - search_plain), 3)
+                       if plain_chain_ms > search_plain else None},
+            "model": "allen_b200/data/seed_pruner.npz", "config": seed_pruner.load_learned_config(),
+        }
+        del truths
 
     # velo_kalman_filter appended to the chain (the next stage of the reference sequence)
     kalman = None
@@ -546,22 +608,6 @@ def run_ours(args):
     # rings in shared memory, no CUDA graph) for comparison; a stress workload (nu = 15, noise 1e-4
     # per pixel, 95 % hit efficiency; slices of 4000, since 16000 such events overflow the 32-bit
     # container offsets), also in learned mode
-    def timed(dev_list, use_graph=True):
-        def once():
-            for d in dev_list:
-                chain.run(d, use_graph=use_graph)
-        for _ in range(max(3, args.warmup)):
-            once()
-        torch.cuda.synchronize()
-        replicas.barrier()
-        t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        t_start.record(stream)
-        for _ in range(args.steps):
-            once()
-        t_end.record(stream)
-        torch.cuda.synchronize()
-        return max_over_ranks(t_start.elapsed_time(t_end))
-
     workloads = None
     if not args.no_workloads:
         workloads = {}
@@ -598,7 +644,8 @@ def run_ours(args):
                            "without a CUDA graph"}
             if name.startswith("stress") and not args.no_learned:
                 from allen_b200 import seed_pruner
-                chain.set_seed_model(seed_pruner.load(os.path.join(REPO, "allen_b200", "data", "seed_pruner.npz")))
+                tuned = chain.get_config()
+                seed_pruner.use_learned(chain)
                 l_ms = timed(c_dev)
                 fb = sc = db = 0
                 for x, d in zip(c_slices, c_dev):
@@ -609,10 +656,11 @@ def run_ours(args):
                     sc += int(st[:, 1].sum())
                     fb += int((st[:, 2] == 2).sum())
                 chain.set_seed_model(None)
+                chain.configure(**tuned)
                 l_val = aggregate_rate(world, c_events, args.steps, l_ms)
                 entry["learned"] = {"value": round(l_val, 1), "unit": UNIT,
                                     "ratio_vs_plain": round(l_val / entry["value"], 4),
-                                    "doublets_scanned_fraction": round(sc / max(db, 1), 4),
+                                    "candidates_searched_fraction": round(sc / max(db, 1), 4),
                                     "fallback_event_fraction": round(fb / max(c_events, 1), 6)}
             workloads[name] = entry
             del c_dev, c_slices

@@ -107,14 +107,16 @@ typedef struct {
   unsigned* dev_offsets_velo_track_hit_number;     /* [tracks + 1] */
   char* dev_velo_track_hits;                       /* [18 TH] */
   uint8_t* dev_accepted_velo_tracks;               /* [tracks + three-hit tracks] */
-  unsigned* dev_seed_stats;                        /* [3 N]: doublets formed, doublets scanned, search
-                                                      mode (0 plain, 1 learned, 2 learned then plain) */
+  unsigned* dev_seed_stats;                        /* [3 N]: seed candidates met unused, candidates searched,
+                                                      mode (0 plain, 1 learned, 2 gate out of bounds: plain) */
   uint8_t* dev_is_backward;                        /* [tracks] velo_kalman_filter (when enabled) */
   char* dev_velo_kalman_beamline_states;           /* [56 tracks] Velo::Consolidated::States */
   char* dev_velo_kalman_endvelo_states;            /* [56 tracks] */
   unsigned* dev_each_sensor_pair_size;             /* retina front end: [S N], S = 208 (v2/v3) or 104 (v4) */
   unsigned* dev_offsets_each_sensor_pair_size;     /* [S N + 1] */
   unsigned* dev_retina_bank_index;                 /* [S] */
+  uint8_t* dev_seed_gate;                          /* [T] learned mode: 1 = the hit is searched as a seed's h1 */
+  unsigned* dev_gate_stats;                        /* [2 N] learned mode: seed candidates, candidates kept */
 } VeloChainOutputs;
 
 /* Host scalars of the last run, available after velo_chain_synchronize(). */
@@ -264,6 +266,8 @@ typedef struct {
                                       events are ranked by comparing every pair of keys */
   unsigned kalman_warp_hits;       /* Kalman filter: hits of a warp's 32 tracks staged in shared memory
                                       (at most 368, default 368); longer spans are read in place */
+  unsigned seed_window;            /* learned mode only: h0 candidates searched per seed candidate after the
+                                      first module pair, 1..4 (0: the reference's 4, SearchByTriplet.cu:228) */
 } VeloLaunchConfig;
 VeloStatus velo_chain_configure(VeloChain* chain, const VeloLaunchConfig* config);
 VeloStatus velo_chain_get_config(const VeloChain* chain, VeloLaunchConfig* config);
@@ -423,13 +427,15 @@ VeloStatus velo_validate_tracks(
   unsigned long long* dev_counts,
   VeloStream stream);
 
-/* Learned seed pruner (no counterpart in the reference).  A 12-32-32-1 network scores each
- * (h0, h1) doublet of the flat seeding (SearchByTriplet.cu:298-446) before its h2 window is
- * scanned; doublets whose logit is not above threshold_logit are not scanned.  An event whose
- * fraction of scanned doublets falls outside [kept_lo, kept_hi] is searched again by the
- * plain search.  Weights are used as bf16 on the tensor cores (mma.sync, fp32 accumulation);
- * inputs are standardised with mean / inv_std.  Parameter order of a flat gradient or
- * parameter vector (VELO_SEED_PARAMS floats): w1, b1, w2, b2, w3, b3. */
+/* Learned seed gate (no counterpart in the reference).  Before the triplet search, a 12-32-32-1
+ * network scores every hit of module pairs 1..24 as a seed candidate (the middle hit h1 of the
+ * seeding, SearchByTriplet.cu:298-446) from geometric features of its neighbours in the module
+ * pairs on either side; the seeding then searches (h0 candidates, h2 windows) only the unused
+ * candidates whose logit is above threshold_logit.  An event whose fraction of kept candidates
+ * falls outside [kept_lo, kept_hi] is searched by the plain search instead.  Weights are used as
+ * bf16 on the tensor cores (fp32 accumulation); inputs are standardised with mean / inv_std.
+ * Parameter order of a flat gradient or parameter vector (VELO_SEED_PARAMS floats): w1, b1, w2,
+ * b2, w3, b3. */
 #define VELO_SEED_FEATURES 12
 #define VELO_SEED_HIDDEN 32
 #define VELO_SEED_PARAMS (32 * 12 + 32 + 32 * 32 + 32 + 32 + 1)
@@ -446,28 +452,31 @@ typedef struct {
   float kept_lo, kept_hi;
 } VeloSeedModel;
 
-/* One training doublet (64 bytes): raw features, label 1 if the plain seeding turned the
- * doublet into a seed, event index and the two hits' indices in the sorted container.
- * Features: tx, ty, |t|, signed distance to the beam axis, z of closest approach,
- * phi(h1) - phi(h0) and phi(h1) (rad / pi), r(h1), dr/dz, |dz|, candidate rank, candidates. */
+/* One training record (64 bytes): a seed candidate's raw features, label 1 if the plain
+ * seeding made a seed with it as middle hit, event index, h0 = 0xFFFFFFFF, and the candidate's
+ * index in the sorted container.  Features: r, z, sqrt of the smallest and second smallest
+ * beam-axis distance of the lines to its 4 nearest-in-phi h0 candidates, z of closest approach
+ * and slope of the best line, sqrt of the smallest h2 scatter of the best and second line,
+ * neighbours within twice the phi tolerance in the two module pairs, smallest |dphi| to the h0
+ * candidates (rad / pi), phi (rad / pi). */
 typedef struct {
   float f[VELO_SEED_FEATURES];
   float label;
   unsigned event, h0, h1;
-} VeloDoubletRecord;
+} VeloSeedRecord;
 
-/* model != NULL: the chain searches in learned mode (flat seeding, search_threads block
- * size); NULL: the plain search. */
+/* model != NULL: the chain searches in learned mode (flat seeding, search_threads block size,
+ * the gate kernel before the search); NULL: the plain search. */
 VeloStatus velo_chain_set_seed_model(VeloChain* chain, const VeloSeedModel* model);
-/* dev_records != NULL: the following runs (plain search) append the doublets of one h1
- * candidate in record_every to dev_records (capacity entries) and count them in *dev_count
- * (device u32; entries beyond the capacity are counted, not written). */
-VeloStatus velo_chain_record_doublets(
-  VeloChain* chain, VeloDoubletRecord* dev_records, unsigned capacity, unsigned record_every, unsigned* dev_count);
+/* dev_records != NULL: the following runs (plain search) append one seed candidate in
+ * record_every (the ones the search met unused) to dev_records (capacity entries) and count them
+ * in *dev_count (device u32; entries beyond the capacity are counted, not written). */
+VeloStatus velo_chain_record_seeds(
+  VeloChain* chain, VeloSeedRecord* dev_records, unsigned capacity, unsigned record_every, unsigned* dev_count);
 
 /* Training on the GPU: binary cross-entropy (positives weighted by pos_weight), mean over the
  * batch, Adam (beta1 0.9, beta2 0.999, eps 1e-8).  Forward and backward passes are warp-level
- * tensor-core kernels over 16-doublet tiles. */
+ * tensor-core kernels over 16-record tiles. */
 typedef struct VeloSeedTrainer VeloSeedTrainer;
 VeloStatus velo_seed_trainer_create(
   const VeloSeedModel* init, float learning_rate, float pos_weight, VeloSeedTrainer** trainer);
@@ -475,7 +484,7 @@ VeloStatus velo_seed_trainer_create(
  * batch's mean loss and makes the call synchronous. */
 VeloStatus velo_seed_trainer_step(
   VeloSeedTrainer* trainer,
-  const VeloDoubletRecord* dev_records,
+  const VeloSeedRecord* dev_records,
   unsigned long long first,
   unsigned batch,
   VeloStream stream,
@@ -483,7 +492,7 @@ VeloStatus velo_seed_trainer_step(
 /* Gradients (VELO_SEED_PARAMS floats, host) and mean loss of a batch, without a step. */
 VeloStatus velo_seed_trainer_gradients(
   VeloSeedTrainer* trainer,
-  const VeloDoubletRecord* dev_records,
+  const VeloSeedRecord* dev_records,
   unsigned long long first,
   unsigned batch,
   VeloStream stream,
@@ -491,7 +500,7 @@ VeloStatus velo_seed_trainer_gradients(
   float* loss);
 /* Logits of records [0, n) into dev_logits (device floats) with the current weights. */
 VeloStatus velo_seed_trainer_score(
-  VeloSeedTrainer* trainer, const VeloDoubletRecord* dev_records, unsigned long long n, float* dev_logits, VeloStream stream);
+  VeloSeedTrainer* trainer, const VeloSeedRecord* dev_records, unsigned long long n, float* dev_logits, VeloStream stream);
 /* The current fp32 weights, with the standardisation, threshold and bounds of the model. */
 VeloStatus velo_seed_trainer_model(VeloSeedTrainer* trainer, VeloSeedModel* model);
 void velo_seed_trainer_destroy(VeloSeedTrainer* trainer);

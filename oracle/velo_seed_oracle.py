@@ -1,17 +1,17 @@
 """CPU oracle of the learned seed pruner (test infrastructure only).
 
-Restates, in numpy, what the CUDA kernels of allen_b200/csrc/velo_mlp.cuh and velo_mlp.cu
-compute, with the same rounding points, so the GPU features, logits and gradients can be
+Restates, in numpy, what the CUDA kernels of allen_b200/csrc/velo_gate.cu, velo_mlp.cuh and
+velo_mlp.cu compute, with the same rounding points, so the GPU features, logits and gradients can be
 checked against it:
 
-* doublet_features(): the 12 fp32 doublet features, operation for operation (IEEE division
-  and square root are correctly rounded in both, and the kernels are built without FMA
-  contraction), so they agree bit for bit;
+* seed_features(): the 12 fp32 features of a seed candidate, operation for operation (IEEE
+  division and square root are correctly rounded in both, and the kernels are built without
+  FMA contraction), so they agree bit for bit;
 * forward() / gradients(): the 12-32-32-1 network with bf16 (round to nearest even) inputs,
   weights and layer inputs and fp32 biases; sums in float64 here, fp32 in the tensor-core
   kernels, so results agree to rounding of the sums.
 
-The pruner has no counterpart in the reference (its seeding is SearchByTriplet.cu:298-446);
+The gate has no counterpart in the reference (its seeding is SearchByTriplet.cu:298-446);
 the training labels come from the plain search, which is itself pinned bit for bit against
 the reference CPU build.
 """
@@ -32,28 +32,120 @@ def bf16(a):
     return r.astype(np.uint32).view(np.float32).reshape(a.shape)
 
 
-def doublet_features(x0, y0, z0, phi0, x1, y1, z1, phi1, rank, found):
-    """Arrays of float32 positions and int16 phi of h0 and h1 -> [n, 12] float32."""
-    f32 = np.float32
-    x0, y0, z0, x1, y1, z1 = (np.asarray(v, f32) for v in (x0, y0, z0, x1, y1, z1))
-    phi0 = np.asarray(phi0, np.int16)
-    phi1 = np.asarray(phi1, np.int16)
-    with np.errstate(divide="ignore", invalid="ignore"):
-        dz = z1 - z0
-        inv = f32(1.0) / dz
+F32 = np.float32
+PI_F = F32(3.141592654)
+CONVERT_I16 = F32(32768.0) / PI_F
+C1 = F32(0.25) * PI_F
+C2 = F32(0.75) * PI_F
+
+
+def float_to_i16(v):
+    """float -> int16 through a 32-bit truncation toward zero (VeloTools.cuh:55-60)."""
+    return np.int16(np.int32(np.trunc(v)).astype(np.int16))
+
+
+def fast_atan2f(y, x):
+    """VeloTools.cuh:18-38, fp32 operation for operation."""
+    y, x = F32(y), F32(x)
+    abs_y = F32(abs(y))
+    nom = (x - abs_y) if x > 0 else (x + abs_y)
+    den = (x + abs_y) if x > 0 else (abs_y - x)
+    r = F32(nom / den)
+    angle = (C1 if x > 0 else C2) - C1 * r
+    return F32(np.copysign(angle, y))
+
+
+def hit_phi_16(x, y):
+    return float_to_i16(fast_atan2f(y, x) * CONVERT_I16)
+
+
+def phi_tolerance_i16(phi_tolerance=0.045):
+    return int(np.int32(np.trunc(F32(phi_tolerance) * CONVERT_I16)).astype(np.int16))
+
+
+def leftmost(phis, value):
+    """binary_search_leftmost (BinarySearch.cuh:15-30): first index with phi >= value."""
+    return int(np.searchsorted(phis.astype(np.int32), int(value), side="left"))
+
+
+def module_zs(geometry: bytes):
+    """The 52 module z of velo_geometry.bin (count, then floats)."""
+    n = int(np.frombuffer(geometry[:8], np.uint64)[0])
+    return np.frombuffer(geometry[8:8 + 4 * n], np.float32)
+
+
+def seed_features(xyz, phi, start, num, zs, m, h1, tol):
+    """The 12 features of seed candidate h1 (event-relative index into xyz [n, 3] float32 and phi
+    int16 of the event's sorted hits) on module pair m = 1..24; start / num: the event's module
+    pair offsets (event-relative) and cluster counts; zs: module z; tol: the phi tolerance as
+    int16.  The kernel's seed_features (allen_b200/csrc/velo_gate.cu), fp32 operation for
+    operation."""
+    def hit(i):
+        return F32(xyz[i, 0]), F32(xyz[i, 1]), F32(xyz[i, 2])
+
+    x1, y1, z1 = hit(h1)
+    phi1 = int(phi[h1])
+    ps, pn = int(start[m + 1]), int(num[m + 1])
+    ns, nn = int(start[m - 1]), int(num[m - 1])
+    pphi, nphi = phi[ps:ps + pn], phi[ns:ns + nn]
+    best_d = second_d = F32(1000.0)
+    best_z = best_t = F32(0.0)
+    min_dphi = F32(1.0)
+    best = second = None
+    pos = leftmost(pphi, phi1)
+    for i in range(min(pn, 4)):
+        pos += i if (i & 1) else -i
+        ib = pos + pn if pos < 0 else (pos - pn if pos >= pn else pos)
+        h0 = ps + ib
+        x0, y0, z0 = hit(h0)
+        inv = F32(1.0) / (z1 - z0)
         tx = (x1 - x0) * inv
         ty = (y1 - y0) * inv
         t2 = tx * tx + ty * ty
-        t = np.sqrt(t2)
-        doca = (x1 * ty - y1 * tx) / np.maximum(t, f32(1e-6))
-        zpoca = z1 - (x1 * tx + y1 * ty) / np.maximum(t2, f32(1e-12))
-        r0 = np.sqrt(x0 * x0 + y0 * y0)
-        r1 = np.sqrt(x1 * x1 + y1 * y1)
-        dphi = (phi1.astype(np.int32) - phi0.astype(np.int32)).astype(np.int16).astype(f32)
-        out = np.stack([tx, ty, t, doca, zpoca, dphi * f32(3.0517578125e-05), r1, (r1 - r0) * inv, np.abs(dz),
-                        np.asarray(rank, f32), np.asarray(found, f32), phi1.astype(f32) * f32(3.0517578125e-05)],
-                       axis=-1)
-    return out.astype(f32)
+        t = F32(np.sqrt(t2))
+        d = F32(abs(x1 * ty - y1 * tx)) / max(t, F32(1e-6))
+        dphi = F32(abs(int(np.int16(np.int32(phi1) - np.int32(phi[h0]))))) * F32(3.0517578125e-05)
+        min_dphi = min(min_dphi, dphi)
+        if d < best_d:
+            second_d, second = best_d, best
+            best_d, best = d, (h0, tx, ty)
+            best_z = z1 - (x1 * tx + y1 * ty) / max(t2, F32(1e-12))
+            best_t = t
+        elif d < second_d:
+            second_d, second = d, (h0, tx, ty)
+    dz_next = F32(zs[2 * (m - 1)]) - F32(zs[2 * (m + 1)])
+    scatter = [F32(1000.0), F32(1000.0)]
+    for c, cand in enumerate((best, second)):
+        if cand is None or nn == 0:
+            continue
+        h0, tx, ty = cand
+        x0, y0, z0 = hit(h0)
+        xp = x0 + tx * dz_next
+        yp = y0 + ty * dz_next
+        phi_p = int(hit_phi_16(xp, yp))
+        lo = int(np.int16(np.int32(phi_p) - np.int32(tol)))
+        st = int(np.int16(leftmost(nphi, lo)))
+        idx = (st & 0xFFFFFFFF) % nn
+        for _ in range(min(nn, 3)):
+            h2 = ns + idx
+            if abs(int(np.int16(np.int32(phi[h2]) - np.int32(phi_p)))) > tol:
+                break
+            x2, y2, z2 = hit(h2)
+            dz = z2 - z0
+            dx = (x0 + tx * dz) - x2
+            dy = (y0 + ty * dz) - y2
+            scatter[c] = min(scatter[c], dx * dx + dy * dy)
+            idx = 0 if idx + 1 == nn else idx + 1
+
+    def count(ph, n):
+        lo = leftmost(ph, max(-32768, min(32767, phi1 - 2 * tol)))
+        hv = phi1 + 2 * tol + 1
+        hi = n if hv > 32767 else leftmost(ph, hv)
+        return F32(min(hi - lo, 16))
+
+    return np.array([np.sqrt(x1 * x1 + y1 * y1), z1, np.sqrt(best_d), best_z, best_t, np.sqrt(second_d),
+                     np.sqrt(scatter[0]), np.sqrt(scatter[1]), count(pphi, pn), count(nphi, nn), min_dphi,
+                     F32(phi1) * F32(3.0517578125e-05)], dtype=np.float32)
 
 
 def split(params):

@@ -44,3 +44,51 @@ def test_sweeps_repeat_until_nothing_changes(monkeypatch):
     assert best1["search_threads"] == 256 and best1["search_lanes_per_seed"] == 0
     # the ring variants were tried with persistent launches, never without
     assert all(t["config"]["persistent"] for t in trials if t["config"]["search_ring_global"])
+
+
+class FakeLearnedChain(FakeChain):
+    """Stand-in for the learned mode: rate rises as the gate keeps less and the window
+    shrinks; quality falls with them (recall below 0.98 or window 2 out of tolerance)."""
+
+    def __init__(self):
+        super().__init__()
+        self.cfg.update(search_threads=128, search_lanes_per_seed=0, search_ring_global=1, persistent=1,
+                        seed_window=0)
+        self.threshold = None
+
+    def configure(self, **cfg):  # VeloChain.configure: the given fields, the others kept
+        merged = dict(self.cfg)
+        merged.update(cfg)
+        super().configure(**merged)
+
+    def set_seed_model(self, model):
+        self.threshold = model.threshold_logit
+
+    def rate(self):
+        r = 1.0 + 0.1 * self.threshold  # higher threshold: fewer candidates searched
+        r *= {0: 1.0, 3: 1.04, 2: 1.08}[self.cfg["seed_window"]]
+        r *= 1.05 if self.cfg["search_threads"] == 128 else 1.0
+        r *= 1.02 if self.cfg["events_per_claim"] == 2 else 1.0
+        return r
+
+    def quality(self):
+        recall = {1.0: 0.995, 2.0: 0.99, 3.0: 0.98, 4.0: 0.97}[self.threshold]
+        eff = 0.994 - (0.003 if recall < 0.98 else 0.0) - (0.004 if self.cfg["seed_window"] == 2 else 0.0)
+        return {"efficiency": eff, "ghost_rate": 0.003}
+
+
+class Model:
+    threshold_logit = 0.0
+
+
+def test_learned_tuning_respects_the_quality_tolerance(monkeypatch):
+    chain = FakeLearnedChain()
+    monkeypatch.setattr(autotune, "measure", lambda ch, dev, repeats=3: ch.rate())
+    thresholds = {0.995: 1.0, 0.99: 2.0, 0.98: 3.0, 0.97: 4.0}
+    best, rate, trials = autotune.tune_learned(chain, Model(), thresholds, [], lambda ch: ch.quality(),
+                                               {"efficiency": 0.994, "ghost_rate": 0.003}, log=lambda *_: None)
+    # the fastest admissible gate: recall 0.98 (0.97 loses too much), window 3 (2 loses too much)
+    assert (best["recall"], best["seed_window"]) == (0.98, 3)
+    assert best["search_threads"] == 128 and best["events_per_claim"] == 2
+    assert [t for t in trials if "admissible" in t and not t["admissible"]]
+    assert rate == chain.rate()
