@@ -42,6 +42,7 @@ namespace velo {
     err_input_capacity = 1u << 6,    // slice larger than the reserved workspace
     err_hits_per_event = 1u << 7,    // more than 65535 estimated hits in one event (u16 indices)
     err_bad_super_pixel = 1u << 8,   // a candidate's flood fill found no pixel (bank index names another bank)
+    err_mma_timeout = 1u << 9,       // a tensor-core MMA of the seed gate did not complete in time (gate off)
   };
 
   // Detector description and super-pixel lookup tables, one copy in global memory

@@ -680,10 +680,16 @@ namespace velo {
       bad = true;
       return false;
     }
-    const uint32_t cx = x / n;
-    const uint32_t cy = y / n;
-    const float fx = __fdiv_rn(__uint2float_rn(x), __uint2float_rn(n)) - __uint2float_rn(cx);
-    const float fy = __fdiv_rn(__uint2float_rn(y), __uint2float_rn(n)) - __uint2float_rn(cy);
+    // The integer centroids x / n and y / n are the truncated correctly rounded quotients: a
+    // quotient below 1024 (columns < 768, rows < 256) with n < 32768 pixels is at least 1 / n
+    // below the next integer, more than half an ulp, so rounding never reaches it.  The
+    // fractions are the reference's fl(x / n) - cx (MaskedVeloClustering.cu:461-466).
+    const float qx = __fdiv_rn(__uint2float_rn(x), __uint2float_rn(n));
+    const float qy = __fdiv_rn(__uint2float_rn(y), __uint2float_rn(n));
+    const uint32_t cx = __float2uint_rz(qx);
+    const uint32_t cy = __float2uint_rz(qy);
+    const float fx = qx - __uint2float_rn(cx);
+    const float fy = qy - __uint2float_rn(cy);
     const uint32_t chip = cx >> 8;
     o.id = lhcb_id(channel_id(sensor_number, chip, cx & 0xFFu, cy));
     const float local_x = column_local_x(g, cx) + fx * column_x_pitch(g, cx);

@@ -1,9 +1,13 @@
 // Learned seed gate: decides, before the triplet search, which hits the seeding searches as the
-// middle hit h1 of a seed.  One CTA per event; every hit of module pairs 1..24 (the pairs the
-// seeding takes h1 from, SearchByTriplet.cu:165-245) gets 12 geometric features from its
-// neighbours in the module pairs on either side, the 12-32-32-1 network scores 32 hits per warp
-// on the tensor cores (two 16-row mma.sync tiles, velo_mlp.cuh), and the hit's gate byte says
-// whether its logit is above the model's threshold.  In recording mode the same features go,
+// middle hit h1 of a seed.  One CTA of 128 threads per event; every hit of module pairs 1..24
+// (the pairs the seeding takes h1 from, SearchByTriplet.cu:165-245) gets 12 geometric features
+// from its neighbours in the module pairs on either side, one hit per thread.  The 12-32-32-1
+// network scores 128 hits at a time on the fifth-generation tensor cores (velo_umma.cuh): the
+// inputs as a 128 x 16 bf16 tile in shared memory, tcgen05.mma by one thread into a 128 x 32
+// fp32 accumulator in tensor memory, read back (tcgen05.ld) by each thread for its own row,
+// ReLU and bf16 into the next tile, the second layer the same way (two K steps), the output
+// unit on the CUDA cores; the hit's gate byte says whether its logit is above the model's
+// threshold.  In recording mode the same features go,
 // with the plain search's outcome for the hit as label, into training records.
 //
 // Why a gate on h1 and not a score per (h0, h1) doublet: the plain seeding searches every
@@ -15,7 +19,10 @@
 //
 // No counterpart in the reference; the features are geometric and independent of which hits are
 // used, so the gate of an event is known before its search.
+#include <type_traits>
+
 #include "velo_kernels.cuh"
+#include "velo_umma.cuh"
 
 namespace velo {
 
@@ -150,28 +157,47 @@ namespace velo {
     }
   } // namespace
 
+  // Shared state of the gate kernel's network (inference): the 128-row input and hidden tiles,
+  // the weight tiles (B operands, N = 32 rows), the MMA completion barrier and the TMEM base.
+  struct GateMlpShared {
+    alignas(128) unsigned char a1[gate_threads * mlp_k1 * 2];    // inputs, 128 x 16 bf16
+    alignas(128) unsigned char a2[gate_threads * mlp_hidden * 2]; // layer-1 outputs, 128 x 32 bf16
+    alignas(128) unsigned char w1[mlp_hidden * mlp_k1 * 2];       // W1, 32 x 16 bf16
+    alignas(128) unsigned char w2[mlp_hidden * mlp_hidden * 2];   // W2, 32 x 32 bf16
+    uint64_t bar;
+    uint32_t tmem;
+  };
+  constexpr unsigned gate_tmem_columns = 32; // one 128 x 32 fp32 accumulator, reused by both layers
+  constexpr unsigned gate_wait_limit = 1u << 22;
+
+  __device__ __forceinline__ void put_u32(unsigned char* tile, unsigned r, unsigned k, unsigned K, uint32_t v)
+  {
+    *reinterpret_cast<uint32_t*>(tile + umma::tile_offset(r, k, K)) = v;
+  }
+
   template<bool RECORD>
-  __global__ void __launch_bounds__(gate_threads, 4) seed_gate_kernel(GateParams p)
+  __global__ void __launch_bounds__(gate_threads) seed_gate_kernel(GateParams p)
   {
     __shared__ uint16_t bucket[n_module_pairs][n_buckets + 1];
     __shared__ unsigned start[n_module_pairs + 1]; // event-relative first hit of each module pair
     __shared__ unsigned num[n_module_pairs];
     __shared__ unsigned first_item[n_module_pairs]; // candidates before module pair m (m = 1..24)
     __shared__ unsigned kept_count;
-    __shared__ __align__(16) uint32_t rows[RECORD ? 1 : gate_threads / 32][32][8]; // per warp: 32 rows of 16 bf16
+    __shared__ std::conditional_t<RECORD, int, GateMlpShared> mlp;
     const unsigned e = blockIdx.x;
     const unsigned T = p.offsets_estimated_input_size[p.n_events * n_module_pairs];
-    if (T > p.cluster_capacity) return; // flagged by the clustering kernel
+    if (T > p.cluster_capacity) return; // flagged by the clustering kernel (before any TMEM is held)
     const unsigned* g_start = p.offsets_estimated_input_size + e * n_module_pairs;
     const unsigned* g_num = p.module_cluster_num + e * n_module_pairs;
     const unsigned hit_offset = g_start[0];
-    if (threadIdx.x < n_module_pairs) {
-      start[threadIdx.x] = g_start[threadIdx.x] - hit_offset;
-      num[threadIdx.x] = g_num[threadIdx.x];
+    const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    if (tid < n_module_pairs) {
+      start[tid] = g_start[tid] - hit_offset;
+      num[tid] = g_num[tid];
     }
-    if (threadIdx.x == 0) kept_count = 0;
+    if (tid == 0) kept_count = 0;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       unsigned s = 0;
       for (unsigned m = 0; m < n_module_pairs; ++m) {
         first_item[m] = s;
@@ -182,25 +208,50 @@ namespace velo {
     const EventHits h {ClusterView {const_cast<char*>(p.sorted_container), T}, hit_offset,
                        ClusterView {const_cast<char*>(p.sorted_container), T}.phi_begin() + hit_offset};
     build_bucket_tables(bucket, h.phi, g_start, g_num, hit_offset);
+    uint32_t tmem = 0;
+    unsigned phase = 0;
+    if constexpr (!RECORD) {
+      // TMEM for the accumulator, the barrier, the weights in their canonical tiles
+      if (warp == 0) umma::alloc(&mlp.tmem, gate_tmem_columns);
+      if (tid == 0) umma::mbar_init(&mlp.bar, 1);
+      for (unsigned i = tid; i < mlp_hidden * (mlp_k1 / 2); i += blockDim.x)
+        put_u32(mlp.w1, i / (mlp_k1 / 2), 2 * (i % (mlp_k1 / 2)), mlp_k1, __ldg(&p.model->w1[0][0] + i));
+      for (unsigned i = tid; i < mlp_hidden * (mlp_hidden / 2); i += blockDim.x)
+        put_u32(mlp.w2, i / (mlp_hidden / 2), 2 * (i % (mlp_hidden / 2)), mlp_hidden, __ldg(&p.model->w2[0][0] + i));
+      umma::fence_async_shared();
+      umma::fence_before_sync();
+    }
     __syncthreads();
+    if constexpr (!RECORD) {
+      umma::fence_after_sync();
+      tmem = mlp.tmem;
+    }
     const unsigned n_items = start[n_module_pairs];
     const Constants k = p.k;
-    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    // 32 consecutive candidates per warp, one per lane
-    for (unsigned base = warp * 32u; base < n_items; base += blockDim.x) {
-      const unsigned item = base + lane;
+    constexpr uint32_t idesc = umma::idesc_bf16(gate_threads, mlp_hidden);
+    bool failed = false;
+    // one candidate per thread, 128 per tile
+    for (unsigned base = 0; base < n_items; base += blockDim.x) {
+      const unsigned item = base + tid;
       unsigned h1 = 0xFFFFFFFFu;
       float f[mlp_features];
       bool active = item < n_items;
+      unsigned m = 1;
       if (active) {
-        unsigned m = 1;
-        while (m < n_module_pairs - 2 && first_item[m + 1] <= item)
-          ++m;
+        // the candidate's module pair: the last m with first_item[m] <= item (binary search)
+        unsigned lo = 1, hi = n_module_pairs - 2;
+        while (lo < hi) {
+          const unsigned mid = (lo + hi + 1) / 2;
+          if (first_item[mid] <= item) lo = mid;
+          else hi = mid - 1;
+        }
+        m = lo;
         h1 = start[m] + (item - first_item[m]);
-        if (RECORD) {
+      }
+      if constexpr (RECORD) {
+        if (active) {
           const uint8_t outcome = p.h1_outcome[hit_offset + h1];
-          active = outcome != 0 &&
-                   ((e * 0x9E3779B1u) ^ ((hit_offset + h1) * 0x85EBCA77u)) % p.record_every == 0;
+          active = outcome != 0 && ((e * 0x9E3779B1u) ^ ((hit_offset + h1) * 0x85EBCA77u)) % p.record_every == 0;
           if (active) {
             const float dz_next = __ldg(p.geo->module_zs + 2 * (m - 1)) - __ldg(p.geo->module_zs + 2 * (m + 1));
             seed_features(h, bucket, k, m, PairRange {start[m + 1], num[m + 1]}, PairRange {start[m - 1], num[m - 1]},
@@ -219,51 +270,78 @@ namespace velo {
             }
           }
         }
-        else {
+      }
+      else {
+        // layer 1: the standardised bf16 inputs as row tid of the input tile
+        uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (active) {
           const float dz_next = __ldg(p.geo->module_zs + 2 * (m - 1)) - __ldg(p.geo->module_zs + 2 * (m + 1));
           seed_features(h, bucket, k, m, PairRange {start[m + 1], num[m + 1]}, PairRange {start[m - 1], num[m - 1]},
                         dz_next, h1, f);
+          standardise_pairs(*p.model, f, w);
         }
-      }
-      if constexpr (!RECORD) {
-        uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (active) standardise_pairs(*p.model, f, w);
 #pragma unroll
         for (unsigned i = 0; i < 8; ++i)
-          rows[warp][lane][i] = w[i];
-        __syncwarp();
-        const float thr = __ldg(&p.model->threshold_logit);
-        unsigned kept = 0;
-#pragma unroll
-        for (unsigned t = 0; t < 2; ++t) {
-          uint32_t a[4];
-          ldmatrix_x4(a, &rows[warp][16 * t + (lane & 15u)][(lane >> 4) * 4]);
-          float lg, lg8;
-          mlp_forward_tile(p.model, a, lg, lg8);
-          // logits of rows g and g + 8 of tile t sit in lane 4 g; hand them to those rows' lanes
-          const unsigned g = lane >> 2;
-          const float from_g = __shfl_sync(0xFFFFFFFFu, lg, (lane & 7u) * 4u);
-          const float from_g8 = __shfl_sync(0xFFFFFFFFu, lg8, (lane & 7u) * 4u);
-          (void) g;
-          if ((lane >> 4) == t) {
-            const float logit = (lane & 8u) ? from_g8 : from_g;
-            if (active) {
-              const bool keep = logit > thr;
-              p.gate[hit_offset + h1] = keep ? 1 : 0;
-              kept += keep ? 1u : 0u;
-            }
-          }
+          put_u32(mlp.a1, tid, 2 * i, mlp_k1, w[i]);
+        umma::fence_async_shared();
+        __syncthreads();
+        if (tid == 0) {
+          umma::fence_after_sync();
+          umma::mma(tmem, umma::desc(mlp.a1, mlp_k1, 0), umma::desc(mlp.w1, mlp_k1, 0), idesc, false);
+          umma::commit(&mlp.bar);
         }
-        __syncwarp(); // rows read before the next chunk overwrites them
-        const unsigned warp_kept = __reduce_add_sync(0xFFFFFFFFu, kept);
-        if (lane == 0 && warp_kept) atomicAdd(&kept_count, warp_kept);
+        failed = __syncthreads_or(!umma::mbar_wait(&mlp.bar, phase, gate_wait_limit));
+        phase ^= 1u;
+        if (failed) break;
+        umma::fence_after_sync();
+        float acc[32];
+        umma::load32(tmem + ((warp * 32u) << 16), acc);
+        // layer 2: bias, ReLU, bf16 as row tid of the hidden tile
+#pragma unroll
+        for (unsigned i = 0; i < mlp_hidden / 2; ++i)
+          put_u32(mlp.a2, tid, 2 * i, mlp_hidden,
+                  pack_bf16(relu(acc[2 * i] + __ldg(&p.model->b1[2 * i])), relu(acc[2 * i + 1] + __ldg(&p.model->b1[2 * i + 1]))));
+        umma::fence_before_sync();
+        umma::fence_async_shared();
+        __syncthreads();
+        if (tid == 0) {
+          umma::fence_after_sync();
+          umma::mma(tmem, umma::desc(mlp.a2, mlp_hidden, 0), umma::desc(mlp.w2, mlp_hidden, 0), idesc, false);
+          umma::mma(tmem, umma::desc(mlp.a2, mlp_hidden, 1), umma::desc(mlp.w2, mlp_hidden, 1), idesc, true);
+          umma::commit(&mlp.bar);
+        }
+        failed = __syncthreads_or(!umma::mbar_wait(&mlp.bar, phase, gate_wait_limit));
+        phase ^= 1u;
+        if (failed) break;
+        umma::fence_after_sync();
+        umma::load32(tmem + ((warp * 32u) << 16), acc);
+        // layer 3 on the CUDA cores: the bf16 hidden units against W3 (fp32 values of bf16 weights)
+        float logit = __ldg(&p.model->b3);
+#pragma unroll
+        for (unsigned i = 0; i < mlp_hidden; ++i) {
+          const float a = __uint_as_float(pack_bf16(relu(acc[i] + __ldg(&p.model->b2[i])), 0.0f) << 16);
+          logit += a * __ldg(&p.model->w3f[i]);
+        }
+        if (active) {
+          const bool keep = logit > __ldg(&p.model->threshold_logit);
+          p.gate[hit_offset + h1] = keep ? 1 : 0;
+          if (keep) atomicAdd(&kept_count, 1u);
+        }
+        umma::fence_before_sync();
+        __syncthreads(); // the tiles and the accumulator are free for the next candidates
       }
     }
     if constexpr (!RECORD) {
+      if (failed) {
+        // an MMA that did not complete in time: flag it, let it drain (bounded), keep no gate
+        if (tid == 0) set_error(p.status, err_mma_timeout);
+        __syncthreads_or(!umma::mbar_wait(&mlp.bar, phase ^ 1u, gate_wait_limit)); // the phase that timed out
+      }
       __syncthreads();
-      if (threadIdx.x == 0) {
+      if (warp == 0) umma::dealloc(tmem, gate_tmem_columns);
+      if (tid == 0) {
         p.gate_stats[2 * e] = n_items;
-        p.gate_stats[2 * e + 1] = kept_count;
+        p.gate_stats[2 * e + 1] = failed ? 0u : kept_count;
       }
     }
   }

@@ -290,7 +290,7 @@ namespace velo {
   };
   template<bool RECORD>
   __global__ void seed_gate_kernel(GateParams p);
-  constexpr unsigned gate_threads = 256;
+  constexpr unsigned gate_threads = 128; // one 128-row tensor-core tile of candidates per round
 
   // Raises a kernel's dynamic shared-memory limit to at least `bytes`, never lowers it: the
   // limit is per kernel and per device, shared by every chain and entry point in the process.
