@@ -1,12 +1,13 @@
 // Training of the learned seed pruner on sm_100a, and the host conversion of a model to
 // its device form.  No counterpart in the reference (see velo_mlp.cuh).
 //
-// mlp_train_kernel: each warp takes 16-record tiles; the forward pass keeps every layer in
-// mma.sync fragments (C layout of one layer = A layout of the next); the backward pass gets
-// the transposed operands of the weight gradients (dZ^T as A, the layer input as B) with
-// movmatrix, so no tile goes through shared memory.  Per-warp gradient sums are reduced in
-// shared memory and added to the global fp32 gradient once per CTA.  adam_kernel updates
-// the fp32 master weights and writes the bf16 copies the kernels read.
+// mlp_train_kernel: 128-record tiles on the fifth-generation tensor cores (tcgen05.mma from
+// shared-memory tiles into tensor memory, velo_umma.cuh), one record per thread for the
+// element-wise work; the weight gradients of both layers accumulate in tensor memory over the
+// CTA's tiles and go to the global fp32 gradient once per CTA.  adam_kernel updates the fp32
+// master weights and publish_kernel writes the bf16 copies the kernels read.
+// mlp_score_kernel (logits of records, for the threshold calibration) stays on warp-level
+// mma.sync tiles of 16 records.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -15,6 +16,7 @@
 
 #include "velo_b200.h"
 #include "velo_mlp.cuh"
+#include "velo_umma.cuh"
 
 namespace velo_host {
   void set_last_error(const std::string& what); // velo_chain.cu
@@ -109,154 +111,222 @@ namespace velo {
     return fminf(fmaxf((__ldg(&r->f[i]) - __ldg(&m.mean[i])) * __ldg(&m.inv_std[i]), -8.0f), 8.0f);
   }
 
-  __global__ void __launch_bounds__(256) mlp_train_kernel(TrainParams p)
+  // Shared tiles of the tcgen05 training kernel (canonical no-swizzle K-major bf16 tiles,
+  // velo_umma.cuh).  The weight gradients of both layers come from one MMA chain: A holds
+  // dZ2^T in rows 0..31 and dZ1^T in rows 32..63 (rows 64..127 zero), B holds a2^T in rows
+  // 0..31 and x^T in rows 32..47, K runs over the tile's 128 records; D[0..31][0..31] is dW2 and
+  // D[32..63][32..47] dW1 (the cross terms are not read), accumulated in TMEM over the tiles.
+  struct TrainShared {
+    alignas(128) unsigned char x[train_rows * mlp_k1 * 2];        // 128 x 16: layer-1 inputs
+    alignas(128) unsigned char a2[train_rows * mlp_hidden * 2];   // 128 x 32: layer-2 inputs
+    alignas(128) unsigned char e2[train_rows * mlp_hidden * 2];   // 128 x 32: dZ2 (A of dH1 = dZ2 W2)
+    alignas(128) unsigned char ga[train_rows * train_rows * 2];   // 128 x 128: [dZ2^T; dZ1^T; 0]
+    alignas(128) unsigned char gb[48 * train_rows * 2];           // 48 x 128: [a2^T; x^T]
+    alignas(128) unsigned char w1[mlp_hidden * mlp_k1 * 2];       // W1 (B of layer 1)
+    alignas(128) unsigned char w2[mlp_hidden * mlp_hidden * 2];   // W2 (B of layer 2)
+    alignas(128) unsigned char w2t[mlp_hidden * mlp_hidden * 2];  // W2^T (B of dH1)
+    uint64_t bar;
+    uint32_t tmem;
+    float sums[3 * mlp_hidden + 2]; // gb1, gb2, gw3, gb3, loss of the CTA
+  };
+  constexpr unsigned train_tmem_columns = 128; // 32 for the layer outputs, 48 for the gradients
+  constexpr unsigned train_wait_limit = 1u << 22;
+
+  __device__ __forceinline__ void put_bf16(unsigned char* tile, unsigned r, unsigned k, unsigned K, float v)
   {
-    __shared__ float block_grads[n_params + 1];
-    for (unsigned i = threadIdx.x; i <= n_params; i += blockDim.x)
-      block_grads[i] = 0.0f;
-    __syncthreads();
+    *reinterpret_cast<__nv_bfloat16*>(tile + umma::tile_offset(r, k, K)) = __float2bfloat16_rn(v);
+  }
+  __device__ __forceinline__ void put_pair(unsigned char* tile, unsigned r, unsigned k, unsigned K, uint32_t v)
+  {
+    *reinterpret_cast<uint32_t*>(tile + umma::tile_offset(r, k, K)) = v;
+  }
+  __device__ __forceinline__ void put_half(unsigned char* tile, unsigned r, unsigned k, unsigned K, uint32_t v)
+  {
+    *reinterpret_cast<uint16_t*>(tile + umma::tile_offset(r, k, K)) = static_cast<uint16_t>(v);
+  }
 
-    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
-    const unsigned warps = blockDim.x >> 5;
+  // One MMA chain of this CTA: issue (thread 0), commit, wait in every thread (bounded).  False
+  // in every thread if the MMAs did not complete in time.
+  template<typename Issue>
+  __device__ __forceinline__ bool run_mma(TrainShared& s, unsigned& phase, Issue issue)
+  {
+    umma::fence_before_sync();
+    umma::fence_async_shared();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      umma::fence_after_sync();
+      issue();
+      umma::commit(&s.bar);
+    }
+    const bool failed = __syncthreads_or(!umma::mbar_wait(&s.bar, phase, train_wait_limit));
+    phase ^= 1u;
+    umma::fence_after_sync();
+    return !failed;
+  }
+
+  // Forward and backward passes over 128-record tiles on the fifth-generation tensor cores, one
+  // record per thread: tcgen05.mma issued by thread 0 from shared-memory tiles into TMEM (the
+  // 128 x 32 layer outputs, then dH1 = dZ2 W2, then the weight gradients accumulated over the
+  // CTA's tiles), tcgen05.ld back per row; bias, ReLU, the output unit and the loss on the CUDA
+  // cores with the same bf16 rounding points as the inference.
+  __global__ void __launch_bounds__(train_rows) mlp_train_kernel(TrainParams p)
+  {
+    extern __shared__ __align__(128) unsigned char train_smem[];
+    TrainShared& s = *reinterpret_cast<TrainShared*>(train_smem);
+    const unsigned tid = threadIdx.x, warp = tid >> 5;
     const MlpModelDevice& m = *p.model;
-    const unsigned n_tiles = (p.batch + 15) / 16;
-
-    float gw1[2][2][4] = {}, gw2[2][4][4] = {}, gb1[4][2] = {}, gb2[4][2] = {}, gw3[4][2] = {};
-    float gb3 = 0.0f, loss = 0.0f;
-    for (unsigned t = blockIdx.x * warps + (threadIdx.x >> 5); t < n_tiles; t += gridDim.x * warps) {
-      const unsigned r0 = 16 * t + g, r1 = r0 + 8;
-      const bool v0 = r0 < p.batch, v1 = r1 < p.batch;
-      const SeedRecord* rec0 = p.records + p.first + (v0 ? r0 : 0);
-      const SeedRecord* rec1 = p.records + p.first + (v1 ? r1 : 0);
-      uint32_t x[4];
-      x[0] = pack_bf16(train_input(m, rec0, v0, 2 * c), train_input(m, rec0, v0, 2 * c + 1));
-      x[1] = pack_bf16(train_input(m, rec1, v1, 2 * c), train_input(m, rec1, v1, 2 * c + 1));
-      x[2] = pack_bf16(train_input(m, rec0, v0, 2 * c + 8), train_input(m, rec0, v0, 2 * c + 9));
-      x[3] = pack_bf16(train_input(m, rec1, v1, 2 * c + 8), train_input(m, rec1, v1, 2 * c + 9));
-
-      float h1[4][4], h2[4][4], lg, lg8;
-      uint32_t a2[2][4], a3[2][4];
-      mlp_forward_tile(p.model, x, h1, a2, h2, a3, lg, lg8);
-      const float z0 = __shfl_sync(0xFFFFFFFFu, lg, lane & ~3u);
-      const float z1 = __shfl_sync(0xFFFFFFFFu, lg8, lane & ~3u);
-
-      // d loss / d logit, per row (weighted binary cross-entropy, mean over the batch)
-      float dz[2] = {0.0f, 0.0f};
-      const float zs[2] = {z0, z1};
-      const bool vs[2] = {v0, v1};
-      const SeedRecord* rs[2] = {rec0, rec1};
-#pragma unroll
-      for (unsigned q = 0; q < 2; ++q) {
-        if (!vs[q]) continue;
-        const float y = __ldg(&rs[q]->label);
-        const float w = y > 0.5f ? p.pos_weight : 1.0f;
-        const float z = zs[q];
-        const float prob = 1.0f / (1.0f + expf(-z));
-        dz[q] = w * (prob - y) * p.inv_batch;
-        if (c == 0) loss += w * (fmaxf(z, 0.0f) - z * y + log1pf(expf(-fabsf(z))));
-      }
-      if (c == 0) gb3 += dz[0] + dz[1];
-
-      // layer 3: dW3 = sum dz * a3, dH2 = dz * W3, dZ2 = dH2 where h2 > 0
-      float d2[4][4];
-#pragma unroll
-      for (unsigned j = 0; j < 4; ++j) {
-        const uint32_t top = a3[j >> 1][(j & 1u) ? 2 : 0], bottom = a3[j >> 1][(j & 1u) ? 3 : 1];
-        gw3[j][0] += dz[0] * bf16_lo(top) + dz[1] * bf16_lo(bottom);
-        gw3[j][1] += dz[0] * bf16_hi(top) + dz[1] * bf16_hi(bottom);
-        const float wl = __ldg(&m.w3f[8 * j + 2 * c]), wh = __ldg(&m.w3f[8 * j + 2 * c + 1]);
-        d2[j][0] = h2[j][0] > 0.0f ? dz[0] * wl : 0.0f;
-        d2[j][1] = h2[j][1] > 0.0f ? dz[0] * wh : 0.0f;
-        d2[j][2] = h2[j][2] > 0.0f ? dz[1] * wl : 0.0f;
-        d2[j][3] = h2[j][3] > 0.0f ? dz[1] * wh : 0.0f;
-        gb2[j][0] += d2[j][0] + d2[j][2];
-        gb2[j][1] += d2[j][1] + d2[j][3];
-      }
-      uint32_t e2[4][2];
-#pragma unroll
-      for (unsigned j = 0; j < 4; ++j) {
-        e2[j][0] = pack_bf16(d2[j][0], d2[j][1]);
-        e2[j][1] = pack_bf16(d2[j][2], d2[j][3]);
-      }
-      // dW2 += dZ2^T a2 (A: dZ2 transposed, B: a2 transposed into k-major pairs)
-#pragma unroll
-      for (unsigned mt = 0; mt < 2; ++mt) {
-        const uint32_t A[4] = {movmatrix_trans(e2[2 * mt][0]), movmatrix_trans(e2[2 * mt + 1][0]),
-                               movmatrix_trans(e2[2 * mt][1]), movmatrix_trans(e2[2 * mt + 1][1])};
-#pragma unroll
-        for (unsigned nt = 0; nt < 4; ++nt) {
-          const uint32_t b0 = movmatrix_trans(a2[nt >> 1][(nt & 1u) ? 2 : 0]);
-          const uint32_t b1 = movmatrix_trans(a2[nt >> 1][(nt & 1u) ? 3 : 1]);
-          mma_bf16(gw2[mt][nt], A, b0, b1);
-        }
-      }
-      // dH1 = dZ2 W2 (A: dZ2 in C-to-A layout, B: W2 transposed), dZ1 = dH1 where h1 > 0
-      float d1[4][4] = {};
-#pragma unroll
-      for (unsigned s = 0; s < 2; ++s) {
-        const uint32_t A[4] = {e2[2 * s][0], e2[2 * s][1], e2[2 * s + 1][0], e2[2 * s + 1][1]};
-#pragma unroll
-        for (unsigned nt = 0; nt < 4; ++nt)
-          mma_bf16(d1[nt], A, __ldg(&m.w2t[8 * nt + g][8 * s + c]), __ldg(&m.w2t[8 * nt + g][8 * s + 4 + c]));
-      }
-      uint32_t e1[4][2];
-#pragma unroll
-      for (unsigned j = 0; j < 4; ++j) {
-#pragma unroll
-        for (unsigned q = 0; q < 4; ++q)
-          d1[j][q] = h1[j][q] > 0.0f ? d1[j][q] : 0.0f;
-        gb1[j][0] += d1[j][0] + d1[j][2];
-        gb1[j][1] += d1[j][1] + d1[j][3];
-        e1[j][0] = pack_bf16(d1[j][0], d1[j][1]);
-        e1[j][1] = pack_bf16(d1[j][2], d1[j][3]);
-      }
-      // dW1 += dZ1^T x
-#pragma unroll
-      for (unsigned mt = 0; mt < 2; ++mt) {
-        const uint32_t A[4] = {movmatrix_trans(e1[2 * mt][0]), movmatrix_trans(e1[2 * mt + 1][0]),
-                               movmatrix_trans(e1[2 * mt][1]), movmatrix_trans(e1[2 * mt + 1][1])};
-#pragma unroll
-        for (unsigned nf = 0; nf < 2; ++nf)
-          mma_bf16(gw1[mt][nf], A, movmatrix_trans(x[nf ? 2 : 0]), movmatrix_trans(x[nf ? 3 : 1]));
-      }
+    if (warp == 0) umma::alloc(&s.tmem, train_tmem_columns);
+    if (tid == 0) umma::mbar_init(&s.bar, 1);
+    for (unsigned i = tid; i < sizeof(s.ga) / 4; i += blockDim.x)
+      reinterpret_cast<uint32_t*>(s.ga)[i] = 0u;
+    for (unsigned i = tid; i < 3 * mlp_hidden + 2; i += blockDim.x)
+      s.sums[i] = 0.0f;
+    for (unsigned i = tid; i < mlp_hidden * (mlp_k1 / 2); i += blockDim.x)
+      put_pair(s.w1, i / (mlp_k1 / 2), 2 * (i % (mlp_k1 / 2)), mlp_k1, __ldg(&m.w1[0][0] + i));
+    for (unsigned i = tid; i < mlp_hidden * (mlp_hidden / 2); i += blockDim.x) {
+      put_pair(s.w2, i / (mlp_hidden / 2), 2 * (i % (mlp_hidden / 2)), mlp_hidden, __ldg(&m.w2[0][0] + i));
+      put_pair(s.w2t, i / (mlp_hidden / 2), 2 * (i % (mlp_hidden / 2)), mlp_hidden, __ldg(&m.w2t[0][0] + i));
     }
-
-    // reduce: per-lane partial sums into the CTA's shared copy
-    float* bg = block_grads;
-#pragma unroll
-    for (unsigned mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (unsigned nf = 0; nf < 2; ++nf)
-#pragma unroll
-        for (unsigned q = 0; q < 4; ++q) {
-          const unsigned o = 16 * mt + g + ((q & 2u) ? 8 : 0), f = 8 * nf + 2 * c + (q & 1u);
-          if (f < mlp_features) atomicAdd(&bg[off_w1 + o * mlp_features + f], gw1[mt][nf][q]);
-        }
-#pragma unroll
-    for (unsigned mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (unsigned nt = 0; nt < 4; ++nt)
-#pragma unroll
-        for (unsigned q = 0; q < 4; ++q) {
-          const unsigned o = 16 * mt + g + ((q & 2u) ? 8 : 0), i = 8 * nt + 2 * c + (q & 1u);
-          atomicAdd(&bg[off_w2 + o * mlp_hidden + i], gw2[mt][nt][q]);
-        }
-#pragma unroll
-    for (unsigned j = 0; j < 4; ++j)
-#pragma unroll
-      for (unsigned q = 0; q < 2; ++q) {
-        atomicAdd(&bg[off_b1 + 8 * j + 2 * c + q], gb1[j][q]);
-        atomicAdd(&bg[off_b2 + 8 * j + 2 * c + q], gb2[j][q]);
-        atomicAdd(&bg[off_w3 + 8 * j + 2 * c + q], gw3[j][q]);
-      }
-    if (c == 0) {
-      atomicAdd(&bg[off_b3], gb3);
-      atomicAdd(&bg[n_params], loss);
-    }
+    umma::fence_before_sync();
     __syncthreads();
-    for (unsigned i = threadIdx.x; i < n_params; i += blockDim.x)
-      atomicAdd(&p.grads[i], block_grads[i]);
-    if (threadIdx.x == 0) atomicAdd(p.loss, block_grads[n_params] * p.inv_batch);
+    umma::fence_after_sync();
+    const uint32_t tmem = s.tmem, lane_base = (warp * 32u) << 16;
+    const uint32_t t_out = tmem, t_grad = tmem + 32u;
+    constexpr uint32_t id32 = umma::idesc_bf16(train_rows, mlp_hidden);
+    constexpr uint32_t id48 = umma::idesc_bf16(train_rows, 48);
+    unsigned phase = 0;
+    bool ok = true, grads_started = false;
+    float gb1[mlp_hidden] = {}, gb2[mlp_hidden] = {}, gw3[mlp_hidden] = {};
+    float gb3 = 0.0f, loss = 0.0f;
+    const unsigned n_tiles = (p.batch + train_rows - 1) / train_rows;
+    for (unsigned t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+      const unsigned r = t * train_rows + tid;
+      const bool valid = r < p.batch;
+      const SeedRecord* rec = p.records + p.first + (valid ? r : 0);
+      // inputs: row tid of x, column tid of x^T (rows 32..47 of B)
+#pragma unroll
+      for (unsigned i = 0; i < mlp_k1; i += 2) {
+        const uint32_t pr = pack_bf16(train_input(m, rec, valid, i), train_input(m, rec, valid, i + 1));
+        put_pair(s.x, tid, i, mlp_k1, pr);
+        put_half(s.gb, 32 + i, tid, train_rows, pr);
+        put_half(s.gb, 33 + i, tid, train_rows, pr >> 16);
+      }
+      // layer 1
+      ok = run_mma(s, phase, [&] { umma::mma(t_out, umma::desc(s.x, mlp_k1, 0), umma::desc(s.w1, mlp_k1, 0), id32, false); });
+      if (!ok) break;
+      float h1[mlp_hidden];
+      umma::load32(t_out + lane_base, h1);
+#pragma unroll
+      for (unsigned i = 0; i < mlp_hidden; i += 2) {
+        h1[i] += __ldg(&m.b1[i]);
+        h1[i + 1] += __ldg(&m.b1[i + 1]);
+        const uint32_t pr = pack_bf16(relu(h1[i]), relu(h1[i + 1]));
+        put_pair(s.a2, tid, i, mlp_hidden, pr);
+        put_half(s.gb, i, tid, train_rows, pr);
+        put_half(s.gb, i + 1, tid, train_rows, pr >> 16);
+      }
+      // layer 2
+      ok = run_mma(s, phase, [&] {
+        umma::mma(t_out, umma::desc(s.a2, mlp_hidden, 0), umma::desc(s.w2, mlp_hidden, 0), id32, false);
+        umma::mma(t_out, umma::desc(s.a2, mlp_hidden, 1), umma::desc(s.w2, mlp_hidden, 1), id32, true);
+      });
+      if (!ok) break;
+      float h2[mlp_hidden];
+      umma::load32(t_out + lane_base, h2);
+      // output unit, loss, dZ2
+      float z = __ldg(&m.b3);
+#pragma unroll
+      for (unsigned i = 0; i < mlp_hidden; ++i) {
+        h2[i] += __ldg(&m.b2[i]);
+        z += bf16_lo(pack_bf16(relu(h2[i]), 0.0f)) * __ldg(&m.w3f[i]);
+      }
+      float dz = 0.0f;
+      if (valid) {
+        const float y = __ldg(&rec->label);
+        const float w = y > 0.5f ? p.pos_weight : 1.0f;
+        const float prob = 1.0f / (1.0f + expf(-z));
+        dz = w * (prob - y) * p.inv_batch;
+        loss += w * (fmaxf(z, 0.0f) - z * y + log1pf(expf(-fabsf(z))));
+      }
+      gb3 += dz;
+#pragma unroll
+      for (unsigned i = 0; i < mlp_hidden; i += 2) {
+        const float a0 = bf16_lo(pack_bf16(relu(h2[i]), 0.0f)), a1 = bf16_lo(pack_bf16(relu(h2[i + 1]), 0.0f));
+        gw3[i] += dz * a0;
+        gw3[i + 1] += dz * a1;
+        const float d0 = h2[i] > 0.0f ? dz * __ldg(&m.w3f[i]) : 0.0f;
+        const float d1 = h2[i + 1] > 0.0f ? dz * __ldg(&m.w3f[i + 1]) : 0.0f;
+        gb2[i] += d0;
+        gb2[i + 1] += d1;
+        const uint32_t pr = pack_bf16(d0, d1);
+        put_pair(s.e2, tid, i, mlp_hidden, pr);
+        put_half(s.ga, i, tid, train_rows, pr);
+        put_half(s.ga, i + 1, tid, train_rows, pr >> 16);
+      }
+      // dH1 = dZ2 W2 (B: W2^T, K-major over the layer-2 units)
+      ok = run_mma(s, phase, [&] {
+        umma::mma(t_out, umma::desc(s.e2, mlp_hidden, 0), umma::desc(s.w2t, mlp_hidden, 0), id32, false);
+        umma::mma(t_out, umma::desc(s.e2, mlp_hidden, 1), umma::desc(s.w2t, mlp_hidden, 1), id32, true);
+      });
+      if (!ok) break;
+      float d1[mlp_hidden];
+      umma::load32(t_out + lane_base, d1);
+#pragma unroll
+      for (unsigned i = 0; i < mlp_hidden; ++i) {
+        const float v = h1[i] > 0.0f ? d1[i] : 0.0f;
+        gb1[i] += v;
+        put_bf16(s.ga, 32 + i, tid, train_rows, v);
+      }
+      // weight gradients of both layers, accumulated in TMEM over the tiles
+      const bool acc = grads_started;
+      ok = run_mma(s, phase, [&] {
+#pragma unroll
+        for (unsigned k = 0; k < train_rows / 16; ++k)
+          umma::mma(t_grad, umma::desc(s.ga, train_rows, k), umma::desc(s.gb, train_rows, k), id48, acc || k > 0);
+      });
+      grads_started = true;
+    }
+    // per-thread sums into the CTA's sums, then the global gradient
+#pragma unroll
+    for (unsigned i = 0; i < mlp_hidden; ++i) {
+      atomicAdd(&s.sums[i], gb1[i]);
+      atomicAdd(&s.sums[mlp_hidden + i], gb2[i]);
+      atomicAdd(&s.sums[2 * mlp_hidden + i], gw3[i]);
+    }
+    atomicAdd(&s.sums[3 * mlp_hidden], gb3);
+    atomicAdd(&s.sums[3 * mlp_hidden + 1], loss);
+    __syncthreads();
+    if (ok && grads_started) {
+      float g[32];
+      if (warp == 0) { // rows 0..31: dW2[j][i], TMEM columns 32..63
+        umma::load32(t_grad + lane_base, g);
+        for (unsigned i = 0; i < mlp_hidden; ++i)
+          atomicAdd(&p.grads[off_w2 + (tid & 31u) * mlp_hidden + i], g[i]);
+      }
+      else if (warp == 1) { // rows 32..63: dW1[j][f], TMEM columns 64..75
+        umma::load32(t_grad + lane_base + 32u, g);
+        for (unsigned f = 0; f < mlp_features; ++f)
+          atomicAdd(&p.grads[off_w1 + (tid & 31u) * mlp_features + f], g[f]);
+      }
+    }
+    else if (!ok) {
+      // an MMA chain that did not complete in time: let it drain (bounded), then mark the step
+      // failed with a NaN in b3's gradient, which the optimiser carries into the weights
+      umma::mbar_wait(&s.bar, phase ^ 1u, train_wait_limit);
+      if (tid == 0) p.grads[off_b3] = __int_as_float(0x7FC00000);
+    }
+    for (unsigned i = tid; i < mlp_hidden; i += blockDim.x) {
+      atomicAdd(&p.grads[off_b1 + i], s.sums[i]);
+      atomicAdd(&p.grads[off_b2 + i], s.sums[mlp_hidden + i]);
+      atomicAdd(&p.grads[off_w3 + i], s.sums[2 * mlp_hidden + i]);
+    }
+    if (tid == 0) {
+      atomicAdd(&p.grads[off_b3], s.sums[3 * mlp_hidden]);
+      atomicAdd(p.loss, s.sums[3 * mlp_hidden + 1] * p.inv_batch);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::dealloc(tmem, train_tmem_columns);
   }
 
 } // namespace velo
@@ -376,10 +446,10 @@ namespace {
     p.model = t->model;
     p.grads = t->grads;
     p.loss = t->loss;
-    const unsigned tiles = (batch + 15) / 16;
-    const unsigned grid = std::min<unsigned>((tiles + 7) / 8, unsigned(t->sm_count) * 4u);
+    const unsigned tiles = (batch + velo::train_rows - 1) / velo::train_rows;
+    const unsigned grid = std::min<unsigned>(tiles, unsigned(t->sm_count));
     VELO_TRY(cudaMemsetAsync(t->loss, 0, sizeof(float), s));
-    velo::mlp_train_kernel<<<grid, 256, 0, s>>>(p);
+    velo::mlp_train_kernel<<<grid, velo::train_rows, sizeof(velo::TrainShared), s>>>(p);
     VELO_TRY(cudaGetLastError());
     return VELO_OK;
   }
@@ -397,6 +467,12 @@ VeloStatus velo_seed_trainer_create(const VeloSeedModel* init, float learning_ra
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&t->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  const cudaError_t attr = cudaFuncSetAttribute(
+    velo::mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(velo::TrainShared)));
+  if (attr != cudaSuccess) {
+    delete t;
+    return fail(VELO_ERR_CUDA, std::string("training kernel shared memory: ") + cudaGetErrorString(attr));
+  }
   float* block = nullptr;
   cudaError_t e = cudaMalloc(&block, sizeof(float) * (4 * velo::n_params + 1));
   if (e != cudaSuccess) {

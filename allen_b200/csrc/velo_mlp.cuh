@@ -27,6 +27,7 @@ namespace velo {
   constexpr unsigned mlp_features = 12; // inputs of the network
   constexpr unsigned mlp_k1 = 16;       // inputs padded to one k-step
   constexpr unsigned mlp_hidden = 32;   // units of each hidden layer
+  constexpr unsigned train_rows = 128;  // records per tensor-core tile of the training kernel
 
   // The network as the kernels read it: bf16 weights in [out][in] order (PyTorch's Linear
   // layout, so a B fragment pair is one aligned 32-bit word), fp32 biases and the feature
