@@ -447,7 +447,8 @@ namespace {
     p.grads = t->grads;
     p.loss = t->loss;
     const unsigned tiles = (batch + velo::train_rows - 1) / velo::train_rows;
-    const unsigned grid = std::min<unsigned>(tiles, unsigned(t->sm_count));
+    // two CTAs per SM (256 registers a thread, 71 KB of tiles each) overlap each other's MMA waits
+    const unsigned grid = std::min<unsigned>(tiles, 2u * unsigned(t->sm_count));
     VELO_TRY(cudaMemsetAsync(t->loss, 0, sizeof(float), s));
     velo::mlp_train_kernel<<<grid, velo::train_rows, sizeof(velo::TrainShared), s>>>(p);
     VELO_TRY(cudaGetLastError());
