@@ -252,21 +252,25 @@ namespace velo {
     return static_cast<int>(i);
   }
 
-  // The bucket tables of an event's 26 module pairs (one CTA; phis event-relative).
+  // The bucket table of one module pair, hits [s0, s0 + cnt) (one CTA; phi_of(i) = phi of
+  // the event's hit i).
+  template<typename PhiOf>
+  __device__ __forceinline__ void build_bucket_table_of(uint16_t* t, PhiOf phi_of, unsigned s0, unsigned cnt)
+  {
+    for (unsigned i = threadIdx.x; i <= cnt; i += blockDim.x) {
+      const unsigned lo = i == 0 ? 0u : bucket_of(phi_of(s0 + i - 1)) + 1;
+      const unsigned hi = i == cnt ? n_buckets : bucket_of(phi_of(s0 + i));
+      for (unsigned b = lo; b <= hi; ++b)
+        t[b] = static_cast<uint16_t>(i);
+    }
+  }
+
+  // The bucket tables of an event's 26 module pairs (phis event-relative).
   __device__ __forceinline__ void build_bucket_tables(
     uint16_t (*table)[n_buckets + 1], const int16_t* phis, const unsigned* start, const unsigned* num, unsigned hit_offset)
   {
-    for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
-      const unsigned s0 = start[mp] - hit_offset;
-      const unsigned cnt = num[mp];
-      uint16_t* t = table[mp];
-      for (unsigned i = threadIdx.x; i <= cnt; i += blockDim.x) {
-        const unsigned lo = i == 0 ? 0u : bucket_of(phis[s0 + i - 1]) + 1;
-        const unsigned hi = i == cnt ? n_buckets : bucket_of(phis[s0 + i]);
-        for (unsigned b = lo; b <= hi; ++b)
-          t[b] = static_cast<uint16_t>(i);
-      }
-    }
+    for (unsigned mp = 0; mp < n_module_pairs; ++mp)
+      build_bucket_table_of(table[mp], [phis](unsigned i) { return phis[i]; }, start[mp] - hit_offset, num[mp]);
   }
 
   // ---- learned seed gate (velo_gate.cu): one byte per hit, 1 = searched as a seed's middle hit ----
@@ -309,7 +313,7 @@ namespace velo {
   constexpr unsigned kalman_warp_hits = 368; // hits of a warp's 32 tracks staged in shared memory (4.4 KB)
   constexpr unsigned scan_threads = 1024;
   constexpr unsigned consolidate_threads = 256;
-  constexpr unsigned search_hit_bytes = 15; // x, y, z, phi, flags per staged hit
+  constexpr unsigned search_hit_bytes = 16; // one record (x, y, z, phi, flags) per staged hit
 
 } // namespace velo
 

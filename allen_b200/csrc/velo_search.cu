@@ -6,10 +6,11 @@
 // ThreeHitTracksFilter.cu:48-169.
 //
 // Design.
-//  * The event's sorted hits are staged once as structure-of-arrays (x, y, z, phi and a
-//    flag byte holding hit_used and the module parity that forwarding needs) in shared
-//    memory: 15 bytes per hit.  Events above the shared-memory capacity use the same
-//    layout in a global scratch slice, through the same generic pointers.
+//  * The event's sorted hits are staged once as 16-byte records (x, y, z, phi and a flag
+//    byte holding hit_used and the module parity that forwarding needs), so that every
+//    hit a walk visits costs one vector load: in shared memory, or for events above the
+//    shared-memory capacity (and in the tuned launch, every event) in a global scratch
+//    slice that stays in L2, through the same code.
 //  * Within a step every seed candidate (h1) and every track to follow is independent:
 //    seeding only reads hit_used, forwarding only writes it, and each track to follow
 //    owns its track.  Seeding runs LPH lanes per h1: the lanes walk the pendulum of h0
@@ -38,12 +39,13 @@ namespace velo {
   constexpr uint8_t flag_used = 1;
   constexpr uint8_t flag_odd_module = 2;
   constexpr unsigned flat_slots = 1024; // (h1, h0 candidate) slots per chunk of the flat seeding
+  constexpr unsigned pendulum_capacity = 512; // module pairs of up to this many hits get the unused-hit index
 
   struct ModulePair {
     unsigned hit_start;
     unsigned hit_num;
     float z[2];
-    unsigned mp;
+    unsigned table; // slot of its bucket table: the module pair's index % 3
   };
 
   struct SearchShared {
@@ -51,12 +53,13 @@ namespace velo {
     unsigned track_hits;       // sum of hitsNum over the >= 4 hit tracks
     uint32_t tail[max_tail_tracks]; // last two hits of a track (hit[n-2] | hit[n-1] << 16)
     uint8_t tail_n[max_tail_tracks];
-    uint16_t bucket[n_module_pairs][n_buckets + 1];
+    // bucket tables of the three module pairs a step reads, built one per step
+    uint16_t bucket[3][n_buckets + 1];
   };
 
   // Shared state of the flat seeding variant: one slot per (h1, candidate order).
   template<unsigned SLOTS>
-  struct SearchSharedFlatT : SearchShared {
+  struct SearchSharedFlatBase : SearchShared {
     static constexpr unsigned slots = SLOTS;
     // (h0, h1) doublets of a chunk, packed by pack_doublet(), then overwritten in place
     // with the best scatter found for the doublet
@@ -65,13 +68,22 @@ namespace velo {
       float fit;
     } slot[SLOTS];
     uint16_t res_h2[SLOTS];
+    // The unused hits of the seeding's previous module pair: how many lie before each
+    // position (the last entry: all of them), and their positions in phi order
+    uint16_t unused_before[pendulum_capacity + 1];
+    uint16_t unused_at[pendulum_capacity];
+  };
+  template<unsigned SLOTS, bool GATED>
+  struct SearchSharedFlatT : SearchSharedFlatBase<SLOTS> {};
+  template<unsigned SLOTS>
+  struct SearchSharedFlatT<SLOTS, true> : SearchSharedFlatBase<SLOTS> {
     uint16_t cand_list[SLOTS]; // the window's searched candidates (index in the window), h1 order
   };
   // flat-seeding kernels: 512 slots for 128 threads (chunks of 64 or 128 h1), which with the
-  // ring in global scratch leaves room for twelve CTAs per SM
-  template<unsigned THREADS>
+  // ring in global scratch leaves room for sixteen CTAs per SM
+  template<unsigned THREADS, bool GATED = false>
   using SearchSharedFlatPlain =
-    SearchSharedFlatT<(THREADS <= 64 ? flat_slots / 4 : (THREADS <= 128 ? flat_slots / 2 : flat_slots))>;
+    SearchSharedFlatT<(THREADS <= 64 ? flat_slots / 4 : (THREADS <= 128 ? flat_slots / 2 : flat_slots)), GATED>;
 
   // Packed doublet: h0 | h1 index in the chunk << 16 | rank << 25 | (found - 1) << 28
   __device__ __forceinline__ uint32_t pack_doublet(unsigned h0, unsigned h1_local, unsigned rank, unsigned found)
@@ -79,13 +91,45 @@ namespace velo {
     return h0 | (h1_local << 16) | (rank << 25) | ((found - 1u) << 28);
   }
 
-  struct HitsSoA {
-    const float* x;
-    const float* y;
-    const float* z;
-    const int16_t* phi;
-    uint8_t* flags;
+  // A staged hit, unpacked from its 16-byte record.
+  struct Hit {
+    float x, y, z;
+    int16_t phi;
+    unsigned flags;
   };
+
+  // The event's staged hits: one 16-byte record per hit (x, y, z as fp32 bits, then phi in
+  // bits 0-15 and the flags in bits 16-23 of the fourth word), so that a candidate costs
+  // one vector load instead of one load per field.
+  struct Hits {
+    uint4* r;
+    __device__ __forceinline__ Hit operator[](unsigned i) const
+    {
+      const uint4 v = r[i];
+      return Hit {__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), static_cast<int16_t>(v.w & 0xFFFFu),
+                  (v.w >> 16) & 0xFFu};
+    }
+    __device__ __forceinline__ int16_t phi(unsigned i) const { return reinterpret_cast<const int16_t*>(r + i)[6]; }
+    __device__ __forceinline__ unsigned flags(unsigned i) const { return reinterpret_cast<const uint8_t*>(r + i)[14]; }
+    __device__ __forceinline__ void mark_used(unsigned i) const { reinterpret_cast<uint8_t*>(r + i)[14] |= flag_used; }
+  };
+
+  // Position i < n of the pendulum around p0 in [0, n]: p0, p0 + 1, p0 - 1, p0 + 2, ...
+  // with one wrap (SearchByTriplet.cu:351-370).
+  __device__ __forceinline__ unsigned pendulum(int p0, unsigned i, int n)
+  {
+    const int pos = p0 + ((i & 1u) ? static_cast<int>((i + 1) / 2) : -static_cast<int>(i / 2));
+    return static_cast<unsigned>(pos < 0 ? pos + n : (pos >= n ? pos - n : pos));
+  }
+
+  // leftmost() over the staged hits [start, start + n) of a module pair.
+  __device__ __forceinline__ int leftmost_hit(const uint16_t* table, const Hits& h, unsigned start, unsigned n, int16_t value)
+  {
+    unsigned i = table[bucket_of(value)];
+    while (i < n && h.phi(start + i) < value)
+      ++i;
+    return static_cast<int>(i);
+  }
 
   // The event's counters (the reference's dev_atomics_velo and track count), kept in
   // registers: every thread holds the same values and advances them by scan totals.
@@ -140,7 +184,7 @@ namespace velo {
   __device__ __forceinline__ Extrapolation extrapolate(
     const Constants& k,
     const SearchShared& s,
-    const HitsSoA& h,
+    const Hits& h,
     const ModulePair& next,
     float h0x,
     float h0y,
@@ -156,7 +200,7 @@ namespace velo {
     x.phi = hit_phi_16(k, xp, yp);
     const int16_t lo = static_cast<int16_t>(x.phi - static_cast<int16_t>(k.phi_tolerance_i16));
     // find_forward_candidate returns the index as int16
-    x.start = static_cast<int16_t>(leftmost(s.bucket[next.mp], h.phi + next.hit_start, next.hit_num, lo));
+    x.start = static_cast<int16_t>(leftmost_hit(s.bucket[next.table], h, next.hit_start, next.hit_num, lo));
     return x;
   }
 
@@ -165,7 +209,7 @@ namespace velo {
   __device__ __forceinline__ void seed_candidate(
     const Constants& k,
     const SearchShared& s,
-    const HitsSoA& h,
+    const Hits& h,
     const ModulePair& prev,
     const ModulePair& next,
     float h1x,
@@ -179,7 +223,8 @@ namespace velo {
     unsigned& best_h2)
   {
     const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
-    const float h0x = h.x[h0], h0y = h.y[h0], h0z = h.z[h0];
+    const Hit a = h[h0];
+    const float h0x = a.x, h0y = a.y, h0z = a.z;
     const float td = __fdiv_rn(1.0f, h1z - h0z);
     const float txn = h1x - h0x;
     const float tyn = h1y - h0y;
@@ -190,13 +235,14 @@ namespace velo {
     unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
     for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
       const unsigned h2 = next.hit_start + idx;
-      if (phi_outside(h.phi[h2], f.phi, tol)) break;
-      if (h.flags[h2] & flag_used) continue;
-      const float dz = h.z[h2] - h0z;
+      const Hit b = h[h2];
+      if (phi_outside(b.phi, f.phi, tol)) break;
+      if (b.flags & flag_used) continue;
+      const float dz = b.z - h0z;
       const float predx = h0x + tx * dz;
       const float predy = h0y + ty * dz;
-      const float dx = predx - h.x[h2];
-      const float dy = predy - h.y[h2];
+      const float dx = predx - b.x;
+      const float dy = predy - b.y;
       const float scatter = dx * dx + dy * dy;
       if (scatter < best_fit) {
         best_fit = scatter;
@@ -210,7 +256,7 @@ namespace velo {
   // Seeding over the current module pair (SearchByTriplet.cu:298-446), LPH lanes per h1.
   template<unsigned LPH>
   __device__ __forceinline__ void seeding(
-    SearchShared& s, uint64_t* ring, Counters& cnt, const Constants& k, const HitsSoA& h, const ModulePair* md,
+    SearchShared& s, uint64_t* ring, Counters& cnt, const Constants& k, const Hits& h, const ModulePair* md,
     unsigned n_candidates)
   {
     const ModulePair prev = md[0], cur = md[1], next = md[2];
@@ -222,12 +268,13 @@ namespace velo {
     for (unsigned c0 = 0; c0 < cur.hit_num; c0 += groups) {
       const unsigned r = c0 + g;
       const unsigned h1 = cur.hit_start + r;
-      const bool valid = r < cur.hit_num && !(h.flags[h1] & flag_used);
+      const bool valid = r < cur.hit_num && !(h.flags(h1) & flag_used);
       float best_fit = k.max_scatter;
       unsigned best_c = 0xFFFFFFFFu, best_h0 = 0, best_h2 = 0;
       if (valid) {
-        const float h1x = h.x[h1], h1y = h.y[h1], h1z = h.z[h1];
-        const int p0 = leftmost(s.bucket[prev.mp], h.phi + prev.hit_start, prev.hit_num, h.phi[h1]);
+        const Hit b = h[h1];
+        const float h1x = b.x, h1y = b.y, h1z = b.z;
+        const int p0 = leftmost_hit(s.bucket[prev.table], h, prev.hit_start, prev.hit_num, b.phi);
         const int n_prev = static_cast<int>(prev.hit_num);
         unsigned found = 0;
         for (unsigned i0 = 0; i0 < prev.hit_num && found < n_candidates; i0 += LPH) {
@@ -239,7 +286,7 @@ namespace velo {
             const int pos = p0 + ((i & 1u) ? static_cast<int>((i + 1) / 2) : -static_cast<int>(i / 2));
             const int in_bounds = pos < 0 ? pos + n_prev : (pos >= n_prev ? pos - n_prev : pos);
             h0 = prev.hit_start + static_cast<unsigned>(in_bounds);
-            ok = !(h.flags[h0] & flag_used);
+            ok = !(h.flags(h0) & flag_used);
           }
           const unsigned ballot = (__ballot_sync(gmask, ok) & gmask) >> lane0;
           const unsigned rank = __popc(ballot & ((1u << l) - 1u));
@@ -298,7 +345,7 @@ namespace velo {
     uint64_t* ring,
     Counters& cnt,
     const Constants& k,
-    const HitsSoA& h,
+    const Hits& h,
     const ModulePair* md,
     unsigned n_candidates,
     const uint8_t* gate,
@@ -308,6 +355,23 @@ namespace velo {
     const unsigned per_chunk = min(blockDim.x, Flat::slots / n_candidates);
     const int n_prev = static_cast<int>(prev.hit_num);
     const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
+    // The unused-hit index of the previous module pair (its used flags do not change
+    // during the seeding), when a module pair has hits to seed and fits the index
+    const bool indexed = cur.hit_num > 0 && prev.hit_num <= pendulum_capacity;
+    unsigned n_unused = 0;
+    if (indexed) {
+      for (unsigned i0 = 0; i0 < prev.hit_num; i0 += blockDim.x) {
+        const unsigned i = i0 + threadIdx.x;
+        const bool unused = i < prev.hit_num && !(h.flags(prev.hit_start + i) & flag_used);
+        unsigned total;
+        const unsigned before = n_unused + scan1(s, cnt, unused ? 1u : 0u, total);
+        if (i < prev.hit_num) s.unused_before[i] = static_cast<uint16_t>(before);
+        if (unused) s.unused_at[before] = static_cast<uint16_t>(i);
+        n_unused += total;
+      }
+      if (threadIdx.x == 0) s.unused_before[prev.hit_num] = static_cast<uint16_t>(n_unused);
+      __syncthreads();
+    }
     for (unsigned c0 = 0; c0 < cur.hit_num; c0 += per_chunk) {
       const unsigned n_h1 = min(per_chunk, cur.hit_num - c0);
       // Gated: the window's candidates compacted in h1 order (its unused hits that the gate
@@ -320,7 +384,7 @@ namespace velo {
         unsigned n_searched;
         {
           const unsigned hw = cur.hit_start + c0 + threadIdx.x;
-          const bool valid = threadIdx.x < n_h1 && !(h.flags[hw] & flag_used);
+          const bool valid = threadIdx.x < n_h1 && !(h.flags(hw) & flag_used);
           const bool pass = valid && (gate == nullptr || gate[hw] != 0);
           unsigned total;
           const unsigned excl = scan1(s, cnt, (pass ? 1u : 0u) | ((valid ? 1u : 0u) << 16), total);
@@ -336,23 +400,57 @@ namespace velo {
       }
       else {
         hl = threadIdx.x;
-        searched = threadIdx.x < n_h1 && !(h.flags[cur.hit_start + c0 + hl] & flag_used);
+        searched = threadIdx.x < n_h1 && !(h.flags(cur.hit_start + c0 + hl) & flag_used);
       }
       const unsigned h1 = cur.hit_start + c0 + hl;
-      // Phase A: candidates c < 4 in the 16-bit fields of cand_lo, 4..7 in cand_hi
+      // Phase A: candidates c < 4 in the 16-bit fields of cand_lo, 4..7 in cand_hi, the first
+      // n_candidates unused h0 of the pendulum p0, p0 + 1, p0 - 1, p0 + 2, ... (one wrap).
+      // With the unused-hit index, the pendulum's unused hits are the merge of the index's
+      // run from p0 upwards (pendulum step 2d - 1 at offset d > 0, 0 at p0) and its run below
+      // p0 (step 2d at offset d), each wrapping once, taken while the step is below n.
       uint64_t cand_lo = 0, cand_hi = 0;
       unsigned found = 0;
       if (searched) {
-        const int p0 = leftmost(s.bucket[prev.mp], h.phi + prev.hit_start, prev.hit_num, h.phi[h1]);
-        int pos = p0;
-        for (unsigned i = 0; i < prev.hit_num && found < n_candidates; ++i) {
-          pos += (i & 1u) ? static_cast<int>(i) : -static_cast<int>(i);
-          const int in_bounds = pos < 0 ? pos + n_prev : (pos >= n_prev ? pos - n_prev : pos);
-          const unsigned h0 = prev.hit_start + static_cast<unsigned>(in_bounds);
-          if (!(h.flags[h0] & flag_used)) {
+        const int p0 = leftmost_hit(s.bucket[prev.table], h, prev.hit_start, prev.hit_num, h.phi(h1));
+        if (indexed) {
+          const int u = static_cast<int>(n_unused);
+          const int r = s.unused_before[p0];
+          // step and position of the k-th unused hit upwards (k >= r) and downwards (k < r)
+          auto up = [&](int kk, unsigned& pos) {
+            if (kk >= 2 * u) return static_cast<unsigned>(n_prev);
+            const int q = s.unused_at[kk < u ? kk : kk - u];
+            pos = static_cast<unsigned>(q);
+            const int d = (kk < u ? q : q + n_prev) - p0;
+            return d == 0 ? 0u : static_cast<unsigned>(2 * d - 1);
+          };
+          auto down = [&](int kk, unsigned& pos) {
+            if (kk < -u) return static_cast<unsigned>(n_prev);
+            const int q = s.unused_at[kk >= 0 ? kk : kk + u];
+            pos = static_cast<unsigned>(q);
+            return static_cast<unsigned>(2 * (p0 - (kk >= 0 ? q : q - n_prev)));
+          };
+          int ku = r, kd = r - 1;
+          unsigned pu = 0, pd = 0;
+          unsigned iu = up(ku, pu), id = down(kd, pd);
+          while (found < n_candidates) {
+            const bool upward = iu < id;
+            if ((upward ? iu : id) >= prev.hit_num) break;
+            const unsigned h0 = prev.hit_start + (upward ? pu : pd);
             if (found < 4) cand_lo |= uint64_t(h0) << (16 * found);
             else cand_hi |= uint64_t(h0) << (16 * (found - 4));
             ++found;
+            if (upward) iu = up(++ku, pu);
+            else id = down(--kd, pd);
+          }
+        }
+        else {
+          for (unsigned i = 0; i < prev.hit_num && found < n_candidates; ++i) {
+            const unsigned h0 = prev.hit_start + pendulum(p0, i, n_prev);
+            if (!(h.flags(h0) & flag_used)) {
+              if (found < 4) cand_lo |= uint64_t(h0) << (16 * found);
+              else cand_hi |= uint64_t(h0) << (16 * (found - 4));
+              ++found;
+            }
           }
         }
       }
@@ -370,8 +468,9 @@ namespace velo {
         const unsigned hh1 = cur.hit_start + c0 + ((d >> 16) & 0x1FFu);
         float best_fit = k.max_scatter;
         unsigned best_h2 = 0xFFFFu;
-        const float h1x = h.x[hh1], h1y = h.y[hh1], h1z = h.z[hh1];
-        const float h0x = h.x[h0], h0y = h.y[h0], h0z = h.z[h0];
+        const Hit a = h[h0], b = h[hh1];
+        const float h1x = b.x, h1y = b.y, h1z = b.z;
+        const float h0x = a.x, h0y = a.y, h0z = a.z;
         const float td = __fdiv_rn(1.0f, h1z - h0z);
         const float txn = h1x - h0x;
         const float tyn = h1y - h0y;
@@ -381,13 +480,14 @@ namespace velo {
         unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
         for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
           const unsigned h2 = next.hit_start + idx;
-          if (phi_outside(h.phi[h2], f.phi, tol)) break;
-          if (h.flags[h2] & flag_used) continue;
-          const float dz = h.z[h2] - h0z;
+          const Hit c = h[h2];
+          if (phi_outside(c.phi, f.phi, tol)) break;
+          if (c.flags & flag_used) continue;
+          const float dz = c.z - h0z;
           const float predx = h0x + tx * dz;
           const float predy = h0y + ty * dz;
-          const float dx = predx - h.x[h2];
-          const float dy = predy - h.y[h2];
+          const float dx = predx - c.x;
+          const float dy = predy - c.y;
           const float scatter = dx * dx + dy * dy;
           if (scatter < best_fit) {
             best_fit = scatter;
@@ -440,7 +540,7 @@ namespace velo {
     uint64_t* ring,
     Counters& cnt,
     const Constants& k,
-    const HitsSoA& h,
+    const Hits& h,
     const ModulePair& next,
     unsigned prev_ttf,
     unsigned diff_ttf,
@@ -482,9 +582,10 @@ namespace velo {
             nh = 3; // a track that did not fit its container, flagged when created
           }
         }
-        const float h0x = h.x[h0n], h0y = h.y[h0n], h0z = h.z[h0n];
-        const unsigned odd = (h.flags[h0n] & flag_odd_module) ? 1u : 0u;
-        const float h1x = h.x[h1n], h1y = h.y[h1n], h1z = h.z[h1n];
+        const Hit a = h[h0n], b = h[h1n];
+        const float h0x = a.x, h0y = a.y, h0z = a.z;
+        const unsigned odd = (a.flags & flag_odd_module) ? 1u : 0u;
+        const float h1x = b.x, h1y = b.y, h1z = b.z;
         const float td = __fdiv_rn(1.0f, h1z - h0z);
         const float txn = h1x - h0x;
         const float tyn = h1y - h0y;
@@ -495,12 +596,13 @@ namespace velo {
         unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
         for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
           const unsigned h2 = next.hit_start + idx;
-          if (phi_outside(h.phi[h2], f.phi, tol)) break;
-          const float dz = h.z[h2] - h0z;
+          const Hit c = h[h2];
+          if (phi_outside(c.phi, f.phi, tol)) break;
+          const float dz = c.z - h0z;
           const float predx = h0x + tx * dz;
           const float predy = h0y + ty * dz;
-          const float dx = predx - h.x[h2];
-          const float dy = predy - h.y[h2];
+          const float dx = predx - c.x;
+          const float dy = predy - c.y;
           const float scatter = dx * dx + dy * dy;
           if (scatter < best_fit) {
             best_fit = scatter;
@@ -520,12 +622,12 @@ namespace velo {
       if (active) {
         unsigned track_number = tn;
         if (found) {
-          h.flags[best_h2] |= flag_used;
+          h.mark_used(best_h2);
           if (is_seed) {
             const unsigned t0 = static_cast<unsigned>(entry) & 0xFFFFu;
-            h.flags[t0] |= flag_used;
-            h.flags[h0n] |= flag_used;
-            h.flags[h1n] |= flag_used;
+            h.mark_used(t0);
+            h.mark_used(h0n);
+            h.mark_used(h1n);
             track_number = cnt.n_tracks + (excl & 0x3FFu);
             if (track_number < track_limit) {
               TrackHits& t = tracks[track_number];
@@ -580,7 +682,7 @@ namespace velo {
   }
 
   // ThreeHitTracksFilter.cu:48-107
-  __device__ __forceinline__ float means_square_fit_chi2(const HitsSoA& h, const TrackletHits& t)
+  __device__ __forceinline__ float means_square_fit_chi2(const Hit (&r)[3])
   {
     const float w = 6400.f;
     float s0, sx, sz, sxz, sz2, u0, uy, uz, uyz, uz2;
@@ -588,8 +690,7 @@ namespace velo {
     u0 = uy = uz = uyz = uz2 = 0.0f;
 #pragma unroll
     for (unsigned i = 0; i < 3; ++i) {
-      const unsigned hn = t.hits[i];
-      const float x = h.x[hn], y = h.y[hn], z = h.z[hn];
+      const float x = r[i].x, y = r[i].y, z = r[i].z;
       const float wx_t_x = w * x, wx_t_z = w * z;
       s0 += w;
       sx += wx_t_x;
@@ -612,12 +713,11 @@ namespace velo {
     float chi2 = 0.0f;
 #pragma unroll
     for (unsigned i = 0; i < 3; ++i) {
-      const unsigned hn = t.hits[i];
-      const float z = h.z[hn];
+      const float z = r[i].z;
       const float x = state_x + state_tx * z;
       const float y = state_y + state_ty * z;
-      const float dx = x - h.x[hn];
-      const float dy = y - h.y[hn];
+      const float dx = x - r[i].x;
+      const float dy = y - r[i].y;
       chi2 += dx * dx * w + dy * dy * w;
     }
     return chi2 * 0.5f;
@@ -634,7 +734,7 @@ namespace velo {
       md[i].hit_num = num[mp];
       md[i].z[0] = __ldg(g->module_zs + 2 * mp);
       md[i].z[1] = __ldg(g->module_zs + 2 * mp + 1);
-      md[i].mp = mp;
+      md[i].table = mp % 3;
     }
   }
 
@@ -647,7 +747,7 @@ namespace velo {
     Shared& s,
     uint64_t* ring,
     const Constants& k,
-    const HitsSoA& h,
+    const Hits& h,
     const unsigned* start,
     const unsigned* num,
     unsigned hit_offset,
@@ -663,6 +763,8 @@ namespace velo {
     unsigned first = n_module_pairs - 1;
     ModulePair md[3];
     module_pairs(md, p.geo, first, start, num, hit_offset);
+    for (unsigned i = 0; i < 3; ++i)
+      build_bucket_table_of(s.bucket[md[i].table], [h](unsigned j) { return h.phi(j); }, md[i].hit_start, md[i].hit_num);
     __syncthreads(); // bucket tables
 
     if constexpr (LPH == 0) seeding_flat<GATED>(s, ring, cnt, k, h, md, 8, gate, outcome);
@@ -672,11 +774,14 @@ namespace velo {
     --first;
     while (first > 1) {
       module_pairs(md, p.geo, first, start, num, hit_offset);
+      // the table of module pair first - 2 replaces that of first + 1, last read by the
+      // previous step's seeding
+      build_bucket_table_of(s.bucket[md[2].table], [h](unsigned j) { return h.phi(j); }, md[2].hit_start, md[2].hit_num);
       const unsigned prev_ttf = last_ttf;
       last_ttf = cnt.ttf;
       const unsigned diff = last_ttf - prev_ttf;
       cnt.local_hits = 0;
-      __syncthreads(); // ring entries of the last seeding
+      __syncthreads(); // ring entries of the last seeding, the new bucket table
       forwarding(s, ring, cnt, k, h, md[2], prev_ttf, diff, tracks, track_limit, three_hit, p.status);
       // The ring holds 2048 entries; beyond that the reference overwrites entries it has
       // not read yet, an order-dependent outcome this kernel does not reproduce.
@@ -753,29 +858,19 @@ namespace velo {
     TrackHits* tracks = p.tracks + to;
     TrackletHits* three_hit = p.three_hit_tracks + to;
 
-    // Stage the hits as SoA: shared memory when they fit (SMEM), else the event's global
-    // slice (16 bytes per estimated hit, so every slice starts 16-byte aligned).
-    unsigned char* base = SMEM ? dsmem : reinterpret_cast<unsigned char*>(p.hit_scratch) + size_t(16) * hit_offset;
-    const unsigned cap = SMEM ? p.smem_hit_capacity : n_hits;
-    float* xs = reinterpret_cast<float*>(base);
-    float* ys = xs + cap;
-    float* zs = ys + cap;
-    int16_t* phis = reinterpret_cast<int16_t*>(zs + cap);
-    uint8_t* flags = reinterpret_cast<uint8_t*>(phis + cap);
+    // Stage the hits as 16-byte records: shared memory when they fit (SMEM), else the
+    // event's global slice (16 bytes per estimated hit).
+    const Hits h {SMEM ? reinterpret_cast<uint4*>(dsmem) : reinterpret_cast<uint4*>(p.hit_scratch) + hit_offset};
     {
       const ClusterView g {const_cast<char*>(p.sorted_container), T};
       for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x) {
         const unsigned gi = hit_offset + i;
-        xs[i] = g.x(gi);
-        ys[i] = g.y(gi);
-        zs[i] = g.z(gi);
-        phis[i] = g.phi(gi);
         const unsigned module = ((g.id(gi) & 0x3FC0000u) >> 18) / 4;
-        flags[i] = (module & 1u) ? flag_odd_module : 0;
+        const unsigned flags = (module & 1u) ? flag_odd_module : 0u;
+        h.r[i] = make_uint4(__float_as_uint(g.x(gi)), __float_as_uint(g.y(gi)), __float_as_uint(g.z(gi)),
+                            static_cast<uint16_t>(g.phi(gi)) | (flags << 16));
       }
     }
-    const HitsSoA h {xs, ys, zs, phis, flags};
-    build_bucket_tables(s.bucket, phis, start, num, hit_offset);
 
     // Learned mode: the gate of the event's seed candidates, unless the fraction it lets
     // through falls outside the model's bounds, in which case the plain search runs
@@ -812,7 +907,7 @@ namespace velo {
     {
       uint8_t* g_used = reinterpret_cast<uint8_t*>(p.hit_used) + hit_offset;
       for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x)
-        g_used[i] = flags[i] & flag_used;
+        g_used[i] = h.flags(i) & flag_used;
     }
     __syncthreads();
 
@@ -826,9 +921,9 @@ namespace velo {
       TrackletHits t {};
       if (i < n_in) {
         t = three_hit[i];
-        const bool any_used =
-          (flags[t.hits[0]] & flag_used) || (flags[t.hits[1]] & flag_used) || (flags[t.hits[2]] & flag_used);
-        const float chi2 = means_square_fit_chi2(h, t);
+        const Hit r[3] = {h[t.hits[0]], h[t.hits[1]], h[t.hits[2]]};
+        const bool any_used = ((r[0].flags | r[1].flags | r[2].flags) & flag_used) != 0;
+        const float chi2 = means_square_fit_chi2(r);
         keep = !any_used && chi2 < k.max_chi2;
       }
       unsigned total;
@@ -848,13 +943,14 @@ namespace velo {
   // tracks to follow (2048 entries, 16 KiB) sits in shared memory, or with RING = 1 in this
   // CTA's slice of a global scratch (persistent launches only: the slice is the CTA's index),
   // which leaves room for more resident CTAs per SM.
-  // Flat-seeding kernels are register-capped for 1536 threads per SM (40 registers, a few
+  // Flat-seeding kernels are register-capped for 2048 threads per SM (32 registers, some
   // spills): with the hits and the ring staged through L2 shared memory no longer limits the
   // CTAs per SM, and the extra resident events hide more latency than the spills cost
-  // (measured per 16000-event launch: 5.87 / 5.72 ms at five / six 256-thread CTAs, 3.94 ms at
-  // twelve 128-thread CTAs; sixteen at 32 registers, 4.13 ms).
+  // (measured per 16000-event launch: 4.01 ms at twelve 128-thread CTAs and 40 registers,
+  // 3.83 ms at sixteen and 32 registers; the smaller the shared-memory footprint, the larger
+  // the L1 that caches the hit records).
   template<unsigned THREADS, unsigned LPH, unsigned RING>
-  __global__ void __launch_bounds__(THREADS, LPH == 0 ? 1536 / THREADS : 1) search_by_triplet_kernel(SearchParams p)
+  __global__ void __launch_bounds__(THREADS, LPH == 0 ? 2048 / THREADS : 1) search_by_triplet_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
     __shared__ std::conditional_t<LPH == 0, SearchSharedFlatPlain<THREADS>, SearchShared> s;
@@ -872,10 +968,10 @@ namespace velo {
   // search, recording each seed candidate's outcome when h1_outcome is set).  The gate costs
   // one byte read per candidate, so this kernel keeps the plain kernel's register budget.
   template<unsigned THREADS, unsigned RING>
-  __global__ void __launch_bounds__(THREADS, 1536 / THREADS) search_by_triplet_gated_kernel(SearchParams p)
+  __global__ void __launch_bounds__(THREADS, 2048 / THREADS) search_by_triplet_gated_kernel(SearchParams p)
   {
     extern __shared__ __align__(128) unsigned char dsmem[];
-    __shared__ SearchSharedFlatPlain<THREADS> s;
+    __shared__ SearchSharedFlatPlain<THREADS, true> s;
     __shared__ uint64_t ring_smem[RING ? 1 : max_tracks_to_follow];
     uint64_t* ring = RING ? p.ring_scratch + size_t(blockIdx.x) * max_tracks_to_follow : ring_smem;
     for_each_event(p.queue, p.n_events, [&](unsigned e, unsigned) {
