@@ -763,36 +763,34 @@ namespace velo {
     unsigned first = n_module_pairs - 1;
     ModulePair md[3];
     module_pairs(md, p.geo, first, start, num, hit_offset);
-    for (unsigned i = 0; i < 3; ++i)
+    for (unsigned i = 0; i < 2; ++i)
       build_bucket_table_of(s.bucket[md[i].table], [h](unsigned j) { return h.phi(j); }, md[i].hit_start, md[i].hit_num);
-    __syncthreads(); // bucket tables
 
-    if constexpr (LPH == 0) seeding_flat<GATED>(s, ring, cnt, k, h, md, 8, gate, outcome);
-    else seeding<LPH>(s, ring, cnt, k, h, md, 8);
-
+    // One step per module pair first = 25 ... 2 (the first without forwarding), with a single
+    // copy of the seeding code.
     unsigned last_ttf = 0;
-    --first;
-    while (first > 1) {
-      module_pairs(md, p.geo, first, start, num, hit_offset);
+    const unsigned window = GATED && gate != nullptr && p.seed_window ? p.seed_window : 4u;
+    for (;;) {
       // the table of module pair first - 2 replaces that of first + 1, last read by the
       // previous step's seeding
       build_bucket_table_of(s.bucket[md[2].table], [h](unsigned j) { return h.phi(j); }, md[2].hit_start, md[2].hit_num);
+      const bool forward = first < n_module_pairs - 1;
       const unsigned prev_ttf = last_ttf;
-      last_ttf = cnt.ttf;
-      const unsigned diff = last_ttf - prev_ttf;
+      if (forward) last_ttf = cnt.ttf;
       cnt.local_hits = 0;
       __syncthreads(); // ring entries of the last seeding, the new bucket table
-      forwarding(s, ring, cnt, k, h, md[2], prev_ttf, diff, tracks, track_limit, three_hit, p.status);
-      // The ring holds 2048 entries; beyond that the reference overwrites entries it has
-      // not read yet, an order-dependent outcome this kernel does not reproduce.
-      if (threadIdx.x == 0 && cnt.ttf - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
-      __syncthreads(); // hit_used flags written by forwarding
-      if constexpr (LPH == 0)
-        seeding_flat<GATED>(s, ring, cnt, k, h, md, GATED && gate != nullptr && p.seed_window ? p.seed_window : 4u, gate,
-                            outcome);
-      else seeding<LPH>(s, ring, cnt, k, h, md, 4);
-      if (threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
-      --first;
+      if (forward) {
+        forwarding(s, ring, cnt, k, h, md[2], prev_ttf, last_ttf - prev_ttf, tracks, track_limit, three_hit, p.status);
+        // The ring holds 2048 entries; beyond that the reference overwrites entries it has
+        // not read yet, an order-dependent outcome this kernel does not reproduce.
+        if (threadIdx.x == 0 && cnt.ttf - prev_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
+        __syncthreads(); // hit_used flags written by forwarding
+      }
+      if constexpr (LPH == 0) seeding_flat<GATED>(s, ring, cnt, k, h, md, forward ? window : 8u, gate, outcome);
+      else seeding<LPH>(s, ring, cnt, k, h, md, forward ? 4u : 8u);
+      if (forward && threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
+      if (--first <= 1) break;
+      module_pairs(md, p.geo, first, start, num, hit_offset);
     }
     __syncthreads(); // ring entries of the last seeding
 
