@@ -49,7 +49,7 @@ namespace velo {
   };
 
   struct SearchShared {
-    unsigned scan_sums[2][32]; // double-buffered warp totals of the block scans
+    alignas(16) unsigned scan_sums[2][32]; // double-buffered warp totals of the block scans (0 past the last warp)
     unsigned track_hits;       // sum of hitsNum over the >= 4 hit tracks
     uint32_t tail[max_tail_tracks]; // last two hits of a track (hit[n-2] | hit[n-1] << 16)
     uint8_t tail_n[max_tail_tracks];
@@ -159,10 +159,17 @@ namespace velo {
     if (lane == 31) buf[warp] = incl;
     __syncthreads();
     unsigned before = 0, all = 0;
-    for (unsigned w = 0; w < n_warps; ++w) {
-      const unsigned t = buf[w];
-      before += w < warp ? t : 0u;
-      all += t;
+    if (n_warps <= 4) { // one vector read of the four totals (those past the last warp stay 0)
+      const uint4 t = *reinterpret_cast<const uint4*>(buf);
+      all = t.x + t.y + t.z + t.w;
+      before = (warp > 0 ? t.x : 0u) + (warp > 1 ? t.y : 0u) + (warp > 2 ? t.z : 0u);
+    }
+    else {
+      for (unsigned w = 0; w < n_warps; ++w) {
+        const unsigned t = buf[w];
+        before += w < warp ? t : 0u;
+        all += t;
+      }
     }
     total = all;
     return before + incl - v;
@@ -758,6 +765,7 @@ namespace velo {
     uint8_t* outcome)
   {
     if (threadIdx.x == 0) s.track_hits = 0;
+    if (threadIdx.x < 64) s.scan_sums[threadIdx.x >> 5][threadIdx.x & 31u] = 0;
     Counters cnt {0, 0, 0, 0, 0, 0, 0};
     __syncthreads();
     unsigned first = n_module_pairs - 1;
