@@ -51,6 +51,10 @@ namespace velo {
   struct SearchShared {
     alignas(16) unsigned scan_sums[2][32]; // double-buffered warp totals of the block scans (0 past the last warp)
     unsigned track_hits;       // sum of hitsNum over the >= 4 hit tracks
+    // counters only reported (thread 0 keeps them): atomics::local_number_of_hits, the unused
+    // h1 met by the seeding (seed candidates), the candidates whose h0 and h2 windows were
+    // searched (the gate let through)
+    unsigned local_hits, candidates, searched;
     uint32_t tail[max_tail_tracks]; // last two hits of a track (hit[n-2] | hit[n-1] << 16)
     uint8_t tail_n[max_tail_tracks];
     // bucket tables of the three module pairs a step reads, built one per step
@@ -131,29 +135,22 @@ namespace velo {
     return static_cast<int>(i);
   }
 
-  // The event's counters (the reference's dev_atomics_velo and track count), kept in
-  // registers: every thread holds the same values and advances them by scan totals.
+  // The event's counters that place items (the reference's dev_atomics_velo and track
+  // count), kept in registers: every thread holds the same values and advances them by scan
+  // totals.
   struct Counters {
-    unsigned ttf;        // atomics::tracks_to_follow
-    unsigned n_three;    // atomics::number_of_three_hit_tracks
-    unsigned local_hits; // atomics::local_number_of_hits
-    unsigned n_tracks;   // dev_number_of_velo_tracks
+    unsigned ttf;      // atomics::tracks_to_follow
+    unsigned n_three;  // atomics::number_of_three_hit_tracks
+    unsigned n_tracks; // dev_number_of_velo_tracks
     unsigned scan_parity;
-    unsigned candidates; // unused h1 met by the seeding (seed candidates)
-    unsigned searched;   // candidates whose h0 and h2 windows were searched (the gate let through)
   };
 
-  // Block-wide exclusive scan with a single barrier: warp totals go to one of two
-  // buffers, alternating per call, so a call never overwrites totals still being read.
-  __device__ __forceinline__ unsigned scan1(SearchShared& s, Counters& c, unsigned v, unsigned& total)
+  // The block-wide part of an exclusive scan, with a single barrier: warp totals go to one
+  // of two buffers, alternating per call, so a call never overwrites totals still being
+  // read.  incl: the warp-inclusive sum of v.
+  __device__ __forceinline__ unsigned scan_block(SearchShared& s, Counters& c, unsigned incl, unsigned v, unsigned& total)
   {
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
-    unsigned incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= static_cast<unsigned>(o)) incl += t;
-    }
     unsigned* buf = s.scan_sums[c.scan_parity];
     c.scan_parity ^= 1u;
     if (lane == 31) buf[warp] = incl;
@@ -175,6 +172,37 @@ namespace velo {
     return before + incl - v;
   }
 
+  // Block-wide exclusive scan of v (every thread of the block calls it).
+  __device__ __forceinline__ unsigned scan1(SearchShared& s, Counters& c, unsigned v, unsigned& total)
+  {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= static_cast<unsigned>(o)) incl += t;
+    }
+    return scan_block(s, c, incl, v, total);
+  }
+
+  // scan1() of up to three 0/1 flags packed at bits 0, S1 and S2 (each field wide enough for
+  // a block total), the warp part by ballots.
+  template<unsigned NF, unsigned S1 = 16, unsigned S2 = 32>
+  __device__ __forceinline__ unsigned scan_flags(SearchShared& s, Counters& c, bool f0, bool f1, bool f2, unsigned& total)
+  {
+    const unsigned le = 0xFFFFFFFFu >> (31u - (threadIdx.x & 31u)); // this lane and those below
+    unsigned incl = __popc(__ballot_sync(0xFFFFFFFFu, f0) & le);
+    unsigned v = f0 ? 1u : 0u;
+    if constexpr (NF > 1) {
+      incl |= static_cast<unsigned>(__popc(__ballot_sync(0xFFFFFFFFu, f1) & le)) << S1;
+      v |= (f1 ? 1u : 0u) << S1;
+    }
+    if constexpr (NF > 2) {
+      incl |= static_cast<unsigned>(__popc(__ballot_sync(0xFFFFFFFFu, f2) & le)) << S2;
+      v |= (f2 ? 1u : 0u) << S2;
+    }
+    return scan_block(s, c, incl, v, total);
+  }
 
   __device__ __forceinline__ bool phi_outside(int16_t phi, int16_t extrapolated, int16_t tol)
   {
@@ -319,14 +347,14 @@ namespace velo {
       const bool ok = valid && l == 0 && best_fit < k.max_scatter;
       const unsigned unused = (valid && l == 0) ? 1u : 0u;
       unsigned total;
-      const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | (unused << 16), total);
+      const unsigned excl = scan_flags<2>(s, cnt, ok, unused != 0, false, total);
       if (ok) {
         const unsigned tn = (cnt.ttf + (excl & 0xFFFFu)) % max_tracks_to_follow;
         ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
                      (uint64_t(best_h2 & 0xFFFFu) << 32);
       }
       cnt.ttf += total & 0xFFFFu;
-      cnt.local_hits += total >> 16;
+      if (threadIdx.x == 0) s.local_hits += total >> 16;
     }
   }
 
@@ -371,7 +399,7 @@ namespace velo {
         const unsigned i = i0 + threadIdx.x;
         const bool unused = i < prev.hit_num && !(h.flags(prev.hit_start + i) & flag_used);
         unsigned total;
-        const unsigned before = n_unused + scan1(s, cnt, unused ? 1u : 0u, total);
+        const unsigned before = n_unused + scan_flags<1>(s, cnt, unused, false, false, total);
         if (i < prev.hit_num) s.unused_before[i] = static_cast<uint16_t>(before);
         if (unused) s.unused_at[before] = static_cast<uint16_t>(i);
         n_unused += total;
@@ -394,12 +422,14 @@ namespace velo {
           const bool valid = threadIdx.x < n_h1 && !(h.flags(hw) & flag_used);
           const bool pass = valid && (gate == nullptr || gate[hw] != 0);
           unsigned total;
-          const unsigned excl = scan1(s, cnt, (pass ? 1u : 0u) | ((valid ? 1u : 0u) << 16), total);
+          const unsigned excl = scan_flags<2>(s, cnt, pass, valid, false, total);
           if (pass) s.cand_list[excl & 0xFFFFu] = static_cast<uint16_t>(threadIdx.x);
           n_searched = total & 0xFFFFu;
-          cnt.local_hits += total >> 16;
-          cnt.candidates += total >> 16;
-          cnt.searched += n_searched;
+          if (threadIdx.x == 0) {
+            s.local_hits += total >> 16;
+            s.candidates += total >> 16;
+            s.searched += n_searched;
+          }
         }
         __syncthreads();
         searched = threadIdx.x < n_searched;
@@ -526,17 +556,17 @@ namespace velo {
         if (GATED && outcome != nullptr) outcome[h1] = ok ? 2 : 1;
       }
       unsigned total;
-      const unsigned excl = scan1(s, cnt, (ok ? 1u : 0u) | ((!GATED && searched ? 1u : 0u) << 16), total);
+      const unsigned excl = scan_flags<GATED ? 1 : 2>(s, cnt, ok, !GATED && searched, false, total);
       if (ok) {
         const unsigned tn = (cnt.ttf + (excl & 0xFFFFu)) % max_tracks_to_follow;
         ring[tn] = seed_flag | (uint64_t(best_h0 & 0xFFFFu)) | (uint64_t(h1 & 0xFFFFu) << 16) |
                      (uint64_t(best_h2 & 0xFFFFu) << 32);
       }
       cnt.ttf += total & 0xFFFFu;
-      if constexpr (!GATED) {
-        cnt.local_hits += total >> 16;
-        cnt.candidates += total >> 16;
-        cnt.searched += total >> 16;
+      if (!GATED && threadIdx.x == 0) {
+        s.local_hits += total >> 16;
+        s.candidates += total >> 16;
+        s.searched += total >> 16;
       }
     }
   }
@@ -625,7 +655,7 @@ namespace velo {
       const bool three = active && !found && !(skipped < k.max_skipped_modules) && nh == 3 && is_seed;
       unsigned total;
       const unsigned excl =
-        scan1(s, cnt, (new_track ? 1u : 0u) | ((enqueue ? 1u : 0u) << 10) | ((three ? 1u : 0u) << 20), total);
+        scan_flags<3, 10, 20>(s, cnt, new_track, enqueue, three, total);
       if (active) {
         unsigned track_number = tn;
         if (found) {
@@ -764,9 +794,9 @@ namespace velo {
     const uint8_t* gate,
     uint8_t* outcome)
   {
-    if (threadIdx.x == 0) s.track_hits = 0;
+    if (threadIdx.x == 0) s.track_hits = s.candidates = s.searched = 0;
     if (threadIdx.x < 64) s.scan_sums[threadIdx.x >> 5][threadIdx.x & 31u] = 0;
-    Counters cnt {0, 0, 0, 0, 0, 0, 0};
+    Counters cnt {0, 0, 0, 0};
     __syncthreads();
     unsigned first = n_module_pairs - 1;
     ModulePair md[3];
@@ -785,7 +815,7 @@ namespace velo {
       const bool forward = first < n_module_pairs - 1;
       const unsigned prev_ttf = last_ttf;
       if (forward) last_ttf = cnt.ttf;
-      cnt.local_hits = 0;
+      if (threadIdx.x == 0) s.local_hits = 0;
       __syncthreads(); // ring entries of the last seeding, the new bucket table
       if (forward) {
         forwarding(s, ring, cnt, k, h, md[2], prev_ttf, last_ttf - prev_ttf, tracks, track_limit, three_hit, p.status);
@@ -816,7 +846,7 @@ namespace velo {
           seed = (entry & seed_flag) != 0;
         }
         unsigned total;
-        const unsigned excl = scan1(s, cnt, seed ? 1u : 0u, total);
+        const unsigned excl = scan_flags<1>(s, cnt, seed, false, false, total);
         if (seed) {
           const unsigned slot = cnt.n_three + excl;
           if (slot < track_limit) {
@@ -897,8 +927,8 @@ namespace velo {
     Counters cnt =
       search_pass<LPH, GATED>(p, s, ring, k, h, start, num, hit_offset, tracks, track_limit, three_hit, gate, outcome);
     if (p.seed_stats != nullptr && threadIdx.x == 0) {
-      p.seed_stats[3 * e] = cnt.candidates;
-      p.seed_stats[3 * e + 1] = cnt.searched;
+      p.seed_stats[3 * e] = s.candidates;
+      p.seed_stats[3 * e + 1] = s.searched;
       p.seed_stats[3 * e + 2] = mode;
     }
 
@@ -906,7 +936,7 @@ namespace velo {
       unsigned* atomics = p.atomics_velo + 3 * e;
       atomics[0] = cnt.n_three;
       atomics[1] = cnt.ttf;
-      atomics[2] = cnt.local_hits;
+      atomics[2] = s.local_hits;
       p.number_of_velo_tracks[e] = cnt.n_tracks;
       if (cnt.n_tracks > to_next - to) set_error(p.status, err_track_capacity);
     }
@@ -933,7 +963,7 @@ namespace velo {
         keep = !any_used && chi2 < k.max_chi2;
       }
       unsigned total;
-      const unsigned excl = scan1(s, cnt, keep ? 1u : 0u, total);
+      const unsigned excl = scan_flags<1>(s, cnt, keep, false, false, total);
       if (keep) out[filter_count + excl] = t;
       filter_count += total;
     }
