@@ -59,6 +59,8 @@ namespace velo {
     uint8_t tail_n[max_tail_tracks];
     // bucket tables of the three module pairs a step reads, built one per step
     uint16_t bucket[3][n_buckets + 1];
+    // the event's module pairs, last first: a step's three are mps[25 - first] onwards
+    ModulePair mps[n_module_pairs];
   };
 
   // Shared state of the flat seeding variant: one slot per (h1, candidate order).
@@ -124,6 +126,14 @@ namespace velo {
   {
     const int pos = p0 + ((i & 1u) ? static_cast<int>((i + 1) / 2) : -static_cast<int>(i / 2));
     return static_cast<unsigned>(pos < 0 ? pos + n : (pos >= n ? pos - n : pos));
+  }
+
+  // The first h2 of the circular window walk: start % n (0 for an empty module pair), without
+  // a division for start in [0, n], leftmost()'s range.
+  __device__ __forceinline__ unsigned first_candidate(int16_t start, unsigned n)
+  {
+    const unsigned x = static_cast<unsigned>(start);
+    return x < n ? x : (x == n || n == 0 ? 0u : x % n);
   }
 
   // leftmost() over the staged hits [start, start + n) of a module pair.
@@ -267,7 +277,7 @@ namespace velo {
     const float ty = tyn * td;
     const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[0] - prev.z[0]);
     // circular walk from the candidate: index (start + j) % n without a division per step
-    unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
+    unsigned idx = first_candidate(f.start, next.hit_num);
     for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
       const unsigned h2 = next.hit_start + idx;
       const Hit b = h[h2];
@@ -294,7 +304,7 @@ namespace velo {
     SearchShared& s, uint64_t* ring, Counters& cnt, const Constants& k, const Hits& h, const ModulePair* md,
     unsigned n_candidates)
   {
-    const ModulePair prev = md[0], cur = md[1], next = md[2];
+    const ModulePair &prev = md[0], &cur = md[1], &next = md[2];
     const unsigned groups = blockDim.x / LPH;
     const unsigned g = threadIdx.x / LPH;
     const unsigned l = threadIdx.x % LPH;
@@ -386,7 +396,7 @@ namespace velo {
     const uint8_t* gate,
     uint8_t* outcome)
   {
-    const ModulePair prev = md[0], cur = md[1], next = md[2];
+    const ModulePair &prev = md[0], &cur = md[1], &next = md[2];
     const unsigned per_chunk = min(blockDim.x, Flat::slots / n_candidates);
     const int n_prev = static_cast<int>(prev.hit_num);
     const int16_t tol = static_cast<int16_t>(k.phi_tolerance_i16);
@@ -514,7 +524,7 @@ namespace velo {
         const float tx = txn * td;
         const float ty = tyn * td;
         const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[0] - prev.z[0]);
-        unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
+        unsigned idx = first_candidate(f.start, next.hit_num);
         for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
           const unsigned h2 = next.hit_start + idx;
           const Hit c = h[h2];
@@ -630,7 +640,7 @@ namespace velo {
         const float ty = tyn * td;
         float best_fit = k.max_scatter;
         const Extrapolation f = extrapolate(k, s, h, next, h0x, h0y, tx, ty, next.z[odd] - h0z);
-        unsigned idx = next.hit_num ? static_cast<unsigned>(f.start) % next.hit_num : 0u;
+        unsigned idx = first_candidate(f.start, next.hit_num);
         for (unsigned j = 0; j < next.hit_num; ++j, idx = (idx + 1 == next.hit_num) ? 0u : idx + 1) {
           const unsigned h2 = next.hit_start + idx;
           const Hit c = h[h2];
@@ -761,17 +771,18 @@ namespace velo {
   }
 
   // The three module pairs of a step (first, first - 1, first - 2), read by every thread.
+  // The event's module pairs into shared memory, last first (threads 0-25; a barrier follows).
   __device__ __forceinline__ void module_pairs(
-    ModulePair* md, const Geometry* g, unsigned first, const unsigned* start, const unsigned* num, unsigned hit_offset)
+    ModulePair* mps, const Geometry* g, const unsigned* start, const unsigned* num, unsigned hit_offset)
   {
-#pragma unroll
-    for (unsigned i = 0; i < 3; ++i) {
-      const unsigned mp = first - i;
-      md[i].hit_start = start[mp] - hit_offset;
-      md[i].hit_num = num[mp];
-      md[i].z[0] = __ldg(g->module_zs + 2 * mp);
-      md[i].z[1] = __ldg(g->module_zs + 2 * mp + 1);
-      md[i].table = mp % 3;
+    const unsigned mp = threadIdx.x;
+    if (mp < n_module_pairs) {
+      ModulePair& m = mps[n_module_pairs - 1 - mp];
+      m.hit_start = start[mp] - hit_offset;
+      m.hit_num = num[mp];
+      m.z[0] = __ldg(g->module_zs + 2 * mp);
+      m.z[1] = __ldg(g->module_zs + 2 * mp + 1);
+      m.table = mp % 3;
     }
   }
 
@@ -797,10 +808,10 @@ namespace velo {
     if (threadIdx.x == 0) s.track_hits = s.candidates = s.searched = 0;
     if (threadIdx.x < 64) s.scan_sums[threadIdx.x >> 5][threadIdx.x & 31u] = 0;
     Counters cnt {0, 0, 0, 0};
+    module_pairs(s.mps, p.geo, start, num, hit_offset);
     __syncthreads();
     unsigned first = n_module_pairs - 1;
-    ModulePair md[3];
-    module_pairs(md, p.geo, first, start, num, hit_offset);
+    const ModulePair* md = s.mps;
     for (unsigned i = 0; i < 2; ++i)
       build_bucket_table_of(s.bucket[md[i].table], [h](unsigned j) { return h.phi(j); }, md[i].hit_start, md[i].hit_num);
 
@@ -828,7 +839,7 @@ namespace velo {
       else seeding<LPH>(s, ring, cnt, k, h, md, forward ? 4u : 8u);
       if (forward && threadIdx.x == 0 && cnt.ttf - last_ttf > max_tracks_to_follow) set_error(p.status, err_ttf_overflow);
       if (--first <= 1) break;
-      module_pairs(md, p.geo, first, start, num, hit_offset);
+      ++md;
     }
     __syncthreads(); // ring entries of the last seeding
 
