@@ -16,6 +16,7 @@
 namespace velo {
 
   constexpr unsigned max_banks = 512;
+  constexpr unsigned bank_hints = 512; // bank_of() hints, one per 32 SPs
 
   // ------------------------------------------------------------------------------------
   // Bulk copy (TMA engine) into shared memory, completion tracked by an mbarrier.
@@ -142,6 +143,9 @@ namespace velo {
     unsigned flat[max_banks + 1];  // exclusive scan of n_sp over VP/Velo banks
     unsigned source_id[max_banks];
     uint8_t velo[max_banks];
+    // hint[k]: the bank holding flat SP k * 32 (entries up to total_sp / 32), where bank_of()
+    // starts a short forward scan
+    uint16_t hint[bank_hints];
   };
 
   __device__ __forceinline__ unsigned bank_module_pair(unsigned source_id, int version)
@@ -276,9 +280,47 @@ namespace velo {
     __syncthreads();
   }
 
+  // atomicAdd(counter, 1) from the converged lanes of the warp, one atomic per counter (the
+  // lanes that add to the same counter pass the same key): returns this lane's old value, the
+  // lanes of a key taking consecutive values in lane order.
+  __device__ __forceinline__ unsigned warp_aggregated_inc(unsigned* counter, unsigned key)
+  {
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(counter, static_cast<unsigned>(__popc(peers)));
+    return __shfl_sync(peers, base, leader) + __popc(peers & ((1u << lane) - 1u));
+  }
+
+  // atomicAdd(counter, v) from the converged lanes of the warp, one atomic per counter.
+  __device__ __forceinline__ void warp_aggregated_add(unsigned* counter, unsigned key, unsigned v)
+  {
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    const unsigned sum = __reduce_add_sync(peers, v);
+    if ((threadIdx.x & 31u) == static_cast<unsigned>(__ffs(peers) - 1) && sum) atomicAdd(counter, sum);
+  }
+
+  // The hint table of a parsed bank table; ends with a __syncthreads().
+  __device__ __forceinline__ void index_banks(BankTable& bt)
+  {
+    for (unsigned b = threadIdx.x; b < bt.n_banks; b += blockDim.x) {
+      const unsigned hi = bt.flat[b + 1];
+      for (unsigned k = (bt.flat[b] + 31) / 32; k < bank_hints && k * 32 < hi; ++k)
+        bt.hint[k] = static_cast<uint16_t>(b);
+    }
+    __syncthreads();
+  }
+
   __device__ __forceinline__ unsigned bank_of(const BankTable& bt, unsigned f)
   {
-    // last bank b with flat[b] <= f (banks with no SP share their start with the next)
+    // last bank b with flat[b] <= f < total_sp (banks with no SP share their start with the next)
+    if (f / 32 < bank_hints) {
+      unsigned b = bt.hint[f / 32];
+      while (b + 1 < bt.n_banks && bt.flat[b + 1] <= f)
+        ++b;
+      return b;
+    }
     unsigned lo = 0, hi = bt.n_banks;
     while (hi - lo > 1) {
       const unsigned mid = (lo + hi) / 2;
@@ -442,6 +484,7 @@ namespace velo {
     unsigned n_words, staged;
     const uint32_t* words = stage_event(p.in, ev, dsmem, p.smem_blob_bytes, bar, bar_phase, p.status, n_words, staged);
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
+    index_banks(bt);
     (void) staged; // the candidate count runs the full scans: only non-isolated SPs (a third)
                    // search, which costs less than sorting every bank
 
@@ -475,7 +518,7 @@ namespace velo {
           const uint32_t word = words[bt.words_off[b] + f - bt.flat[b]];
           if (word & 0x80000000u) {
             const unsigned mp = bank_module_pair(bt.source_id[b], p.in.bank_version);
-            if (mp < n_module_pairs) atomicAdd(&est_mp[mp], isolated_two_clusters(word & 0xFFu) ? 2u : 1u);
+            if (mp < n_module_pairs) warp_aggregated_add(&est_mp[mp], mp, isolated_two_clusters(word & 0xFFu) ? 2u : 1u);
             else set_error(p.status, err_input_capacity);
           }
           else {
@@ -501,9 +544,9 @@ namespace velo {
         const uint32_t* bank_words = words + bt.words_off[b];
         const uint32_t c = sp_candidates(bank_words[f - bt.flat[b]], bank_words, bt.n_sp[b]);
         const unsigned add = ((c >> 8) & 1u) + ((c >> 24) & 1u);
-        if (add) atomicAdd(&cand_count, add);
+        warp_aggregated_add(&cand_count, 0u, add);
         const unsigned mp = bank_module_pair(bt.source_id[b], p.in.bank_version);
-        if (mp < n_module_pairs) atomicAdd(&est_mp[mp], add);
+        if (mp < n_module_pairs) warp_aggregated_add(&est_mp[mp], mp, add);
         else set_error(p.status, err_input_capacity);
       }
       __syncthreads();
@@ -808,6 +851,7 @@ namespace velo {
     unsigned n_words, staged;
     const uint32_t* words = stage_event(p.in, ev, blob, p.smem_blob_bytes, bar, bar_phase, p.status, n_words, staged);
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
+    index_banks(bt);
     const uint32_t key_mask = sp_key_mask(version);
     // sorted bank copies: behind the staged event (or at the start of the blob), else in the
     // event's slice of the global scratch (L2-resident), else none (full neighbour scans)
@@ -823,7 +867,7 @@ namespace velo {
 
     const Geometry* g = p.geo;
     auto stage_cluster = [&](const ClusterOut& o, unsigned mp) {
-      const unsigned slot = atomicAdd(&mp_count[mp], 1u);
+      const unsigned slot = warp_aggregated_inc(&mp_count[mp], mp);
       if (region[mp] + slot < region[mp + 1]) {
         const unsigned i = region[mp] + slot;
         st.id(i) = o.id;
