@@ -244,4 +244,16 @@ namespace velo {
 
   __device__ __forceinline__ void set_error(unsigned* status, unsigned bit) { atomicOr(status, bit); }
 
+  // Invalidates, without writing them back to HBM, the 128-byte L2 lines that lie wholly
+  // inside [p, p + bytes): a CTA's scratch that no thread reads again (every thread of the
+  // CTA calls it, after a barrier that follows the last read; discard.global.L2).
+  __device__ __forceinline__ void discard_l2(const void* p, size_t bytes)
+  {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uintptr_t lo = (a + 127) & ~uintptr_t(127);
+    const uintptr_t hi = (a + bytes) & ~uintptr_t(127);
+    for (uintptr_t line = lo + uintptr_t(threadIdx.x) * 128; line < hi; line += uintptr_t(blockDim.x) * 128)
+      asm volatile("discard.global.L2 [%0], 128;" ::"l"(line) : "memory");
+  }
+
 } // namespace velo

@@ -856,12 +856,16 @@ namespace velo {
     // sorted bank copies: behind the staged event (or at the start of the blob), else in the
     // event's slice of the global scratch (L2-resident), else none (full neighbour scans)
     uint32_t* sorted = nullptr;
+    bool sorted_in_scratch = false;
     if (staged + 4 * bt.total_sp <= p.smem_blob_bytes) {
       sorted = reinterpret_cast<uint32_t*>(blob + staged);
     }
     else if (p.sp_scratch != nullptr) {
       const unsigned sp_base = p.candidates_offsets[e] / 2;
-      if (sp_base + bt.total_sp <= p.sp_capacity) sorted = p.sp_scratch + sp_base;
+      if (sp_base + bt.total_sp <= p.sp_capacity) {
+        sorted = p.sp_scratch + sp_base;
+        sorted_in_scratch = true;
+      }
     }
     if (sorted) sort_bank_words(bt, words, sorted, key_mask);
 
@@ -1025,17 +1029,23 @@ namespace velo {
         set_error(p.status, err_cluster_capacity);
         continue;
       }
+      // written once here, read by the next kernel: streaming stores (evict first), which
+      // leave L2 to the staging of the events in flight
       const unsigned dst = base + region[mp] + position;
-      out.id(dst) = id;
-      out.phi(dst) = phi;
-      out.x(dst) = st.x(i);
-      out.y(dst) = st.y(i);
-      out.z(dst) = st.z(i);
+      __stcs(&out.id(dst), id);
+      __stcs(&out.phi(dst), phi);
+      __stcs(&out.x(dst), st.x(i));
+      __stcs(&out.y(dst), st.y(i));
+      __stcs(&out.z(dst), st.z(i));
     }
     if (threadIdx.x < n_module_pairs) {
       const unsigned mp = threadIdx.x;
       p.module_cluster_num[e * n_module_pairs + mp] = min(mp_count[mp], region[mp + 1] - region[mp]);
     }
+    // the event's slices of the global staging and of the sorted bank copies are dead
+    __syncthreads();
+    if (!staged_in_smem) discard_l2(stage_base, size_t(24) * est_total);
+    if (sorted && sorted_in_scratch) discard_l2(sorted, size_t(4) * bt.total_sp);
   }
 
   // Capped for 2048 threads per SM (32 registers, no spills: eight 256-thread CTAs, or

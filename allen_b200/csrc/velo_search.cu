@@ -910,12 +910,13 @@ namespace velo {
     const Hits h {SMEM ? reinterpret_cast<uint4*>(dsmem) : reinterpret_cast<uint4*>(p.hit_scratch) + hit_offset};
     {
       const ClusterView g {const_cast<char*>(p.sorted_container), T};
+      // read once: streaming loads (evict first), which leave L2 to the staged hits
       for (unsigned i = threadIdx.x; i < n_hits; i += blockDim.x) {
         const unsigned gi = hit_offset + i;
-        const unsigned module = ((g.id(gi) & 0x3FC0000u) >> 18) / 4;
+        const unsigned module = ((__ldcs(&g.id(gi)) & 0x3FC0000u) >> 18) / 4;
         const unsigned flags = (module & 1u) ? flag_odd_module : 0u;
-        h.r[i] = make_uint4(__float_as_uint(g.x(gi)), __float_as_uint(g.y(gi)), __float_as_uint(g.z(gi)),
-                            static_cast<uint16_t>(g.phi(gi)) | (flags << 16));
+        h.r[i] = make_uint4(__float_as_uint(__ldcs(&g.x(gi))), __float_as_uint(__ldcs(&g.y(gi))),
+                            __float_as_uint(__ldcs(&g.z(gi))), static_cast<uint16_t>(__ldcs(&g.phi(gi))) | (flags << 16));
       }
     }
 
@@ -982,6 +983,8 @@ namespace velo {
       p.number_of_three_hit_tracks_output[e] = filter_count;
       p.event_track_hits[e] = s.track_hits + 3 * filter_count;
     }
+    // the staged hits are dead (the filter's last scan is a barrier after the last read)
+    if (!SMEM) discard_l2(h.r, size_t(16) * n_hits);
   }
 
   // One instantiation per (block size, lanes per seed, ring place); the chain launches the one
