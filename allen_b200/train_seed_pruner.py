@@ -35,6 +35,15 @@ LEARNED_CONFIG = os.path.join(DATA, "launch_config_learned.json")
 TOLERANCE = 0.002
 
 
+def _portable(v):
+    """A path inside the repository as a path relative to its root (the report names no machine
+    path); other values unchanged."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if isinstance(v, str) and os.path.isabs(v) and os.path.commonpath([root, os.path.abspath(v)]) == root:
+        return os.path.relpath(v, root)
+    return v
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--train-events", type=int, default=300000)
@@ -121,7 +130,8 @@ def main():
     torch.cuda.set_device(0)
     t0 = time.time()
     log = lambda m: print(f"[{time.time() - t0:7.1f} s] {m}", flush=True)  # noqa: E731
-    report = {"args": vars(args), "device": torch.cuda.get_device_name(0)}
+    report = {"args": {k: _portable(v) for k, v in vars(args).items() if k != "report"},
+              "device": torch.cuda.get_device_name(0)}
     chain = VeloChain()
     plain_config = chain.get_config()
 
