@@ -278,7 +278,8 @@ struct VeloChain {
     event_track_hits, event_track_hit_base, offsets_all, track_hit_number, offsets_hit_number;
   DeviceBuffer<char> sorted, staging, track_hits, hit_scratch;
   DeviceBuffer<uint64_t> ring_scratch; // search_ring_global: one ring of 2048 entries per resident search CTA
-  DeviceBuffer<uint32_t> sp_scratch;   // sorted bank copies that do not fit the clustering kernel's blob
+  DeviceBuffer<uint32_t> sp_scratch;   // sorted bank copies (the estimate kernel's, which the clustering kernel reads)
+  DeviceBuffer<unsigned> sp_base, sp_alloc; // each event's place in sp_scratch, the allocation counter
   DeviceBuffer<velo::TrackHits> tracks;
   DeviceBuffer<velo::TrackletHits> three_hit, three_out;
   DeviceBuffer<uint8_t> hit_used, accepted;
@@ -390,6 +391,8 @@ namespace {
     f(c->staging, 24 * T, scratch_buffer);
     f(c->hit_scratch, 16 * T, scratch_buffer);
     f(c->sp_scratch, b.super_pixels + 64, scratch_buffer);
+    f(c->sp_base, n, scratch_buffer);
+    f(c->sp_alloc, 1, scratch_buffer);
     f(c->tracks, tracks, scratch_buffer);
     f(c->three_hit, tracks, scratch_buffer);
     f(c->three_out, tracks, scratch_buffer);
@@ -565,7 +568,12 @@ namespace {
       ep.designated_stride = (n + 255) / 256;
       ep.status = c->status.p;
       ep.smem_blob_bytes = c->estimate_blob_bytes;
+      ep.sp_scratch = c->sp_scratch.p;
+      ep.sp_capacity = static_cast<unsigned>(c->sp_scratch.n);
+      ep.sp_alloc = c->sp_alloc.p;
+      ep.sp_base = c->sp_base.p;
       ep.queue = queue(0);
+      VELO_CUDA(cudaMemsetAsync(c->sp_alloc.p, 0, sizeof(unsigned), stream));
       estimate_kernel<<<grid(c->resident_estimate), decode_threads, c->estimate_blob_bytes, stream>>>(ep);
       VELO_CUDA(cudaGetLastError());
       VELO_CUDA(mark());
@@ -591,6 +599,7 @@ namespace {
       cp.candidates_offsets = c->candidates_offsets.p;
       cp.sp_scratch = c->sp_scratch.p;
       cp.sp_capacity = static_cast<unsigned>(c->sp_scratch.n);
+      cp.sp_base = c->sp_base.p;
       cp.status = c->status.p;
       cp.smem_blob_bytes = c->cluster_blob_bytes;
       cp.smem_cluster_capacity = c->cluster_stage_capacity;

@@ -354,8 +354,16 @@ namespace velo {
       const uint32_t* w = words + bt.words_off[b];
       const unsigned n = bt.flat[b + 1] - bt.flat[b];
       const uint32_t mine = (((w[i] >> 8) & key_mask) << 16) | i;
-      unsigned rank = 0;
-      for (unsigned j = 0; j < n; ++j)
+      unsigned rank = 0, j = 0;
+      // four independent loads per round: the bank's words are L1 hits, the loop is latency-bound
+      for (; j + 4 <= n; j += 4) {
+        const uint32_t a0 = w[j], a1 = w[j + 1], a2 = w[j + 2], a3 = w[j + 3];
+        rank += ((((a0 >> 8) & key_mask) << 16) | j) < mine;
+        rank += ((((a1 >> 8) & key_mask) << 16) | (j + 1)) < mine;
+        rank += ((((a2 >> 8) & key_mask) << 16) | (j + 2)) < mine;
+        rank += ((((a3 >> 8) & key_mask) << 16) | (j + 3)) < mine;
+      }
+      for (; j < n; ++j)
         rank += ((((w[j] >> 8) & key_mask) << 16) | j) < mine;
       sorted[bt.flat[b] + rank] = w[i];
     }
@@ -473,6 +481,7 @@ namespace velo {
     __shared__ unsigned warp_sums[33];
     __shared__ uint16_t queue[estimate_queue];
     __shared__ unsigned queue_count[2];
+    __shared__ unsigned sorted_at;
 
     const unsigned ev = e + p.in.event_start;
     const bool v23 = p.in.bank_version == 2 || p.in.bank_version == 3;
@@ -485,8 +494,24 @@ namespace velo {
     const uint32_t* words = stage_event(p.in, ev, dsmem, p.smem_blob_bytes, bar, bar_phase, p.status, n_words, staged);
     parse_banks(p.in, ev, words, n_words, bt, warp_sums, p.status);
     index_banks(bt);
-    (void) staged; // the candidate count runs the full scans: only non-isolated SPs (a third)
-                   // search, which costs less than sorting every bank
+    (void) staged;
+    // The event's banks sorted by key into its allocation of the sort scratch: this kernel's
+    // neighbour search then scans key ranges, and the clustering kernel reuses the copies.
+    // Without scratch (or room in it) the search scans every SP of the bank.
+    const uint32_t key_mask = sp_key_mask(p.in.bank_version);
+    const uint32_t* sorted = nullptr;
+    if (p.sp_scratch != nullptr) {
+      if (threadIdx.x == 0) {
+        const unsigned at = atomicAdd(p.sp_alloc, bt.total_sp);
+        sorted_at = (at <= p.sp_capacity && bt.total_sp <= p.sp_capacity - at) ? at : no_sorted_copy;
+        p.sp_base[e] = sorted_at;
+      }
+      __syncthreads();
+      if (sorted_at != no_sorted_copy) {
+        sort_bank_words(bt, words, p.sp_scratch + sorted_at, key_mask);
+        sorted = p.sp_scratch + sorted_at;
+      }
+    }
 
     // velo_calculate_number_of_candidates: block 0 of the reference's launch (grid of
     // ceil(N / 256) blocks, one thread per event) handles events 0, stride, 2 stride, ...
@@ -542,7 +567,9 @@ namespace velo {
         const unsigned f = chunk_base + queue[q];
         const unsigned b = bank_of(bt, f);
         const uint32_t* bank_words = words + bt.words_off[b];
-        const uint32_t c = sp_candidates(bank_words[f - bt.flat[b]], bank_words, bt.n_sp[b]);
+        const uint32_t word = bank_words[f - bt.flat[b]];
+        const uint32_t c = sorted ? sp_candidates(word, sorted + bt.flat[b], bt.n_sp[b], key_mask)
+                                  : sp_candidates(word, bank_words, bt.n_sp[b]);
         const unsigned add = ((c >> 8) & 1u) + ((c >> 24) & 1u);
         warp_aggregated_add(&cand_count, 0u, add);
         const unsigned mp = bank_module_pair(bt.source_id[b], p.in.bank_version);
@@ -857,7 +884,15 @@ namespace velo {
     // event's slice of the global scratch (L2-resident), else none (full neighbour scans)
     uint32_t* sorted = nullptr;
     bool sorted_in_scratch = false;
-    if (staged + 4 * bt.total_sp <= p.smem_blob_bytes) {
+    if (p.sp_base != nullptr) {
+      // sorted by the estimate kernel (no copy when its scratch had no room: full scans)
+      const unsigned at = p.sp_base[e];
+      if (at != no_sorted_copy) {
+        sorted = p.sp_scratch + at;
+        sorted_in_scratch = true;
+      }
+    }
+    else if (staged + 4 * bt.total_sp <= p.smem_blob_bytes) {
       sorted = reinterpret_cast<uint32_t*>(blob + staged);
     }
     else if (p.sp_scratch != nullptr) {
@@ -867,7 +902,7 @@ namespace velo {
         sorted_in_scratch = true;
       }
     }
-    if (sorted) sort_bank_words(bt, words, sorted, key_mask);
+    if (sorted && p.sp_base == nullptr) sort_bank_words(bt, words, sorted, key_mask);
 
     const Geometry* g = p.geo;
     auto stage_cluster = [&](const ClusterOut& o, unsigned mp) {

@@ -54,8 +54,17 @@ namespace velo {
     unsigned designated_stride;           // events e with e % stride == 0 set the bank index
     unsigned* status;
     unsigned smem_blob_bytes;
+    // sorted bank copies for this kernel's neighbour search and the clustering kernel's (null:
+    // full scans): each event takes total_sp words of sp_scratch from the counter sp_alloc
+    // (zeroed before the launch) and records where in sp_base[e] (no_sorted_copy: no room)
+    uint32_t* sp_scratch;
+    unsigned sp_capacity;
+    unsigned* sp_alloc;
+    unsigned* sp_base;
     WorkQueue queue;
   };
+
+  constexpr unsigned no_sorted_copy = 0xFFFFFFFFu;
 
   // ---- masked clustering + phi + sort by phi, one event per CTA ----
   struct ClusterSortParams {
@@ -73,6 +82,8 @@ namespace velo {
     uint32_t* sp_scratch;                       // [S] sorted bank copies of events whose copies do not
                                                 //     fit the shared-memory blob (null: full scans)
     unsigned sp_capacity;                       // S, allocated words of sp_scratch
+    const unsigned* sp_base;                    // [N] where the estimate kernel sorted each event's banks
+                                                //     in sp_scratch (null: this kernel sorts them)
     unsigned* status;
     unsigned smem_blob_bytes;
     unsigned smem_cluster_capacity;             // clusters staged in shared memory per event
