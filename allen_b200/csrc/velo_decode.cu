@@ -354,16 +354,8 @@ namespace velo {
       const uint32_t* w = words + bt.words_off[b];
       const unsigned n = bt.flat[b + 1] - bt.flat[b];
       const uint32_t mine = (((w[i] >> 8) & key_mask) << 16) | i;
-      unsigned rank = 0, j = 0;
-      // four independent loads per round: the bank's words are L1 hits, the loop is latency-bound
-      for (; j + 4 <= n; j += 4) {
-        const uint32_t a0 = w[j], a1 = w[j + 1], a2 = w[j + 2], a3 = w[j + 3];
-        rank += ((((a0 >> 8) & key_mask) << 16) | j) < mine;
-        rank += ((((a1 >> 8) & key_mask) << 16) | (j + 1)) < mine;
-        rank += ((((a2 >> 8) & key_mask) << 16) | (j + 2)) < mine;
-        rank += ((((a3 >> 8) & key_mask) << 16) | (j + 3)) < mine;
-      }
-      for (; j < n; ++j)
+      unsigned rank = 0;
+      for (unsigned j = 0; j < n; ++j)
         rank += ((((w[j] >> 8) & key_mask) << 16) | j) < mine;
       sorted[bt.flat[b] + rank] = w[i];
     }
@@ -828,6 +820,7 @@ namespace velo {
     __shared__ BankTable bt;
     __shared__ unsigned region[n_module_pairs + 1]; // estimated start of each module pair, event-relative
     __shared__ unsigned mp_count[n_module_pairs];
+    __shared__ unsigned staged_first[n_module_pairs + 1]; // staged clusters before each module pair
     __shared__ unsigned warp_sums[33];
     __shared__ unsigned sorted_total;
     __shared__ uint32_t queue[queue_size];
@@ -1015,7 +1008,15 @@ namespace velo {
       }
       unsigned total;
       unsigned excl = block_exclusive_scan(sum, warp_sums, &total);
-      if (threadIdx.x == 0) sorted_total = total;
+      if (threadIdx.x == 0) {
+        sorted_total = total;
+        unsigned staged = 0;
+        for (unsigned mp = 0; mp < n_module_pairs; ++mp) {
+          staged_first[mp] = staged;
+          staged += min(mp_count[mp], region[mp + 1] - region[mp]);
+        }
+        staged_first[n_module_pairs] = staged;
+      }
       for (unsigned q = 0; q < per; ++q) {
         const unsigned b = threadIdx.x * per + q;
         if (b < sort_counters) {
@@ -1026,29 +1027,31 @@ namespace velo {
       }
     }
     __syncthreads();
-    auto module_pair_of = [&](unsigned i) {
+    // the k-th staged cluster of the event: its module pair (the last one whose first staged
+    // cluster is at most k, empty ones skipped) and its staging index
+    const unsigned n_staged = staged_first[n_module_pairs];
+    auto module_pair_of = [&](unsigned k) {
       unsigned lo = 0, hi = n_module_pairs;
       while (hi - lo > 1) {
         const unsigned mid = (lo + hi) / 2;
-        if (region[mid] <= i) lo = mid;
+        if (staged_first[mid] <= k) lo = mid;
         else hi = mid;
       }
       return lo;
     };
-    for (unsigned i = threadIdx.x; i < est_total; i += blockDim.x) {
-      const unsigned mp = module_pair_of(i);
-      const unsigned count = min(mp_count[mp], region[mp + 1] - region[mp]);
-      if (i - region[mp] >= count) continue;
+    for (unsigned k = threadIdx.x; k < n_staged; k += blockDim.x) {
+      const unsigned mp = module_pair_of(k);
+      const unsigned i = region[mp] + (k - staged_first[mp]);
       const unsigned b = mp * sort_buckets + sort_bucket(st.phi(i));
       const unsigned q = bucket_start[b] + slot_in_bucket[i];
       if (q < cap) members[q] = static_cast<uint16_t>(i);
     }
     __syncthreads();
     ClusterView out {p.sorted_container, T};
-    for (unsigned i = threadIdx.x; i < est_total; i += blockDim.x) {
-      const unsigned mp = module_pair_of(i);
-      const unsigned count = min(mp_count[mp], region[mp + 1] - region[mp]);
-      if (i - region[mp] >= count) continue;
+    for (unsigned k = threadIdx.x; k < n_staged; k += blockDim.x) {
+      const unsigned mp = module_pair_of(k);
+      const unsigned i = region[mp] + (k - staged_first[mp]);
+      const unsigned count = staged_first[mp + 1] - staged_first[mp];
       const int16_t phi = st.phi(i);
       const uint32_t id = st.id(i);
       const unsigned b = mp * sort_buckets + sort_bucket(phi);
@@ -1075,7 +1078,7 @@ namespace velo {
     }
     if (threadIdx.x < n_module_pairs) {
       const unsigned mp = threadIdx.x;
-      p.module_cluster_num[e * n_module_pairs + mp] = min(mp_count[mp], region[mp + 1] - region[mp]);
+      p.module_cluster_num[e * n_module_pairs + mp] = staged_first[mp + 1] - staged_first[mp];
     }
     // the event's slices of the global staging and of the sorted bank copies are dead
     __syncthreads();
