@@ -584,7 +584,7 @@ namespace velo {
     (void) v23;
   }
 
-  __global__ void __launch_bounds__(decode_threads) estimate_kernel(EstimateParams p)
+  __global__ void __launch_bounds__(decode_threads, 2048 / decode_threads) estimate_kernel(EstimateParams p)
   {
     __shared__ __align__(8) uint64_t bar;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
