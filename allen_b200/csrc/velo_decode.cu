@@ -2,11 +2,13 @@
 // (velo_calculate_number_of_candidates + velo_estimate_input_size), masked clustering,
 // phi and the sort by phi (velo_masked_clustering + velo_sort_by_phi), one event per CTA.
 //
-// Each CTA stages its event's raw blob (bank offsets + SP words) into shared memory
-// with one bulk copy through the TMA engine (cp.async.bulk, 16-byte aligned span, the
-// ragged tail by plain loads), so the O(n_sp^2) neighbour scans of the reference
-// (EstimateInputSize.cu:111-141, MaskedVeloClustering.cu:361-402) run out of shared
-// memory.  Work is spread one thread per super pixel over the flattened bank list.
+// A CTA reads its event's raw blob (bank offsets + SP words) through L1/L2, or stages it
+// into shared memory with one bulk copy through the TMA engine (cp.async.bulk, 16-byte
+// aligned span, the ragged tail by plain loads) when the launch configuration gives it room.
+// The O(n_sp^2) neighbour scans of the reference (EstimateInputSize.cu:111-141,
+// MaskedVeloClustering.cu:361-402) become binary-searched key ranges of key-sorted bank
+// copies, which the estimate kernel writes once per event and the clustering kernel reuses.
+// Work is spread one thread per super pixel over the flattened bank list.
 //
 // The sorted container is independent of the order in which clusters are produced
 // (rank by (phi, id), SortByPhi.cu:104-122), so clusters are appended to their module
@@ -338,8 +340,10 @@ namespace velo {
   // matching one is.  With a copy of the bank sorted by key (address bits 22:8, plus the
   // sensor bit 23 for bank version 4), all SPs that can match lie in one key range, found
   // by binary search.  The readout does not write SPs in column order, so the copy is made
-  // here, in shared memory behind the staged event; events that leave no room for it keep
-  // the full scans.
+  // here: by the estimate kernel into the event's allocation of a global sort scratch, which
+  // the clustering kernel then reads; without that scratch, by the clustering kernel itself
+  // (in shared memory behind the staged event, or in its slice of the scratch); events that
+  // leave no room for it keep the full scans.
   // ------------------------------------------------------------------------------------
   __device__ __forceinline__ uint32_t sp_key_mask(int version) { return version > 3 ? 0xFFFFu : 0x7FFFu; }
 
