@@ -19,6 +19,7 @@ namespace velo {
 
   constexpr unsigned max_banks = 512;
   constexpr unsigned bank_hints = 512; // bank_of() hints, one per 32 SPs
+  constexpr unsigned estimate_sort_keys = 3584; // SPs of an event whose sort keys fit the estimate kernel's shared memory
 
   // ------------------------------------------------------------------------------------
   // Bulk copy (TMA engine) into shared memory, completion tracked by an mbarrier.
@@ -350,8 +351,31 @@ namespace velo {
   // sorted[bt.flat[b] + r] = the SP word of VP/Velo bank b with rank r by (key, position).
   // Banks hold fewer than 2^16 SPs (the event fits the staging buffer).  Ends with a
   // __syncthreads().
-  __device__ void sort_bank_words(const BankTable& bt, const uint32_t* words, uint32_t* sorted, uint32_t key_mask)
+  // With `keys` (shared memory of key_capacity words, the event's SPs fitting it), the
+  // (key, position) pairs are formed once per SP and the rank loop reads them from there.
+  __device__ void sort_bank_words(const BankTable& bt, const uint32_t* words, uint32_t* sorted, uint32_t key_mask,
+                                  uint32_t* keys = nullptr, unsigned key_capacity = 0)
   {
+    if (keys != nullptr && bt.total_sp <= key_capacity) {
+      for (unsigned f = threadIdx.x; f < bt.total_sp; f += blockDim.x) {
+        const unsigned b = bank_of(bt, f);
+        const unsigned i = f - bt.flat[b];
+        keys[f] = (((words[bt.words_off[b] + i] >> 8) & key_mask) << 16) | i;
+      }
+      __syncthreads();
+      for (unsigned f = threadIdx.x; f < bt.total_sp; f += blockDim.x) {
+        const unsigned b = bank_of(bt, f);
+        const uint32_t* k = keys + bt.flat[b];
+        const unsigned n = bt.flat[b + 1] - bt.flat[b];
+        const uint32_t mine = keys[f];
+        unsigned rank = 0;
+        for (unsigned j = 0; j < n; ++j)
+          rank += k[j] < mine;
+        sorted[f - (mine & 0xFFFFu) + rank] = words[bt.words_off[b] + (mine & 0xFFFFu)];
+      }
+      __syncthreads();
+      return;
+    }
     for (unsigned f = threadIdx.x; f < bt.total_sp; f += blockDim.x) {
       const unsigned b = bank_of(bt, f);
       const unsigned i = f - bt.flat[b];
@@ -478,6 +502,7 @@ namespace velo {
     __shared__ uint16_t queue[estimate_queue];
     __shared__ unsigned queue_count[2];
     __shared__ unsigned sorted_at;
+    __shared__ uint32_t sort_keys[estimate_sort_keys];
 
     const unsigned ev = e + p.in.event_start;
     const bool v23 = p.in.bank_version == 2 || p.in.bank_version == 3;
@@ -504,7 +529,7 @@ namespace velo {
       }
       __syncthreads();
       if (sorted_at != no_sorted_copy) {
-        sort_bank_words(bt, words, p.sp_scratch + sorted_at, key_mask);
+        sort_bank_words(bt, words, p.sp_scratch + sorted_at, key_mask, sort_keys, estimate_sort_keys);
         sorted = p.sp_scratch + sorted_at;
       }
     }
