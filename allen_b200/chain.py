@@ -141,6 +141,8 @@ def _lib():
     lib.velo_chain_synchronize.argtypes = [C.c_void_p, C.POINTER(TotalsC)]
     lib.velo_chain_outputs.restype = C.c_int
     lib.velo_chain_outputs.argtypes = [C.c_void_p, C.POINTER(OutputsC)]
+    lib.velo_check_contracts.restype = C.c_int
+    lib.velo_check_contracts.argtypes = [C.POINTER(OutputsC), C.POINTER(TotalsC), C.c_void_p, C.c_void_p]
     lib.velo_chain_destroy.argtypes = [C.c_void_p]
     lib.velo_chain_sizes.restype = C.c_int
     lib.velo_chain_sizes.argtypes = [C.c_void_p, C.c_uint, C.c_ulonglong, C.c_int, C.POINTER(SizesC)]
@@ -193,6 +195,24 @@ def _lib():
     lib.velo_seed_trainer_destroy.argtypes = [C.c_void_p]
     lib._typed = True
     return lib
+
+
+CONTRACTS = ["cluster_outside", "unsorted", "track_size", "repeated_hit", "zero_id", "id_type", "offsets"]
+
+
+def check_contracts(outputs: dict, totals: dict, stream=None) -> dict:
+    """The reference's contracts on a run's outputs, counted on the device
+    (velo_check_contracts): outputs maps Allen output names to device pointers (FP32 layout),
+    totals holds the run's host totals (VeloChainTotals fields).  Returns violations per
+    contract (all zero for a correct run)."""
+    import torch
+    lib = _lib()
+    o = OutputsC(**{f: outputs.get(f) for f in OUTPUT_FIELDS})
+    t = TotalsC(**{f: int(totals.get(f, 0)) for f, _ in TotalsC._fields_})
+    counts = torch.zeros(len(CONTRACTS), dtype=torch.int32, device="cuda")
+    _check(lib, lib.velo_check_contracts(C.byref(o), C.byref(t), stream if stream is not None else _current_stream(),
+                                         C.c_void_p(counts.data_ptr())))
+    return dict(zip(CONTRACTS, (int(v) for v in counts.cpu().tolist())))
 
 
 def _check(lib, status, flags=0):

@@ -132,6 +132,30 @@ typedef struct {
   unsigned device_flags;                                 /* velo::ErrorBits raised by the kernels */
 } VeloChainTotals;
 
+/* The reference's debug-build contracts on a run's outputs, checked on the device: the
+ * cluster checks of SearchByTripletContracts.cu:6-81 (per module pair the sorted container is
+ * strictly increasing in (phi, id, x, y); -100 < x, y < 100 mm), its track checks (:83-120: at
+ * most 26 hits, no hit twice) and lhcb_id_container_checks (VeloConsolidateTracks.cu:194-269:
+ * consolidated LHCb ids non-zero with the VELO type in bits 28-31; offsets that never decrease
+ * and end at the run's totals).  Counts of violations go to dev_counts[VELO_CONTRACTS] (device
+ * u32, zeroed by this call); outputs in the FP32 coordinate layout (velo_chain_outputs) with
+ * the totals velo_chain_synchronize() returned for them, which bound every read (from a run
+ * that raised no device flag, every buffer holds at least what its total names).  Enqueued on
+ * `stream` without host synchronisation and without allocation; all zero for a correct run, in
+ * plain and learned mode alike. */
+typedef enum {
+  VELO_CONTRACT_CLUSTER_OUTSIDE = 0, /* clusters outside (-100, 100) mm in x or y */
+  VELO_CONTRACT_UNSORTED = 1,        /* neighbouring clusters of a module pair out of (phi, id, x, y) order */
+  VELO_CONTRACT_TRACK_SIZE = 2,      /* tracks above 26 hits (or beyond their container) */
+  VELO_CONTRACT_REPEATED_HIT = 3,    /* tracks with a hit twice */
+  VELO_CONTRACT_ZERO_ID = 4,         /* zero consolidated LHCb ids */
+  VELO_CONTRACT_ID_TYPE = 5,         /* consolidated LHCb ids without the VELO type */
+  VELO_CONTRACT_OFFSETS = 6,         /* decreasing track or hit offsets, or ends other than the totals */
+  VELO_CONTRACTS = 7
+} VeloContract;
+VeloStatus velo_check_contracts(
+  const VeloChainOutputs* outputs, const VeloChainTotals* totals, VeloStream stream, unsigned* dev_counts);
+
 /* Library */
 const char* velo_last_error_string(void);
 VeloStatus velo_device_check(void); /* an sm_100 device is current and the kernels load */
