@@ -407,6 +407,7 @@ def run_ours(args):
     learned = None
     if not args.no_learned:
         from allen_b200 import seed_pruner
+        from allen_b200.chain import check_contracts
         from allen_b200.validation import DeviceTruth, evaluate_device
         plain_cfg = chain.get_config()
         plain_stages = {k: v["ms_per_launch"] for k, v in per_kernel.items()}
@@ -415,9 +416,11 @@ def run_ours(args):
         def quality():
             tot = dict(tracks=0, ghosts=0, reconstructible=0, reconstructed=0, clones=0)
             cand = searched = fallback = 0
+            violations = 0  # the reference's output contracts, counted on the device
             for s_, d, t in zip(slices, dev, truths):
                 chain.run(d, use_graph=True)
-                chain.synchronize(check=False)
+                slice_totals = chain.synchronize(check=False)
+                violations += sum(check_contracts(chain.device_outputs(), slice_totals).values())
                 r = evaluate_device(chain, t)
                 for k in tot:
                     tot[k] += r[k]
@@ -430,7 +433,8 @@ def run_ours(args):
                     "clone_rate": round(tot["clones"] / max(tot["reconstructed"] + tot["clones"], 1), 6),
                     "tracks": tot["tracks"], "reconstructible": tot["reconstructible"],
                     "candidates_searched_fraction": round(searched / max(cand, 1), 4),
-                    "fallback_event_fraction": round(fallback / max(events_step, 1), 6)}
+                    "fallback_event_fraction": round(fallback / max(events_step, 1), 6),
+                    "contract_violations": violations}
 
         q_plain = quality()
         seed_pruner.use_learned(chain)
